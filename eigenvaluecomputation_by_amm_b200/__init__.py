@@ -1,0 +1,11 @@
+"""B200-native power method for λ_max(A·Aᵀ): exact, previous AMM and proposed AMM.
+
+The compute path is libamm.so (hand-written sm_100a CUDA behind the C ABI of include/amm.h);
+this package is its Python face.  The library is loaded on first use and every entry point
+fails loudly (ImportError) when it has not been built
+(``python -m eigenvaluecomputation_by_amm_b200.build``); there is no CPU fallback.
+"""
+from ._lib import AmmError  # noqa: F401
+from .api import AMMContext, column_major  # noqa: F401
+
+__all__ = ["AMMContext", "column_major", "AmmError"]

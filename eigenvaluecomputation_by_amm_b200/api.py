@@ -1,0 +1,265 @@
+"""Python face of libamm over the C ABI (include/amm.h).
+
+PyTorch provides device memory and streams; every computation runs in libamm's CUDA kernels.
+Matrices are column-major m x n: a torch tensor ``A`` of shape (m, n) with ``A.stride(0) == 1``
+(``column_major(t)`` makes one), exactly the layout the reference uses (lda = m).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import AmmError, amm_config, check
+
+__all__ = ["AMMContext", "column_major", "AmmError"]
+
+
+def column_major(A: torch.Tensor) -> torch.Tensor:
+    """A column-major copy (stride (1, m)) of a 2-D tensor, keeping shape (m, n)."""
+    return A.t().contiguous().t()
+
+
+def _stream(stream=None) -> int:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream)
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else int(t.data_ptr())
+
+
+def _u32(t: torch.Tensor) -> torch.Tensor:
+    """View an int32/uint32 tensor as the int32 carrier used for uint32 buffers."""
+    if t.dtype == torch.int32:
+        return t
+    if t.dtype == torch.uint32:
+        return t.view(torch.int32)
+    raise TypeError("sampling states/indices must be int32 or uint32 tensors (bit pattern kept)")
+
+
+class AMMContext:
+    """One libamm context (the reference's ``device_memory`` with its buffers and handles).
+
+    Parameters mirror ``host_memory`` (host_memory.h:26-50): ``c`` samples (0 = n), ``step``
+    iterations, ``vr_period`` / ``vr_adaptive_threshold`` variance reduction, ``sanity``.
+    ``dtype`` is the storage type of A ("f32" or "bf16"); ``cdf_precision`` "f64" (default)
+    or "f32" (the reference's FP32 CDF and target).
+    """
+
+    def __init__(self, m: int, n: int, c: int = 0, step: int = 10, vr_period: int = 0,
+                 vr_adaptive_threshold: float = 0.0, tol: float = 0.0, dtype: str = "f32",
+                 cdf_precision: str = "f64", sanity: bool = False, use_graph: bool = True,
+                 device: Optional[int] = None):
+        self.lib = _lib.load()
+        cfg = amm_config()
+        self.lib.amm_config_default(C.byref(cfg))
+        cfg.m, cfg.n, cfg.c, cfg.step = int(m), int(n), int(c), int(step)
+        cfg.vr_period = int(vr_period)
+        cfg.vr_adaptive_threshold = float(vr_adaptive_threshold)
+        cfg.tol = float(tol)
+        cfg.dtype = {"f32": _lib.AMM_F32, "bf16": _lib.AMM_BF16}[dtype]
+        cfg.cdf_precision = {"f64": _lib.AMM_CDF_F64, "f32": _lib.AMM_CDF_F32}[cdf_precision]
+        cfg.sanity = 1 if sanity else 0
+        cfg.use_graph = 1 if use_graph else 0
+        self.cfg = cfg
+        self.m, self.n = int(m), int(n)
+        self.c = int(c) if c else int(n)
+        self.step = int(step)
+        self.dtype = dtype
+        self.cdf_precision = cdf_precision
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self._ctx = C.c_void_p()
+        check(self.lib.amm_create(C.byref(self._ctx), C.byref(cfg), self.device), "amm_create")
+        self._A = None
+        self._vstar = None
+        self._dev = torch.device("cuda", self.device)
+
+    # -- lifetime ---------------------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            check(self.lib.amm_destroy(self._ctx), "amm_destroy")
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- inputs -------------------------------------------------------------------------
+    def set_matrix(self, A: torch.Tensor, stream=None):
+        """Bind A (kept referenced) and run the one-pass set-up (stats, z, v, CDFs)."""
+        want = torch.float32 if self.dtype == "f32" else torch.bfloat16
+        if A.dtype != want or A.device.type != "cuda" or A.dim() != 2:
+            raise AmmError(_lib.AMM_ERR_INVALID_ARGUMENT, f"set_matrix: need a CUDA {want} matrix")
+        if tuple(A.shape) != (self.m, self.n):
+            raise AmmError(_lib.AMM_ERR_INVALID_ARGUMENT, "set_matrix: shape must be (m, n)")
+        if A.stride(0) != 1 and self.n > 1:
+            raise AmmError(_lib.AMM_ERR_INVALID_ARGUMENT, "set_matrix: A must be column-major")
+        ld = A.stride(1) if self.n > 1 else self.m
+        check(self.lib.amm_set_matrix(self._ctx, _ptr(A), ld, _stream(stream)), "amm_set_matrix")
+        self._A = A
+
+    def set_rng_state(self, states: torch.Tensor, stream=None):
+        s = _u32(states)
+        check(self.lib.amm_set_rng_state(self._ctx, _ptr(s), s.numel(), _stream(stream)),
+              "amm_set_rng_state")
+
+    def get_rng_state(self, count: Optional[int] = None, stream=None) -> torch.Tensor:
+        count = self.c if count is None else int(count)
+        out = torch.empty(count, dtype=torch.int32, device=self._dev)
+        check(self.lib.amm_get_rng_state(self._ctx, _ptr(out), count, _stream(stream)),
+              "amm_get_rng_state")
+        return out
+
+    def seed_rng(self, seed: int, count: Optional[int] = None, stream=None):
+        count = max(self.m, self.c) if count is None else int(count)
+        check(self.lib.amm_seed_rng(self._ctx, int(seed), count, _stream(stream)), "amm_seed_rng")
+
+    def seed_start_vectors(self, seed: int):
+        check(self.lib.amm_seed_start_vectors(self._ctx, int(seed)), "amm_seed_start_vectors")
+
+    def draw_start_vector(self, stream=None) -> torch.Tensor:
+        x0 = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        check(self.lib.amm_draw_start_vector(self._ctx, _ptr(x0), _stream(stream)),
+              "amm_draw_start_vector")
+        return x0
+
+    def set_cdf(self, which: int, cdf: torch.Tensor, stream=None):
+        want = torch.float32 if self.cdf_precision == "f32" else torch.float64
+        cdf = cdf.to(device=self._dev, dtype=want).contiguous()
+        check(self.lib.amm_set_cdf(self._ctx, int(which), _ptr(cdf), _stream(stream)),
+              "amm_set_cdf")
+        torch.cuda.current_stream().synchronize()
+
+    def set_eigenvector(self, vstar: Optional[torch.Tensor], stream=None):
+        if vstar is None:
+            check(self.lib.amm_set_eigenvector(self._ctx, None, _stream(stream)), "amm_set_eigenvector")
+            self._vstar = None
+            return
+        v = vstar.to(device=self._dev, dtype=torch.float64).contiguous()
+        check(self.lib.amm_set_eigenvector(self._ctx, _ptr(v), _stream(stream)), "amm_set_eigenvector")
+        self._vstar = v
+
+    # -- power method ---------------------------------------------------------------------
+    def power_method(self, method: str, x0: torch.Tensor, stream=None) -> "AMMContext":
+        """Enqueue one power-method call (asynchronous); read it with trace()/vectors()."""
+        x0 = x0.to(device=self._dev, dtype=torch.float32).contiguous()
+        check(self.lib.amm_power_method(self._ctx, _lib.METHODS[method], _ptr(x0), _stream(stream)),
+              f"amm_power_method({method})")
+        self._x0_keep = x0
+        return self
+
+    def trace(self, stream=None) -> dict:
+        cap = self.step
+        eigs = np.zeros(cap, np.float64)
+        errs = np.zeros(cap, np.float64)
+        coss = np.zeros(cap, np.float64)
+        kinds = np.zeros(cap, np.int32)
+        distinct = np.zeros(cap, np.int64)
+        t_ns = np.zeros(cap, np.float64)
+        run = C.c_int64(0)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        check(self.lib.amm_get_trace(self._ctx, p(eigs), p(errs), p(coss), p(kinds), p(distinct),
+                                     p(t_ns), C.byref(run), _stream(stream)), "amm_get_trace")
+        k = int(run.value)
+        return {"eigs": eigs[:k], "errs": errs[:k], "coss": coss[:k],
+                "kinds": [_lib.STEP_KINDS[int(v)] for v in kinds[:k]], "distinct": distinct[:k],
+                "t_ns": t_ns[:k], "steps_run": k}
+
+    def vectors(self, stream=None):
+        x = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        y = torch.empty_like(x)
+        check(self.lib.amm_get_vectors(self._ctx, _ptr(x), _ptr(y), _stream(stream)), "amm_get_vectors")
+        return x, y
+
+    # -- single products and helpers (the reference's per-step functions) -----------------
+    def _vec(self, t):
+        return None if t is None else t.to(device=self._dev, dtype=torch.float32).contiguous()
+
+    def core_previousAMM(self, x, x_memo=None, y_memo=None, stream=None):
+        x, xm, ym = self._vec(x), self._vec(x_memo), self._vec(y_memo)
+        y = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        idx = torch.empty(self.c, dtype=torch.int32, device=self._dev)
+        check(self.lib.amm_core_previousAMM(self._ctx, _ptr(x), _ptr(xm), _ptr(ym), _ptr(y), _ptr(idx),
+                                            _stream(stream)), "amm_core_previousAMM")
+        return y, idx
+
+    def core_proposedAMM(self, x, x_memo=None, y_memo=None, stream=None):
+        x, xm, ym = self._vec(x), self._vec(x_memo), self._vec(y_memo)
+        y = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        idx = torch.empty(self.c, dtype=torch.int32, device=self._dev)
+        check(self.lib.amm_core_proposedAMM(self._ctx, _ptr(x), _ptr(xm), _ptr(ym), _ptr(y), _ptr(idx),
+                                            _stream(stream)), "amm_core_proposedAMM")
+        return y, idx
+
+    def exact_product(self, x, stream=None):
+        x = self._vec(x)
+        y = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        check(self.lib.amm_exact_product(self._ctx, _ptr(x), _ptr(y), _stream(stream)), "amm_exact_product")
+        return y
+
+    def rayleigh_normalize(self, x: torch.Tensor, y: torch.Tensor, stream=None):
+        """Returns (λ, err, cos) and normalises x <- y/‖y‖ in place."""
+        out = torch.zeros(4, dtype=torch.float64, device=self._dev)
+        check(self.lib.amm_rayleigh_normalize(self._ctx, _ptr(x), _ptr(self._vec(y)), _ptr(out),
+                                              _stream(stream)), "amm_rayleigh_normalize")
+        o = out.cpu().numpy()
+        return float(o[0]), float(o[1]), float(o[2])
+
+    def normalize(self, x: torch.Tensor, stream=None):
+        check(self.lib.amm_normalize(self._ctx, _ptr(x), _stream(stream)), "amm_normalize")
+        return x
+
+    def column_stats(self, stream=None) -> dict:
+        n, m = self.n, self.m
+        out = {k: torch.empty(n, dtype=torch.float32, device=self._dev) for k in ("alpha", "norm", "normp")}
+        out.update({k: torch.empty(m, dtype=torch.float32, device=self._dev) for k in ("z", "v")})
+        a2 = C.c_double(0.0)
+        check(self.lib.amm_get_column_stats(self._ctx, _ptr(out["alpha"]), _ptr(out["norm"]),
+                                            _ptr(out["normp"]), _ptr(out["z"]), _ptr(out["v"]),
+                                            C.byref(a2), _stream(stream)), "amm_get_column_stats")
+        out["alpha2"] = a2.value
+        return out
+
+    def sampling_tables(self, which: int, stream=None):
+        dt = torch.float32 if self.cdf_precision == "f32" else torch.float64
+        cdf = torch.empty(self.n, dtype=dt, device=self._dev)
+        w = torch.empty(self.n, dtype=torch.float32, device=self._dev)
+        check(self.lib.amm_get_sampling_tables(self._ctx, int(which), _ptr(cdf), _ptr(w), _stream(stream)),
+              "amm_get_sampling_tables")
+        return cdf, w
+
+    def sample_indices(self, which: int, stream=None) -> torch.Tensor:
+        idx = torch.empty(self.c, dtype=torch.int32, device=self._dev)
+        check(self.lib.amm_sample_indices(self._ctx, int(which), _ptr(idx), _stream(stream)),
+              "amm_sample_indices")
+        return idx
+
+    def benchmark_product(self, kind: str, reps: int = 10, stream=None):
+        """Mean CUDA-event time (ms) of one fused product launch and its distinct columns."""
+        k = {"exact": 1, "previous": 2, "proposed": 3}[kind]
+        ms = C.c_float(0.0)
+        d = C.c_int64(0)
+        check(self.lib.amm_benchmark_product(self._ctx, k, int(reps), C.byref(ms), C.byref(d),
+                                             _stream(stream)), "amm_benchmark_product")
+        return float(ms.value), int(d.value)
+
+    def grad_lambda(self, v: torch.Tensor, stream=None) -> torch.Tensor:
+        """∂λ/∂A = 2·v·(vᵀA) as an (m, n) column-major FP32 tensor."""
+        v = self._vec(v)
+        g = torch.empty(self.n, self.m, dtype=torch.float32, device=self._dev).t()
+        check(self.lib.amm_grad_lambda(self._ctx, _ptr(v), _ptr(g), self.m, _stream(stream)),
+              "amm_grad_lambda")
+        return g

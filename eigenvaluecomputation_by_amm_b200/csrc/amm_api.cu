@@ -1,0 +1,777 @@
+// Host side of libamm: the context, the C ABI of include/amm.h and the CUDA-graph cache.
+#include <cuda_runtime.h>
+#include <curand.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "amm.h"
+#include "amm_internal.h"
+
+using amm::Buffers;
+using amm::CallCfg;
+using amm::PanelGeom;
+
+namespace {
+
+thread_local std::string g_last_cuda_error;
+
+int cuda_fail(cudaError_t e, const char* what) {
+  g_last_cuda_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return AMM_ERR_CUDA;
+}
+
+#define AMM_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+struct DeviceGuard {
+  int old = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&old);
+    if (old != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (old >= 0 && cur != old) cudaSetDevice(old);
+  }
+};
+
+// key of a captured call: method + every CallCfg field that changes the launch sequence
+using GraphKey = std::tuple<int, int, double, double, int, int, int, int>;
+
+}  // namespace
+
+struct amm_ctx {
+  amm_config cfg{};
+  int device = 0;
+  int nsm = 0;
+  int sanity_active = 0;
+  Buffers b{};
+  PanelGeom geom{};
+  bool matrix_set = false;
+  bool setup_done = false;   // column statistics, z, v and CDFs of the bound matrix
+  void* pool = nullptr;
+  size_t pool_bytes = 0;
+  int64_t state_len = 0;
+  float* x0_buf = nullptr;
+  float* x_final = nullptr;
+  float* y_final = nullptr;
+  double* out3 = nullptr;
+  cudaStream_t cap_stream = nullptr;
+  curandGenerator_t x0_gen = nullptr;
+  std::map<GraphKey, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+  int last_step = 0;
+  bool has_run = false;
+  CallCfg last_cc{};
+};
+
+namespace {
+
+void drop_graphs(amm_ctx* ctx) {
+  for (auto& kv : ctx->graphs) {
+    if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
+    if (kv.second.first) cudaGraphDestroy(kv.second.first);
+  }
+  ctx->graphs.clear();
+}
+
+int elem_size(int dtype) { return dtype == AMM_BF16 ? 2 : 4; }
+
+// Carve every buffer out of one allocation (256-byte aligned pieces).
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base ? base + off : nullptr);
+    off += sizeof(T) * (count ? count : 1);
+    return p;
+  }
+};
+
+void layout(amm_ctx* ctx, Carver& cv) {
+  Buffers& b = ctx->b;
+  const int64_t m = ctx->cfg.m, n = ctx->cfg.n, c = ctx->cfg.c, step = ctx->cfg.step;
+  const bool f32 = ctx->cfg.cdf_precision == AMM_CDF_F32;
+  b.alpha = cv.take<float>(n);
+  b.norm = cv.take<float>(n);
+  b.normp = cv.take<float>(n);
+  for (int w = 0; w < 2; ++w) {
+    b.cdf64[w] = f32 ? nullptr : cv.take<double>(n);
+    b.cdf32[w] = f32 ? cv.take<float>(n) : nullptr;
+    b.wts[w] = cv.take<float>(n);
+    b.coarse64[w] = f32 ? nullptr : cv.take<double>(b.ncoarse);
+    b.coarse32[w] = f32 ? cv.take<float>(b.ncoarse) : nullptr;
+  }
+  b.z = cv.take<float>(m);
+  b.v = cv.take<float>(m);
+  b.y[0] = cv.take<float>(m);
+  b.y[1] = cv.take<float>(m);
+  b.x_memo = cv.take<float>(m);
+  b.y_memo = cv.take<float>(m);
+  b.vstar = cv.take<double>(m);
+  for (int w = 0; w < 2; ++w) {
+    b.states[w] = cv.take<uint32_t>(ctx->state_len);
+    b.count[w] = cv.take<uint32_t>(n);
+    b.chunk[w] = cv.take<uint32_t>(b.nchunks);
+    b.samples[w] = cv.take<uint32_t>(c);
+  }
+  b.distinct_idx = cv.take<uint32_t>(c);
+  b.distinct_mult = cv.take<uint32_t>(c);
+  b.partials = cv.take<float>((size_t)ctx->nsm * m);
+  b.spart = cv.take<float>(ctx->nsm);
+  b.spart64 = cv.take<double>(ctx->nsm);
+  b.rpart = cv.take<double>(4 * ((m + 127) / 128));
+  b.ticket = cv.take<uint32_t>(4);
+  b.alpha2 = cv.take<double>(1);
+  b.colvec = cv.take<float>(n);
+  b.st = cv.take<amm::IterState>(2);
+  b.eigs = cv.take<double>(step);
+  b.errs = cv.take<double>(step);
+  b.coss = cv.take<double>(step);
+  b.kinds = cv.take<int32_t>(step);
+  b.distinct_hist = cv.take<int32_t>(step);
+  b.tstamp = cv.take<unsigned long long>(step + 1);
+  b.status = cv.take<uint32_t>(1);
+  ctx->x0_buf = cv.take<float>(m);
+  ctx->x_final = cv.take<float>(m);
+  ctx->y_final = cv.take<float>(m);
+  ctx->out3 = cv.take<double>(4);
+}
+
+CallCfg make_cc(const amm_ctx* ctx, int method) {
+  CallCfg cc{};
+  cc.method = method;
+  cc.vr_period = (int32_t)ctx->cfg.vr_period;
+  cc.vr_thr = ctx->cfg.vr_adaptive_threshold;
+  cc.tol = ctx->cfg.tol;
+  cc.variance_reduction = (ctx->cfg.vr_period > 0 || ctx->cfg.vr_adaptive_threshold > 0.0) ? 1 : 0;
+  cc.sanity = ctx->sanity_active;
+  cc.uses_amm = method != amm::kMethodExact;
+  cc.step = (int32_t)ctx->cfg.step;
+  return cc;
+}
+
+int ensure_setup(amm_ctx* ctx, cudaStream_t s);
+
+// The launch sequence of one call (captured into a graph or issued directly).
+int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
+                 cudaStream_t s) {
+  const Buffers& b = ctx->b;
+  AMM_CUDA(amm::launch_init(b, cc, x0, no_normalize, s));
+  for (int i = 0; i < cc.step; ++i) {
+    AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, s));
+    AMM_CUDA(amm::launch_iter_reduce(b, cc, i, s));
+  }
+  AMM_CUDA(amm::launch_finalize(b, cc, ctx->x_final, ctx->y_final, s));
+  return AMM_OK;
+}
+
+int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
+             cudaStream_t s) {
+  if (cc.uses_amm) {
+    int rc = ensure_setup(ctx, s);
+    if (rc) return rc;
+  }
+  if (x0 != ctx->x0_buf)
+    AMM_CUDA(cudaMemcpyAsync(ctx->x0_buf, x0, sizeof(float) * ctx->cfg.m,
+                             cudaMemcpyDeviceToDevice, s));
+  ctx->last_cc = cc;
+  ctx->last_step = cc.step;
+  ctx->has_run = true;
+  if (!ctx->cfg.use_graph) return enqueue_call(ctx, cc, ctx->x0_buf, no_normalize, s);
+  const GraphKey key{cc.method, cc.vr_period, cc.vr_thr, cc.tol, cc.variance_reduction,
+                     cc.sanity, cc.step, no_normalize};
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    if (!ctx->cap_stream)
+      AMM_CUDA(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+    AMM_CUDA(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeRelaxed));
+    const int64_t before = amm::launch_count();
+    int rc = enqueue_call(ctx, cc, ctx->x0_buf, no_normalize, ctx->cap_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(ctx->cap_stream, &g);
+    // captured launches run when the graph is launched; count them there instead
+    amm::count_launch(-(int)(amm::launch_count() - before));
+    if (rc != AMM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    cudaGraphExec_t ex = nullptr;
+    ce = cudaGraphInstantiate(&ex, g, 0);
+    if (ce != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_fail(ce, "cudaGraphInstantiate");
+    }
+    it = ctx->graphs.emplace(key, std::make_pair(g, ex)).first;
+  }
+  AMM_CUDA(cudaGraphLaunch(it->second.second, s));
+  amm::count_launch(2 + 2 * cc.step);
+  return AMM_OK;
+}
+
+int check_ready(amm_ctx* ctx) {
+  if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
+  if (!ctx->matrix_set) return AMM_ERR_NOT_READY;
+  return AMM_OK;
+}
+
+// The one-pass set-up (statistics, z, v, CDFs) runs on first need: AMM calls and the
+// accessors; exact calls never need it.
+int ensure_setup(amm_ctx* ctx, cudaStream_t s) {
+  if (ctx->setup_done) return AMM_OK;
+  AMM_CUDA(amm::launch_setup_panel(ctx->b, ctx->geom, s));
+  AMM_CUDA(amm::launch_setup_reduce(ctx->b, s));
+  AMM_CUDA(amm::launch_build_cdf(ctx->b, -1, 0, ctx->sanity_active, s));
+  ctx->setup_done = true;
+  return AMM_OK;
+}
+
+int read_status(amm_ctx* ctx, cudaStream_t s) {
+  uint32_t st = 0;
+  AMM_CUDA(cudaMemcpyAsync(&st, ctx->b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  AMM_CUDA(cudaStreamSynchronize(s));
+  if (st) {
+    AMM_CUDA(cudaMemsetAsync(ctx->b.status, 0, sizeof(uint32_t), s));
+    if (st & amm::kDevTimeout) {
+      // the sampling buffers may be inconsistent after an aborted kernel
+      for (int w = 0; w < 2; ++w) {
+        AMM_CUDA(cudaMemsetAsync(ctx->b.count[w], 0, sizeof(uint32_t) * ctx->cfg.n, s));
+        AMM_CUDA(cudaMemsetAsync(ctx->b.chunk[w], 0, sizeof(uint32_t) * ctx->b.nchunks, s));
+      }
+      AMM_CUDA(cudaMemsetAsync(ctx->b.ticket, 0, sizeof(uint32_t) * 4, s));
+      return AMM_ERR_DEVICE_TIMEOUT;
+    }
+    return AMM_ERR_DEGENERATE;
+  }
+  return AMM_OK;
+}
+
+int single_product(amm_ctx* ctx, int method, const float* x, const float* x_memo,
+                   const float* y_memo, float* y, uint32_t* idx_out, cudaStream_t s) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!x || !y) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  const size_t vb = sizeof(float) * ctx->cfg.m;
+  if (x_memo)
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.x_memo, x_memo, vb, cudaMemcpyDeviceToDevice, s));
+  else
+    AMM_CUDA(cudaMemsetAsync(ctx->b.x_memo, 0, vb, s));
+  if (y_memo)
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.y_memo, y_memo, vb, cudaMemcpyDeviceToDevice, s));
+  else
+    AMM_CUDA(cudaMemsetAsync(ctx->b.y_memo, 0, vb, s));
+  CallCfg cc = make_cc(ctx, method);
+  cc.vr_period = 0;
+  cc.vr_thr = 0.0;
+  cc.variance_reduction = 0;
+  cc.tol = 0.0;
+  cc.step = 1;
+  if (cc.uses_amm) {
+    rc = ensure_setup(ctx, s);
+    if (rc) return rc;
+  }
+  AMM_CUDA(cudaMemcpyAsync(ctx->x0_buf, x, vb, cudaMemcpyDeviceToDevice, s));
+  ctx->last_cc = cc;
+  ctx->last_step = 1;
+  ctx->has_run = true;
+  rc = enqueue_call(ctx, cc, ctx->x0_buf, /*no_normalize=*/1, s);
+  if (rc) return rc;
+  AMM_CUDA(cudaMemcpyAsync(y, ctx->y_final, vb, cudaMemcpyDeviceToDevice, s));
+  if (idx_out && method != amm::kMethodExact) {
+    if (ctx->sanity_active) {
+      std::vector<uint32_t> seq(ctx->cfg.n);
+      for (int64_t k = 0; k < ctx->cfg.n; ++k) seq[k] = (uint32_t)k;
+      AMM_CUDA(cudaMemcpyAsync(idx_out, seq.data(), sizeof(uint32_t) * ctx->cfg.n,
+                               cudaMemcpyHostToDevice, s));
+      AMM_CUDA(cudaStreamSynchronize(s));
+    } else {
+      AMM_CUDA(amm::launch_expand_sorted(ctx->b, ctx->b.distinct_hist, idx_out, s));
+    }
+  }
+  return AMM_OK;
+}
+
+}  // namespace
+
+// ============================================================================================
+// C ABI
+// ============================================================================================
+extern "C" {
+
+void amm_config_default(amm_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->m = 128;
+  cfg->n = 128;
+  cfg->c = 0;
+  cfg->step = 10;
+  cfg->vr_period = 0;
+  cfg->vr_adaptive_threshold = 0.0;
+  cfg->tol = 0.0;
+  cfg->dtype = AMM_F32;
+  cfg->cdf_precision = AMM_CDF_F64;
+  cfg->sanity = 0;
+  cfg->use_graph = 1;
+}
+
+const char* amm_status_string(int status) {
+  switch (status) {
+    case AMM_OK: return "ok";
+    case AMM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case AMM_ERR_ALIGNMENT: return "misaligned matrix: A and ld*elem_size must be 16-byte aligned, m*elem_size a multiple of 16";
+    case AMM_ERR_UNSUPPORTED: return "unsupported shape (m > 16384 or m not a multiple of 16/elem_size)";
+    case AMM_ERR_NOT_READY: return "no matrix bound: call amm_set_matrix first";
+    case AMM_ERR_DEGENERATE: return "degenerate input: zero or non-finite sampling CDF, start vector or eigenvalue";
+    case AMM_ERR_CUDA: return "CUDA runtime error";
+    case AMM_ERR_DEVICE_TIMEOUT: return "a bounded device-side wait timed out";
+    case AMM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case AMM_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* amm_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+int64_t amm_kernel_launch_count(void) { return amm::launch_count(); }
+
+int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
+  if (!out || !cfg_in) return AMM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  amm_config cfg = *cfg_in;
+  if (cfg.c == 0) cfg.c = cfg.n;
+  if (cfg.m < 1 || cfg.n < 1 || cfg.c < 1 || cfg.step < 1) return AMM_ERR_INVALID_ARGUMENT;
+  if (cfg.n > (int64_t)1 << 30 || cfg.m > (int64_t)1 << 30 || cfg.c > (int64_t)1 << 26 ||
+      cfg.step > (int64_t)1 << 24)
+    return AMM_ERR_INVALID_ARGUMENT;
+  if (cfg.dtype != AMM_F32 && cfg.dtype != AMM_BF16) return AMM_ERR_INVALID_ARGUMENT;
+  if (cfg.cdf_precision != AMM_CDF_F64 && cfg.cdf_precision != AMM_CDF_F32)
+    return AMM_ERR_INVALID_ARGUMENT;
+  if (cfg.vr_period < 0 || cfg.vr_adaptive_threshold < 0.0 || cfg.tol < 0.0)
+    return AMM_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AMM_ERR_NO_DEVICE;
+  if (device < 0 || device >= ndev) return AMM_ERR_INVALID_ARGUMENT;
+  if ((cfg.m * elem_size(cfg.dtype)) % 16 != 0) return AMM_ERR_ALIGNMENT;
+  if (cfg.m > 16384) return AMM_ERR_UNSUPPORTED;
+
+  DeviceGuard dg(device);
+  auto* ctx = new amm_ctx();
+  ctx->cfg = cfg;
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (ctx->nsm < 1) ctx->nsm = 1;
+  ctx->sanity_active = (cfg.sanity && cfg.c == cfg.n) ? 1 : 0;
+  if (!amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm, &ctx->geom)) {
+    delete ctx;
+    return AMM_ERR_UNSUPPORTED;
+  }
+  Buffers& b = ctx->b;
+  b.m = (int32_t)cfg.m;
+  b.n = (int32_t)cfg.n;
+  b.c = (int32_t)cfg.c;
+  b.dtype = cfg.dtype;
+  b.cdf_f32 = cfg.cdf_precision == AMM_CDF_F32 ? 1 : 0;
+  b.nsm = ctx->nsm;
+  int seg = amm::kSeg;
+  while (cfg.n / seg > amm::kCoarseMax) seg <<= 1;
+  b.seg = seg;
+  b.ncoarse = (int32_t)(cfg.n / seg);
+  int shift = 7;
+  while (((cfg.n + (1 << shift) - 1) >> shift) > 4096) ++shift;
+  b.chunk_shift = shift;
+  b.nchunks = (int32_t)((cfg.n + (1 << shift) - 1) >> shift);
+  ctx->state_len = cfg.c > cfg.m ? cfg.c : cfg.m;
+
+  Carver probe{nullptr};
+  layout(ctx, probe);
+  ctx->pool_bytes = probe.off + 256;
+  cudaError_t e = cudaMalloc(&ctx->pool, ctx->pool_bytes);
+  if (e != cudaSuccess) {
+    delete ctx;
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? AMM_ERR_OUT_OF_MEMORY : cuda_fail(e, "cudaMalloc");
+  }
+  Carver cv{static_cast<char*>(ctx->pool)};
+  layout(ctx, cv);
+  e = cudaMemset(ctx->pool, 0, ctx->pool_bytes);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaFree(ctx->pool);
+    delete ctx;
+    return cuda_fail(e, "cudaMemset");
+  }
+  *out = ctx;
+  return AMM_OK;
+}
+
+int amm_destroy(amm_ctx* ctx) {
+  if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  drop_graphs(ctx);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->x0_gen) curandDestroyGenerator(ctx->x0_gen);
+  if (ctx->pool) cudaFree(ctx->pool);
+  delete ctx;
+  return AMM_OK;
+}
+
+int amm_set_matrix(amm_ctx* ctx, const void* dA, int64_t ld, void* stream) {
+  if (!ctx || !dA) return AMM_ERR_INVALID_ARGUMENT;
+  const int es = elem_size(ctx->cfg.dtype);
+  if (ld < ctx->cfg.m) return AMM_ERR_INVALID_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(dA) & 15) != 0 || (ld * es) % 16 != 0) return AMM_ERR_ALIGNMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  (void)s;
+  ctx->b.A = dA;
+  ctx->b.ld = ld;
+  drop_graphs(ctx);
+  ctx->matrix_set = true;
+  ctx->setup_done = false;
+  return AMM_OK;
+}
+
+int amm_set_rng_state(amm_ctx* ctx, const uint32_t* d_states, int64_t count, void* stream) {
+  if (!ctx || !d_states || count < ctx->cfg.c || count > ctx->state_len)
+    return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  for (int w = 0; w < 2; ++w)
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.states[w], d_states, sizeof(uint32_t) * count,
+                             cudaMemcpyDeviceToDevice, s));
+  return AMM_OK;
+}
+
+int amm_get_rng_state(amm_ctx* ctx, uint32_t* d_out, int64_t count, void* stream) {
+  if (!ctx || !d_out || count < 1 || count > ctx->state_len) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  AMM_CUDA(cudaMemcpyAsync(d_out, ctx->b.states[0], sizeof(uint32_t) * count,
+                           cudaMemcpyDeviceToDevice, as_stream(stream)));
+  return AMM_OK;
+}
+
+int amm_seed_rng(amm_ctx* ctx, uint64_t seed, int64_t count, void* stream) {
+  if (!ctx || count < ctx->cfg.c || count > ctx->state_len) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  curandGenerator_t gen;
+  if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS)
+    return AMM_ERR_CUDA;
+  curandStatus_t cs = curandSetStream(gen, s);
+  if (cs == CURAND_STATUS_SUCCESS) cs = curandSetPseudoRandomGeneratorSeed(gen, seed + 1234ULL);
+  if (cs == CURAND_STATUS_SUCCESS) cs = curandGenerate(gen, ctx->b.states[0], (size_t)count);
+  curandDestroyGenerator(gen);
+  if (cs != CURAND_STATUS_SUCCESS) {
+    g_last_cuda_error = "curandGenerate failed";
+    return AMM_ERR_CUDA;
+  }
+  AMM_CUDA(cudaMemcpyAsync(ctx->b.states[1], ctx->b.states[0], sizeof(uint32_t) * count,
+                           cudaMemcpyDeviceToDevice, s));
+  return AMM_OK;
+}
+
+int amm_seed_start_vectors(amm_ctx* ctx, uint64_t seed) {
+  if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  if (!ctx->x0_gen &&
+      curandCreateGenerator(&ctx->x0_gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) {
+    ctx->x0_gen = nullptr;
+    g_last_cuda_error = "curandCreateGenerator failed";
+    return AMM_ERR_CUDA;
+  }
+  if (curandSetPseudoRandomGeneratorSeed(ctx->x0_gen, seed) != CURAND_STATUS_SUCCESS) {
+    g_last_cuda_error = "curandSetPseudoRandomGeneratorSeed failed";
+    return AMM_ERR_CUDA;
+  }
+  return AMM_OK;
+}
+
+int amm_draw_start_vector(amm_ctx* ctx, float* d_x0, void* stream) {
+  if (!ctx || !d_x0) return AMM_ERR_INVALID_ARGUMENT;
+  if (!ctx->x0_gen) return AMM_ERR_NOT_READY;
+  if (ctx->cfg.m % 2 != 0) return AMM_ERR_UNSUPPORTED;  // Box-Muller pairs
+  DeviceGuard dg(ctx->device);
+  curandStatus_t cs = curandSetStream(ctx->x0_gen, as_stream(stream));
+  if (cs == CURAND_STATUS_SUCCESS)
+    cs = curandGenerateNormal(ctx->x0_gen, d_x0, (size_t)ctx->cfg.m, 0.0f, 1.0f);
+  if (cs != CURAND_STATUS_SUCCESS) {
+    g_last_cuda_error = "curandGenerateNormal failed";
+    return AMM_ERR_CUDA;
+  }
+  return AMM_OK;
+}
+
+int amm_set_cdf(amm_ctx* ctx, int which, const void* d_cdf, void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (which < 0 || which > 1 || !d_cdf) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  rc = ensure_setup(ctx, s);
+  if (rc) return rc;
+  if (ctx->b.cdf_f32)
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.cdf32[which], d_cdf, sizeof(float) * ctx->cfg.n,
+                             cudaMemcpyDeviceToDevice, s));
+  else
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.cdf64[which], d_cdf, sizeof(double) * ctx->cfg.n,
+                             cudaMemcpyDeviceToDevice, s));
+  AMM_CUDA(amm::launch_build_cdf(ctx->b, which, 1, ctx->sanity_active, s));
+  return AMM_OK;
+}
+
+int amm_set_eigenvector(amm_ctx* ctx, const double* d_vstar, void* stream) {
+  if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  const int had = ctx->b.has_vstar;
+  if (d_vstar) {
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.vstar, d_vstar, sizeof(double) * ctx->cfg.m,
+                             cudaMemcpyDeviceToDevice, as_stream(stream)));
+    ctx->b.has_vstar = 1;
+  } else {
+    ctx->b.has_vstar = 0;
+  }
+  if (had != ctx->b.has_vstar) drop_graphs(ctx);
+  return AMM_OK;
+}
+
+int amm_power_method(amm_ctx* ctx, int method, const float* d_x0, void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!d_x0) return AMM_ERR_INVALID_ARGUMENT;
+  if (method < AMM_METHOD_EXACT || method > AMM_METHOD_PROPOSED_V2) return AMM_ERR_INVALID_ARGUMENT;
+  if (method == AMM_METHOD_PROPOSED_V2 &&
+      (ctx->cfg.vr_period < 1 || ctx->cfg.step < ctx->cfg.vr_period))
+    return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  return run_call(ctx, make_cc(ctx, method), d_x0, 0, as_stream(stream));
+}
+
+int amm_power_exact(amm_ctx* ctx, const float* d_x0, void* stream) {
+  return amm_power_method(ctx, AMM_METHOD_EXACT, d_x0, stream);
+}
+int amm_power_previous(amm_ctx* ctx, const float* d_x0, void* stream) {
+  return amm_power_method(ctx, AMM_METHOD_PREVIOUS, d_x0, stream);
+}
+int amm_power_proposed(amm_ctx* ctx, const float* d_x0, void* stream) {
+  return amm_power_method(ctx, AMM_METHOD_PROPOSED, d_x0, stream);
+}
+int amm_power_proposed_v2(amm_ctx* ctx, const float* d_x0, void* stream) {
+  return amm_power_method(ctx, AMM_METHOD_PROPOSED_V2, d_x0, stream);
+}
+
+int amm_get_trace(amm_ctx* ctx, double* eigs, double* errs, double* coss, int32_t* kinds,
+                  int64_t* distinct, double* t_ns, int64_t* steps_run, void* stream) {
+  if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
+  if (!ctx->has_run) return AMM_ERR_NOT_READY;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  const int step = ctx->last_step;
+  amm::IterState st{};
+  AMM_CUDA(cudaMemcpyAsync(&st, ctx->b.st + (step & 1), sizeof(st), cudaMemcpyDeviceToHost, s));
+  AMM_CUDA(cudaStreamSynchronize(s));
+  const int run = st.steps_run;
+  if (steps_run) *steps_run = run;
+  if (eigs) AMM_CUDA(cudaMemcpy(eigs, ctx->b.eigs, sizeof(double) * run, cudaMemcpyDeviceToHost));
+  if (errs) AMM_CUDA(cudaMemcpy(errs, ctx->b.errs, sizeof(double) * run, cudaMemcpyDeviceToHost));
+  if (coss) AMM_CUDA(cudaMemcpy(coss, ctx->b.coss, sizeof(double) * run, cudaMemcpyDeviceToHost));
+  if (kinds)
+    AMM_CUDA(cudaMemcpy(kinds, ctx->b.kinds, sizeof(int32_t) * run, cudaMemcpyDeviceToHost));
+  if (distinct) {
+    std::vector<int32_t> d(run > 0 ? run : 1);
+    AMM_CUDA(cudaMemcpy(d.data(), ctx->b.distinct_hist, sizeof(int32_t) * run,
+                        cudaMemcpyDeviceToHost));
+    for (int i = 0; i < run; ++i) distinct[i] = d[i];
+  }
+  if (t_ns) {
+    std::vector<unsigned long long> t(run + 1);
+    AMM_CUDA(cudaMemcpy(t.data(), ctx->b.tstamp, sizeof(unsigned long long) * (run + 1),
+                        cudaMemcpyDeviceToHost));
+    for (int i = 0; i < run; ++i) t_ns[i] = (double)(t[i + 1] - t[0]);
+  }
+  return read_status(ctx, s);
+}
+
+int amm_get_vectors(amm_ctx* ctx, float* d_x, float* d_y, void* stream) {
+  if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
+  if (!ctx->has_run) return AMM_ERR_NOT_READY;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  const size_t vb = sizeof(float) * ctx->cfg.m;
+  if (d_x) AMM_CUDA(cudaMemcpyAsync(d_x, ctx->x_final, vb, cudaMemcpyDeviceToDevice, s));
+  if (d_y) AMM_CUDA(cudaMemcpyAsync(d_y, ctx->y_final, vb, cudaMemcpyDeviceToDevice, s));
+  return AMM_OK;
+}
+
+int amm_core_previousAMM(amm_ctx* ctx, const float* d_x, const float* d_x_memo,
+                         const float* d_y_memo, float* d_y, uint32_t* d_idx_out, void* stream) {
+  return single_product(ctx, amm::kMethodPrevious, d_x, d_x_memo, d_y_memo, d_y, d_idx_out,
+                        as_stream(stream));
+}
+
+int amm_core_proposedAMM(amm_ctx* ctx, const float* d_x, const float* d_x_memo,
+                         const float* d_y_memo, float* d_y, uint32_t* d_idx_out, void* stream) {
+  return single_product(ctx, amm::kMethodProposed, d_x, d_x_memo, d_y_memo, d_y, d_idx_out,
+                        as_stream(stream));
+}
+
+int amm_exact_product(amm_ctx* ctx, const float* d_x, float* d_y, void* stream) {
+  return single_product(ctx, amm::kMethodExact, d_x, nullptr, nullptr, d_y, nullptr,
+                        as_stream(stream));
+}
+
+int amm_rayleigh_normalize(amm_ctx* ctx, float* d_x, const float* d_y, double* d_out3,
+                           void* stream) {
+  if (!ctx || !d_x || !d_y || !d_out3) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  AMM_CUDA(amm::launch_rayleigh(d_x, d_x, d_y, ctx->b.has_vstar ? ctx->b.vstar : nullptr,
+                                (int)ctx->cfg.m, d_out3, as_stream(stream)));
+  return AMM_OK;
+}
+
+int amm_normalize(amm_ctx* ctx, float* d_x, void* stream) {
+  if (!ctx || !d_x) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  AMM_CUDA(amm::launch_normalize(d_x, (int)ctx->cfg.m, as_stream(stream)));
+  return AMM_OK;
+}
+
+int amm_get_column_stats(amm_ctx* ctx, float* d_alpha, float* d_norm, float* d_normp,
+                         float* d_z, float* d_v, double* alpha2, void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  rc = ensure_setup(ctx, s);
+  if (rc) return rc;
+  const size_t nb = sizeof(float) * ctx->cfg.n, mb = sizeof(float) * ctx->cfg.m;
+  if (d_alpha) AMM_CUDA(cudaMemcpyAsync(d_alpha, ctx->b.alpha, nb, cudaMemcpyDeviceToDevice, s));
+  if (d_norm) AMM_CUDA(cudaMemcpyAsync(d_norm, ctx->b.norm, nb, cudaMemcpyDeviceToDevice, s));
+  if (d_normp) AMM_CUDA(cudaMemcpyAsync(d_normp, ctx->b.normp, nb, cudaMemcpyDeviceToDevice, s));
+  if (d_z) AMM_CUDA(cudaMemcpyAsync(d_z, ctx->b.z, mb, cudaMemcpyDeviceToDevice, s));
+  if (d_v) AMM_CUDA(cudaMemcpyAsync(d_v, ctx->b.v, mb, cudaMemcpyDeviceToDevice, s));
+  if (alpha2) {
+    AMM_CUDA(cudaMemcpyAsync(alpha2, ctx->b.alpha2, sizeof(double), cudaMemcpyDeviceToHost, s));
+    AMM_CUDA(cudaStreamSynchronize(s));
+  }
+  return AMM_OK;
+}
+
+int amm_get_sampling_tables(amm_ctx* ctx, int which, void* d_cdf, float* d_weights,
+                            void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (which < 0 || which > 1) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  rc = ensure_setup(ctx, s);
+  if (rc) return rc;
+  const int64_t n = ctx->cfg.n;
+  if (d_cdf) {
+    if (ctx->b.cdf_f32)
+      AMM_CUDA(cudaMemcpyAsync(d_cdf, ctx->b.cdf32[which], sizeof(float) * n,
+                               cudaMemcpyDeviceToDevice, s));
+    else
+      AMM_CUDA(cudaMemcpyAsync(d_cdf, ctx->b.cdf64[which], sizeof(double) * n,
+                               cudaMemcpyDeviceToDevice, s));
+  }
+  if (d_weights)
+    AMM_CUDA(cudaMemcpyAsync(d_weights, ctx->b.wts[which], sizeof(float) * n,
+                             cudaMemcpyDeviceToDevice, s));
+  return AMM_OK;
+}
+
+int amm_sample_indices(amm_ctx* ctx, int which, uint32_t* d_idx, void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (which < 0 || which > 1 || !d_idx) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  rc = ensure_setup(ctx, as_stream(stream));
+  if (rc) return rc;
+  AMM_CUDA(amm::launch_sample_only(ctx->b, which, d_idx, as_stream(stream)));
+  return AMM_OK;
+}
+
+int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch,
+                          int64_t* distinct, void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (reps < 1 || !ms_per_launch) return AMM_ERR_INVALID_ARGUMENT;
+  int method;
+  if (kind == AMM_STEP_EXACT || kind == AMM_STEP_EXACT_MEMO)
+    method = amm::kMethodExact;
+  else if (kind == AMM_STEP_PREVIOUS)
+    method = amm::kMethodPrevious;
+  else if (kind == AMM_STEP_PROPOSED)
+    method = amm::kMethodProposed;
+  else
+    return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  if (method != amm::kMethodExact) {
+    rc = ensure_setup(ctx, s);
+    if (rc) return rc;
+  }
+  if (!ctx->has_run) {
+    std::vector<float> ones(ctx->cfg.m, 1.0f);
+    AMM_CUDA(cudaMemcpyAsync(ctx->x0_buf, ones.data(), sizeof(float) * ones.size(),
+                             cudaMemcpyHostToDevice, s));
+    AMM_CUDA(cudaStreamSynchronize(s));
+  }
+  CallCfg cc = make_cc(ctx, method);
+  cc.vr_period = 0;
+  cc.vr_thr = 0.0;
+  cc.variance_reduction = 0;
+  cc.tol = 0.0;
+  cc.step = 1;
+  AMM_CUDA(amm::launch_init(ctx->b, cc, ctx->x0_buf, 0, s));
+  cudaEvent_t e0, e1;
+  AMM_CUDA(cudaEventCreate(&e0));
+  AMM_CUDA(cudaEventCreate(&e1));
+  AMM_CUDA(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) AMM_CUDA(amm::launch_iter_panel(ctx->b, ctx->geom, cc, 0, s));
+  AMM_CUDA(cudaEventRecord(e1, s));
+  // drop the picks (finalize with step 0 reads st[0]: pending picks in count[0], states[0] kept)
+  CallCfg fc = cc;
+  fc.step = 0;
+  AMM_CUDA(amm::launch_finalize(ctx->b, fc, nullptr, nullptr, s));
+  AMM_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  AMM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_per_launch = ms / (float)reps;
+  if (distinct) {
+    int32_t d = (int32_t)ctx->cfg.n;
+    if (method != amm::kMethodExact && !ctx->sanity_active)
+      AMM_CUDA(cudaMemcpy(&d, ctx->b.distinct_hist, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    *distinct = d;
+  }
+  AMM_CUDA(cudaStreamSynchronize(s));
+  return read_status(ctx, s);
+}
+
+int amm_grad_lambda(amm_ctx* ctx, const float* d_v, float* d_grad, int64_t ld_grad, void* stream) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!d_v || !d_grad || ld_grad < ctx->cfg.m) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  AMM_CUDA(amm::launch_grad(ctx->b, d_v, d_grad, ld_grad, as_stream(stream)));
+  return AMM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// Internal declarations shared by the kernels (amm_kernels.cu) and the host side (amm_api.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace amm {
+
+// Step kinds, identical to enum amm_step_kind in include/amm.h.
+enum StepKind : int32_t { kExactMemo = 0, kExact = 1, kPrevious = 2, kProposed = 3 };
+enum Method : int32_t { kMethodExact = 0, kMethodPrevious = 1, kMethodProposed = 2, kMethodProposedV2 = 3 };
+
+// Device status bits (ORed into Buffers::status).
+enum DevStatus : uint32_t { kDevTimeout = 1u, kDevNonFinite = 2u };
+
+constexpr int kMaxThreads = 512;   // panel kernel block size limit
+constexpr int kGcMax = 8;          // columns per pipeline stage, upper bound
+constexpr int kSeg = 32;           // fine-search window of the sampler (elements)
+constexpr int kCoarseMax = 2048;   // coarse CDF table entries held in shared memory
+
+// Iteration state, double-buffered by iteration parity: kernels of iteration i read
+// st[i & 1]; the last CTA of the reduce kernel of iteration i writes st[(i + 1) & 1].
+struct IterState {
+  int32_t mode;        // StepKind of this iteration
+  int32_t last_exact;  // proposed AMM: index of the last VR step
+  int32_t done;        // early stop reached: later kernels of the call do nothing
+  int32_t sb;          // pending picks were drawn from states[sb]; advanced copy in states[sb^1]
+  int32_t pb;          // pending picks live in count[pb] / chunk[pb] / samples[pb]
+  int32_t steps_run;   // completed steps
+  int32_t distinct;    // distinct columns of the last AMM product (written by the panel kernel)
+  int32_t pad;
+  float scale;         // x_i = scale * y_{i-1} (FP32 multiply)
+  float pad2;
+  double cos_prev;     // cos of the previous step (adaptive VR)
+  double lam_prev;     // λ of the previous step (tolerance stop)
+  double sum_dx;       // Σ(x_i − x_memo)    (proposed)
+  double zdx;          // z·(x_i − x_memo)   (proposed)
+};
+
+// Static description of one power-method call, passed by value to the kernels.
+struct CallCfg {
+  int32_t method;
+  int32_t vr_period;
+  double vr_thr;
+  double tol;
+  int32_t variance_reduction;
+  int32_t sanity;      // sanity mode active (sanity && c == n)
+  int32_t uses_amm;    // the call draws samples at all
+  int32_t step;
+};
+
+// Every device buffer of a context.
+struct Buffers {
+  // matrix
+  const void* A;
+  int64_t ld;
+  int32_t m, n, c;
+  int32_t dtype;       // 0 FP32, 1 BF16
+  int32_t cdf_f32;     // 1: FP32 CDF and target
+  int32_t nsm;         // panel-kernel CTAs (= partial sums)
+  // per-column statistics (n)
+  float* alpha;
+  float* norm;
+  float* normp;
+  // sampling tables per weighting (0 = norm, 1 = normp)
+  double* cdf64[2];
+  float* cdf32[2];
+  float* wts[2];
+  double* coarse64[2];
+  float* coarse32[2];
+  int32_t seg;         // elements per coarse segment (power of two >= kSeg)
+  int32_t ncoarse;     // full segments = n / seg
+  int32_t chunk_shift; // log2 of the distinct-count chunk
+  int32_t nchunks;
+  // vectors (m)
+  float* z;
+  float* v;
+  float* y[2];         // y[i & 1] = y_i; y[1] holds the raw start vector for i = 0
+  float* x_memo;
+  float* y_memo;
+  double* vstar;       // may be null
+  int32_t has_vstar;
+  // sampling
+  uint32_t* states[2];   // xorshift states (c used)
+  uint32_t* count[2];    // per-column multiplicity of the pending picks (n)
+  uint32_t* chunk[2];    // distinct columns per chunk (nchunks)
+  uint32_t* samples[2];  // raw picks in draw order (c)
+  uint32_t* distinct_idx;   // sorted distinct indices of the last AMM product (c)
+  uint32_t* distinct_mult;  // their multiplicities (c)
+  // partial sums
+  float* partials;     // nsm x m
+  float* spart;        // nsm  (Σ α_k t_k of each CTA, proposed)
+  double* spart64;     // nsm  (Σ α_j² of each CTA, set-up)
+  double* rpart;       // reduce CTAs x 4 (x·y, y·y, y·v*, spare)
+  uint32_t* ticket;    // last-CTA counters [0]: reduce, [1]: small kernels
+  double* alpha2;      // ‖α‖²
+  float* colvec;       // n floats of scratch (vᵀA for the gradient)
+  // iteration state and traces
+  IterState* st;       // [2]
+  double* eigs;
+  double* errs;
+  double* coss;
+  int32_t* kinds;
+  int32_t* distinct_hist;
+  unsigned long long* tstamp;  // step+1 entries: [0] start, [i+1] end of step i
+  uint32_t* status;
+};
+
+// Launch geometry of the panel kernel for a given (m, dtype).
+struct PanelGeom {
+  int threads;      // block size
+  int slots;        // vector slots per thread (R)
+  int elems;        // elements per 16-byte vector (E)
+  int colbytes;     // m * elem_size
+  int gc;           // columns per stage
+  int nstages;
+  int stage_bytes;  // gc * colbytes
+  int smem_bytes;   // dynamic shared memory
+  int wl_cap;       // work-list capacity per CTA
+};
+
+bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g);
+
+// ---- launchers (amm_kernels.cu); each returns the cudaError_t of the launch ----
+// Set-up pass over A: column statistics and per-CTA partial sums of z = A·α.
+cudaError_t launch_setup_panel(const Buffers& b, const PanelGeom& g, cudaStream_t s);
+// Reduce the set-up partials into z and v = z − ‖α‖².
+cudaError_t launch_setup_reduce(const Buffers& b, cudaStream_t s);
+// Build the CDFs, weights and coarse tables of both weightings (or one if which >= 0,
+// keeping an imported CDF when keep_cdf is set).
+cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sanity, cudaStream_t s);
+// Start of a call: x0 into y[1], scale, initial state, first picks.
+// no_normalize: use x0 as x_0 unscaled (single-product entry points).
+cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, int no_normalize,
+                        cudaStream_t s);
+// One iteration: panel product and reduce/Rayleigh/next-picks.
+cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
+                              cudaStream_t s);
+cudaError_t launch_iter_reduce(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
+// x_final = scale * y_last into dst (length m); y_last into ydst (optional); commits the
+// sampling states to states[0] and clears any pending picks.
+cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, float* ydst,
+                            cudaStream_t s);
+// Standalone helpers.
+cudaError_t launch_normalize(float* x, int m, cudaStream_t s);
+cudaError_t launch_rayleigh(const float* x_in, float* x_out, const float* y, const double* vstar,
+                            int m, double* out3, cudaStream_t s);
+cudaError_t launch_sample_only(const Buffers& b, int which, uint32_t* idx, cudaStream_t s);
+cudaError_t launch_expand_sorted(const Buffers& b, const int32_t* d_cd, uint32_t* out,
+                                 cudaStream_t s);
+cudaError_t launch_grad(const Buffers& b, const float* v, float* grad, int64_t ldg,
+                        cudaStream_t s);
+
+// Count of this library's launches (for the bench's gpu_launches field).
+void count_launch(int k = 1);
+int64_t launch_count();
+
+}  // namespace amm

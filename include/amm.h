@@ -1,0 +1,208 @@
+/*
+ * amm.h — C ABI of libamm: the power method for λ_max of C = A·Aᵀ on one B200 (sm_100a),
+ * exact and by approximate matrix multiplication (AMM).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns an int status
+ * (AMM_OK = 0).  Device pointers are CUDA device addresses on the context's device; stream is
+ * a cudaStream_t passed as void* (NULL = the legacy default stream).  All work is
+ * stream-ordered on that stream.  Calls on one context are not thread-safe; distinct contexts
+ * are independent.  The caller owns A, x0 and every output buffer; the context owns its
+ * scratch (column statistics, CDFs, sampling states, per-CTA partial sums, traces).
+ *
+ * Matrix layout: A is m x n, column-major, leading dimension ld (elements), FP32 or BF16.
+ * Column j is the contiguous run A + j*ld.  For the single-pass TMA kernels the columns must
+ * start on 16-byte boundaries (ld*elem_size % 16 == 0, A 16-byte aligned) and m*elem_size
+ * must be a multiple of 16; m <= 16384.
+ *
+ * The reference (Takuya-Okuyama/eigenvalueComputation_by_AMM) keeps everything in one
+ * translation unit of C++ headers with no C interface; each function below names the
+ * reference function it replaces (file:line in that repository).
+ */
+#ifndef AMM_H_
+#define AMM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+enum amm_status {
+  AMM_OK = 0,
+  AMM_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, c < 1, unknown method ...      */
+  AMM_ERR_ALIGNMENT = 2,        /* A or ld not 16-byte aligned, m*elem_size % 16 != 0      */
+  AMM_ERR_UNSUPPORTED = 3,      /* shape outside the kernels' range (m > 16384)            */
+  AMM_ERR_NOT_READY = 4,        /* amm_set_matrix has not been called                      */
+  AMM_ERR_DEGENERATE = 5,       /* sampling CDF total is 0 or not finite (all-zero A, NaN) */
+  AMM_ERR_CUDA = 6,             /* a CUDA runtime call failed (see amm_last_cuda_error)   */
+  AMM_ERR_DEVICE_TIMEOUT = 7,   /* a bounded device-side wait gave up                      */
+  AMM_ERR_OUT_OF_MEMORY = 8,
+  AMM_ERR_NO_DEVICE = 9
+};
+
+enum amm_dtype { AMM_F32 = 0, AMM_BF16 = 1 };
+
+/* Sampling CDF precision.  AMM_CDF_F64 (default): FP64 prefix sum and FP64 target.
+ * AMM_CDF_F32: FP32 CDF and FP32 target exactly as the reference's pick_index
+ * (device_memory.h:516-545); the CDF array is the correctly rounded prefix sum unless the
+ * caller imports one with amm_set_cdf (e.g. the reference's own CUB-built d_acc_weight). */
+enum amm_cdf_precision { AMM_CDF_F64 = 0, AMM_CDF_F32 = 1 };
+
+/* Power-method variants (the reference's -kernel names, host_memory.h:87-89,132-141). */
+enum amm_method {
+  AMM_METHOD_EXACT = 0,       /* powerMethod_by_exact       (powerMethod_by_exact.cuh:4-100)      */
+  AMM_METHOD_PREVIOUS = 1,    /* powerMethod_by_previous    (powerMethod_by_previous.cuh:100-210) */
+  AMM_METHOD_PROPOSED = 2,    /* powerMethod_by_proposed    (powerMethod_by_proposed.cuh:317-447) */
+  AMM_METHOD_PROPOSED_V2 = 3  /* powerMethod_by_proposed_v2 (powerMethod_by_proposed_v2.cuh:199-377) */
+};
+
+/* Per-step kinds recorded in the trace. */
+enum amm_step_kind {
+  AMM_STEP_EXACT_MEMO = 0,   /* exact C·x, then [x_memo|y_memo] <- [x|y] (a VR step)      */
+  AMM_STEP_EXACT = 1,        /* exact C·x, memo untouched                                  */
+  AMM_STEP_PREVIOUS = 2,     /* previous AMM (norm-proportional sampling)                  */
+  AMM_STEP_PROPOSED = 3      /* proposed AMM (centred sampling + rank-one correction)      */
+};
+
+/* Parameters (the reference's host_memory fields, host_memory.h:26-50, plus n, ld, dtype). */
+typedef struct amm_config {
+  int64_t m;                     /* rows of A = size of C                                   */
+  int64_t n;                     /* columns of A                                            */
+  int64_t c;                     /* samples per AMM product (-c); 0 means n                 */
+  int64_t step;                  /* iterations per power-method call (-step)                */
+  int64_t vr_period;             /* periodic variance reduction (-vr); 0 = off              */
+  double vr_adaptive_threshold;  /* adaptive VR when cos > 1 - threshold (-vr_adaptive)    */
+  double tol;                    /* stop once |λ_i − λ_{i−1}| <= tol·|λ_i|; 0 = run all     */
+  int32_t dtype;                 /* enum amm_dtype                                          */
+  int32_t cdf_precision;         /* enum amm_cdf_precision                                  */
+  int32_t sanity;                /* -sanity: with c == n, weights 1 and indices 0..n-1      */
+  int32_t use_graph;             /* capture the iteration loop in a CUDA graph (default 1) */
+} amm_config;
+
+typedef struct amm_ctx amm_ctx;
+
+/* Fill cfg with the reference's defaults (host_memory.h:26-50): step 10, no VR, FP32. */
+void amm_config_default(amm_config *cfg);
+
+/* Create a context on CUDA device `device` (replaces the device_memory constructor,
+ * device_memory.h:172-276).  Allocates all scratch for the configured sizes. */
+int amm_create(amm_ctx **out, const amm_config *cfg, int device);
+/* Release a context (device_memory destructor, device_memory.h:278-314). */
+int amm_destroy(amm_ctx *ctx);
+
+/* Bind A (borrowed device pointer; it must outlive its use).  The one-pass set-up over A
+ * runs on the stream of the first call that needs it (an AMM call or a statistics accessor;
+ * exact calls never do): per-column mean α_j, ‖A_j‖, ‖A_j − α_j‖ in FP64 (get_norms,
+ * device_memory.h:34-59), ‖α‖² (device_memory.h:335-336), z = A·α and v = z − ‖α‖²
+ * (powerMethod_by_proposed.cuh:132-145), both sampling CDFs and the inverse-probability
+ * weights (set_weights / InclusiveSum / update_weights, powerMethod_by_previous.cuh:9-44). */
+int amm_set_matrix(amm_ctx *ctx, const void *dA, int64_t ld, void *stream);
+
+/* xorshift32 sampling states (the reference's d_rnd).  count >= c. */
+int amm_set_rng_state(amm_ctx *ctx, const uint32_t *d_states, int64_t count, void *stream);
+int amm_get_rng_state(amm_ctx *ctx, uint32_t *d_states_out, int64_t count, void *stream);
+/* States as the reference derives them from -seed: curandGenerate with the default
+ * (XORWOW) generator seeded with seed + 1234 (set_internal_randomness,
+ * device_memory.h:339-343); count values are generated (the reference uses m). */
+int amm_seed_rng(amm_ctx *ctx, uint64_t seed, int64_t count, void *stream);
+
+/* Start vectors as the reference draws them: a context-owned default (XORWOW) cuRAND
+ * generator re-seeded with `seed` (the reference seeds with 1234 + -seed, AMM.cu:85), and
+ * one curandGenerateNormal(m, mean 0, sd 1) per call, continuing the sequence
+ * (powerMethod_by_exact.cuh:32 and the same line in every driver). */
+int amm_seed_start_vectors(amm_ctx *ctx, uint64_t seed);
+int amm_draw_start_vector(amm_ctx *ctx, float *d_x0, void *stream);
+
+/* Replace the sampling CDF of one weighting (0 = ‖A_j‖², previous AMM; 1 = ‖A_j − α_j‖²,
+ * proposed AMM) with a caller-supplied inclusive prefix sum of length n (FP32 when the
+ * context uses AMM_CDF_F32, FP64 otherwise).  The weights w_j = total/(weight_j·c) are
+ * rebuilt from it.  Used to feed the reference's own CUB-built CDF for bit-exact sampling. */
+int amm_set_cdf(amm_ctx *ctx, int which, const void *d_cdf, void *stream);
+
+/* Exact top eigenvector v* (FP64, length m) for the error column; NULL clears it
+ * (the reference reads data/exact_eigenvector, device_memory.h:246-254). */
+int amm_set_eigenvector(amm_ctx *ctx, const double *d_vstar, void *stream);
+
+/* Run one power-method call of `method` from the raw start vector d_x0 (length m; it is
+ * normalised first, common.h:156-183), cfg->step iterations (fewer if tol stops it).
+ * Replaces powerMethod_by_exact / _previous / _proposed / _proposed_v2.  Asynchronous;
+ * read the results with amm_get_trace / amm_get_vectors. */
+int amm_power_method(amm_ctx *ctx, int method, const float *d_x0, void *stream);
+int amm_power_exact(amm_ctx *ctx, const float *d_x0, void *stream);        /* powerMethod_by_exact.cuh:4-100 */
+int amm_power_previous(amm_ctx *ctx, const float *d_x0, void *stream);     /* powerMethod_by_previous.cuh:100-210 */
+int amm_power_proposed(amm_ctx *ctx, const float *d_x0, void *stream);     /* powerMethod_by_proposed.cuh:317-447 */
+int amm_power_proposed_v2(amm_ctx *ctx, const float *d_x0, void *stream);  /* powerMethod_by_proposed_v2.cuh:199-377 */
+
+/* Synchronise `stream` and copy the trace of the last call to HOST arrays of length
+ * >= cfg->step (any may be NULL): λ_i = x_i·y_i, err_i = (y_i·v*)/‖y_i‖, cos_i = λ_i/‖y_i‖,
+ * the step kind, the number of distinct columns read, and device timestamps in ns relative
+ * to the start of the call.  *steps_run receives the number of completed steps. */
+int amm_get_trace(amm_ctx *ctx, double *eigs, double *errs, double *coss, int32_t *kinds,
+                  int64_t *distinct, double *t_ns, int64_t *steps_run, void *stream);
+
+/* Copy the final iterate x (normalised) and the last product y into device buffers of
+ * length m (either may be NULL). */
+int amm_get_vectors(amm_ctx *ctx, float *d_x, float *d_y, void *stream);
+
+/* One sampled product, the reference's square_of_A_by_previous / previousAMM_kernel1+2
+ * (powerMethod_by_previous.cuh:7-98, core_previousAMM.cuh:4-263):
+ *   y = y_memo + Σ_k w_{s_k}·A_{s_k}·(A_{s_k}ᵀ(x − x_memo)),
+ * drawing c indices from the current states (which advance).  d_idx_out (optional,
+ * length c) receives the sorted sampled indices. */
+int amm_core_previousAMM(amm_ctx *ctx, const float *d_x, const float *d_x_memo,
+                         const float *d_y_memo, float *d_y, uint32_t *d_idx_out, void *stream);
+/* The proposed product (powerMethod_by_proposed.cuh:7-103, core_proposedAMM.cuh:17-313):
+ *   y = y_memo + Σdx·v + (z·dx)·1 + Σ_k w_{s_k}·(A_{s_k} − α_{s_k})·((A_{s_k} − α_{s_k})ᵀdx). */
+int amm_core_proposedAMM(amm_ctx *ctx, const float *d_x, const float *d_x_memo,
+                         const float *d_y_memo, float *d_y, uint32_t *d_idx_out, void *stream);
+/* Exact product y = A·(Aᵀ·x) (the two cublasSgemv of powerMethod_by_exact.cuh:37-53). */
+int amm_exact_product(amm_ctx *ctx, const float *d_x, float *d_y, void *stream);
+
+/* Rayleigh step on [x | y] (dotProduct_and_generate_x, common.h:89-154): writes
+ * out3 = {x·y, (y·v*)/‖y‖, (x·y)/‖y‖} (device, FP64) and x <- y/‖y‖. */
+int amm_rayleigh_normalize(amm_ctx *ctx, float *d_x, const float *d_y, double *d_out3,
+                           void *stream);
+/* x <- x/‖x‖ (normalize, common.h:156-183). */
+int amm_normalize(amm_ctx *ctx, float *d_x, void *stream);
+
+/* Per-column statistics from the set-up pass (device buffers of length n; any may be NULL),
+ * z and v (length m), ‖α‖² (host). */
+int amm_get_column_stats(amm_ctx *ctx, float *d_alpha, float *d_norm, float *d_normp,
+                         float *d_z, float *d_v, double *alpha2, void *stream);
+/* The CDF (length n, FP32 or FP64 per the context) and weights (FP32, length n) of one
+ * weighting (0 = previous, 1 = proposed). */
+int amm_get_sampling_tables(amm_ctx *ctx, int which, void *d_cdf, float *d_weights,
+                            void *stream);
+/* Draw c indices from the current states with weighting `which` without advancing them
+ * (pick_index, device_memory.h:516-545) into d_idx (length c, in draw order). */
+int amm_sample_indices(amm_ctx *ctx, int which, uint32_t *d_idx, void *stream);
+
+/* Measurement hook: time `reps` back-to-back launches of the fused product kernel for one
+ * step kind (AMM_STEP_EXACT, AMM_STEP_PREVIOUS or AMM_STEP_PROPOSED) on the bound matrix,
+ * with CUDA events on `stream`, from the start vector of the last call (ones before any
+ * call).  AMM kinds draw one set of picks from the current states without advancing them.
+ * *ms_per_launch receives the mean time per launch and *distinct the distinct columns read
+ * per launch (n for an exact launch).  Synchronises `stream`.  No counterpart in the
+ * reference (its per-step timing is cudaEventElapsedTime around whole steps,
+ * powerMethod_by_exact.cuh:60-64). */
+int amm_benchmark_product(amm_ctx *ctx, int kind, int reps, float *ms_per_launch,
+                          int64_t *distinct, void *stream);
+
+/* ∂λ_max/∂A = 2·v·(vᵀA) for a unit vector v (length m), written to d_grad (m x n,
+ * column-major, leading dimension ld_grad, FP32).  No counterpart in the reference. */
+int amm_grad_lambda(amm_ctx *ctx, const float *d_v, float *d_grad, int64_t ld_grad,
+                    void *stream);
+
+/* Human-readable name of a status code; the last CUDA error string of this thread. */
+const char *amm_status_string(int status);
+const char *amm_last_cuda_error(void);
+/* Number of this library's kernel launches so far in this process (all contexts). */
+int64_t amm_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMM_H_ */

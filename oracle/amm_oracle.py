@@ -1,0 +1,449 @@
+"""CPU oracle for the power method on C = A·Aᵀ: exact, previous AMM, proposed AMM, proposed AMM v2.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker that the CUDA library is compared
+against; it is imported by ``tests/``, by ``__graft_entry__.smoke()`` and by the CPU-baseline
+leg of ``bench.py``, and by nothing in the product path.  It restates, in numpy, the algorithm
+of Takuya-Okuyama/eigenvalueComputation_by_AMM; every function cites the reference file:line
+it follows.
+
+Conventions
+-----------
+* ``A`` is an (m, n) numpy array.  Column j is ``A[:, j]`` (the reference stores A column-major
+  with lda = m, so "column j" is the contiguous run ``dA + m*j``).  The reference only handles
+  square m x m matrices; here n may differ from m, and every per-column quantity has length n
+  while x, y, z, v have length m.
+* Arithmetic the reference does in FP32 and stores in FP32 is rounded to FP32 here at the same
+  points; sums the reference accumulates in FP32 with a GPU-specific order (cuBLAS, CUB,
+  BlockReduce, atomics) are accumulated in FP64 here and rounded once.  So FP32 results agree
+  with the reference to FP32 rounding, and integer results (xorshift states, sampled indices)
+  agree bit for bit.
+* Two CDF precisions exist.  ``"f32"`` reproduces the reference's ``pick_index`` exactly for a
+  given FP32 CDF array (the reference builds that array with ``cub::DeviceScan::InclusiveSum``,
+  whose association order is CUB's; ``cdf_f32`` below is the correctly rounded prefix, which is
+  what the CUDA library builds in compat mode).  ``"f64"`` is the production mode: an FP64 CDF
+  and an FP64 target.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Optional
+
+import numpy as np
+
+F32 = np.float32
+F64 = np.float64
+U32 = np.uint32
+
+__all__ = [
+    "get_norms", "alpha_squared", "set_weights", "cdf_f32", "cdf_f64", "update_weights",
+    "xorshift32", "pick_index", "sample_sorted", "previous_amm", "proposed_amm", "dots",
+    "exact_product", "dot_product_and_generate_x", "normalize", "generate_zv",
+    "PowerTrace", "power_method", "reported_eigenvalue", "grad_lambda", "lambda_max_f64",
+]
+
+
+# --------------------------------------------------------------------------------------------
+# Column statistics and sampling probabilities
+# --------------------------------------------------------------------------------------------
+
+def get_norms(A: np.ndarray):
+    """Per-column mean, norm and centred norm (device_memory.h:34-59, ``get_norms``).
+
+    The reference accumulates ``sum`` and ``sum_pow2`` in FP64 over the m rows of column j and
+    writes ``alpha = (float)(sum/m)``, ``normA = (float)sqrt(sum_pow2)`` and
+    ``normAprime = (float)sqrt(sum_pow2 - mean*mean*m)``.  The last expression can go slightly
+    negative through cancellation for a constant column (the reference then stores NaN); it is
+    clamped at 0 here and in the CUDA library.
+    """
+    A64 = np.asarray(A, dtype=F64)
+    m = A64.shape[0]
+    s = A64.sum(axis=0)
+    q = np.einsum("ij,ij->j", A64, A64)
+    mean = s / F64(m)
+    alpha = mean.astype(F32)
+    norm = np.sqrt(q).astype(F32)
+    normp = np.sqrt(np.maximum(q - mean * mean * F64(m), 0.0)).astype(F32)
+    return alpha, norm, normp
+
+
+def alpha_squared(alpha: np.ndarray) -> float:
+    """‖α‖² (device_memory.h:335-336: ``cublasSnrm2`` of α, squared).  Accumulated in FP64."""
+    a = np.asarray(alpha, dtype=F64)
+    return float(np.dot(a, a))
+
+
+def set_weights(norm: np.ndarray) -> np.ndarray:
+    """weight_j = norm_j² in FP32 (common.h:34-40, ``set_weights``)."""
+    norm = np.asarray(norm, dtype=F32)
+    return (norm * norm).astype(F32)
+
+
+def cdf_f64(weight: np.ndarray) -> np.ndarray:
+    """Unnormalised inclusive prefix sum of the weights, in FP64 (production CDF; it replaces
+    the FP32 ``cub::DeviceScan::InclusiveSum`` at powerMethod_by_previous.cuh:26-32)."""
+    return np.cumsum(np.asarray(weight, dtype=F64), dtype=F64)
+
+
+def cdf_f32(weight: np.ndarray) -> np.ndarray:
+    """FP32 CDF used by compat mode: the correctly rounded prefix sum of the FP32 weights.
+
+    The reference's FP32 CDF (powerMethod_by_previous.cuh:26-32) comes from CUB's scan, whose
+    rounding depends on CUB's tile order; any FP32 scan is within a few ulps of this one.
+    """
+    return cdf_f64(weight).astype(F32)
+
+
+def update_weights(weight: np.ndarray, total: float, c: int, precision: str = "f64") -> np.ndarray:
+    """Inverse-probability scale w_j = total / (weight_j · c) = 1/(c·p_j) (common.h:42-53).
+
+    ``precision="f32"`` divides in FP32 like the reference (which, compiled with
+    ``--use_fast_math``, uses an approximate division: within 2 ulp of this); ``"f64"``
+    divides in FP64 and rounds once (what the CUDA library stores).
+    """
+    if precision == "f32":
+        w = np.asarray(weight, dtype=F32)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return (F32(total) / (w * F32(c))).astype(F32)
+    w = np.asarray(weight, dtype=F64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return (F64(total) / (w * F64(c))).astype(F32)
+
+
+# --------------------------------------------------------------------------------------------
+# Random draws and inverse-CDF sampling (integer work: bit exact)
+# --------------------------------------------------------------------------------------------
+
+def xorshift32(states: np.ndarray):
+    """One xorshift32 step per state and the derived uniform (device_memory.h:506-514).
+
+    y ^= y << 13; y ^= y >> 17; y ^= y << 5 (uint32 wrap-around).  The uniform is the float
+    with exponent 0 and the low 23 bits of y as mantissa, minus 1: exact, in [0, 1).
+    Returns (new_states, u) with u float32.
+    """
+    y = np.array(states, dtype=U32, copy=True)
+    y ^= (y << U32(13))
+    y ^= (y >> U32(17))
+    y ^= (y << U32(5))
+    bits = (y & U32(0x007FFFFF)) | U32(0x3F800000)
+    u = bits.view(F32) - F32(1.0)
+    return y, u.astype(F32)
+
+
+def pick_index(cdf: np.ndarray, states: np.ndarray, c: int):
+    """Inverse-CDF sampling of c column indices (device_memory.h:516-545, ``pick_index``).
+
+    Sample k advances ``states[k]`` once and searches for the first index i in [0, n-1] with
+    ``cdf[i] > target``, where target = cdf[n-1] · u_k; if there is none it returns n-1 (the
+    upper bound the reference's bisection starts from).  For a non-decreasing CDF every correct
+    bisection returns this same index, so the search order does not matter.
+
+    With an FP32 CDF the target is the FP32 product (as in the reference); with an FP64 CDF it
+    is the FP64 product of the FP64 total and the (exact) uniform.
+    Returns (indices uint32[c], new_states); states beyond the first c are not touched.
+    """
+    cdf = np.asarray(cdf)
+    states = np.asarray(states, dtype=U32)
+    n = cdf.shape[0]
+    new_states = states.copy()
+    s, u = xorshift32(states[:c])
+    new_states[:c] = s
+    if cdf.dtype == F32:
+        target = (F32(cdf[n - 1]) * u).astype(F32)
+    else:
+        target = F64(cdf[n - 1]) * u.astype(F64)
+    idx = np.searchsorted(cdf, target, side="right")
+    idx = np.minimum(idx, n - 1).astype(U32)
+    return idx, new_states
+
+
+def sample_sorted(cdf: np.ndarray, states: np.ndarray, c: int):
+    """``pick_index`` followed by the ascending sort the reference does with
+    ``cub::DeviceRadixSort::SortKeys`` (powerMethod_by_previous.cuh:56-70)."""
+    idx, new_states = pick_index(cdf, states, c)
+    return np.sort(idx), new_states
+
+
+# --------------------------------------------------------------------------------------------
+# Products
+# --------------------------------------------------------------------------------------------
+
+def exact_product(A: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """y = A·(Aᵀ·x), FP64 accumulation, FP32 result.
+
+    The reference computes ``tmp = A·x; y = A·tmp`` with two ``cublasSgemv(OP_N)`` calls
+    (powerMethod_by_exact.cuh:31-53); for its symmetric A that is A·Aᵀ·x.  For a rectangular
+    A the meaning kept here is C·x with C = A·Aᵀ.
+    """
+    A64 = np.asarray(A, dtype=F64)
+    t = A64.T @ np.asarray(x, dtype=F64)
+    return (A64 @ t).astype(F32)
+
+
+def previous_amm(A, x, x_memo, y_memo, idx_sorted, w):
+    """One previous-AMM product (core_previousAMM.cuh:4-263 with the launch at
+    powerMethod_by_previous.cuh:73-96).
+
+    kernel1: tmp_k = w[s_k] · (A_{s_k}ᵀ (x − x_memo))            (:163-168)
+             y ← y_memo                                              (:170-174)
+    kernel2: y += Σ_k A_{s_k} · tmp_k                                 (:203-262)
+    Returns (tmp float32[c], y float32[m]).
+    """
+    A = np.asarray(A)
+    dx = np.asarray(x, dtype=F32) - np.asarray(x_memo, dtype=F32)     # FP32 subtraction
+    cols = A[:, idx_sorted].astype(F64)
+    d = cols.T @ dx.astype(F64)
+    tmp = (d.astype(F32) * np.asarray(w, dtype=F32)[idx_sorted]).astype(F32)
+    y = np.asarray(y_memo, dtype=F64) + cols @ tmp.astype(F64)
+    return tmp, y.astype(F32)
+
+
+def dots(x, x_memo, z):
+    """(Σ dx, z·dx) in FP64 with dx = x − x_memo in FP32 (common.h:55-87, ``dots``)."""
+    dx = (np.asarray(x, dtype=F32) - np.asarray(x_memo, dtype=F32)).astype(F64)
+    return float(dx.sum()), float(np.dot(dx, np.asarray(z, dtype=F64)))
+
+
+def generate_zv(A, alpha, alpha2):
+    """z = A·α and v = z − ‖α‖² (powerMethod_by_proposed.cuh:132-145 and
+    core_proposedAMM.cuh:4-15).  FP64 accumulation, FP32 storage."""
+    z = (np.asarray(A, dtype=F64) @ np.asarray(alpha, dtype=F64)).astype(F32)
+    v = (z.astype(F64) - F64(alpha2)).astype(F32)
+    return z, v
+
+
+def proposed_amm(A, alpha, x, x_memo, y_memo, idx_sorted, w, z, v):
+    """One proposed-AMM product (core_proposedAMM.cuh:17-313, launched at
+    powerMethod_by_proposed.cuh:258-313).
+
+    dots:    Σdx and z·dx                                            (common.h:55-87)
+    kernel1: tmp_k = (A_{s_k}ᵀ dx − α_{s_k}·Σdx) · w[s_k]              (:191-196)
+             y ← y_memo + Σdx·v + z·dx   (FP64, rounded to FP32)      (:198-212)
+    kernel2: y += Σ_k (A_{s_k} − α_{s_k}) · tmp_k                      (:257-312)
+    Returns (tmp float32[c], y float32[m]).
+    """
+    A = np.asarray(A)
+    sum_dx, zdx = dots(x, x_memo, z)
+    dx = np.asarray(x, dtype=F32) - np.asarray(x_memo, dtype=F32)
+    cols = A[:, idx_sorted].astype(F64)
+    al = np.asarray(alpha, dtype=F32)[idx_sorted].astype(F64)
+    d = cols.T @ dx.astype(F64)
+    tmp = ((d - al * sum_dx) * np.asarray(w, dtype=F32)[idx_sorted].astype(F64)).astype(F32)
+    base = (np.asarray(y_memo, dtype=F64) + (sum_dx * np.asarray(v, dtype=F64) + zdx)).astype(F32)
+    corr = cols @ tmp.astype(F64) - np.dot(al, tmp.astype(F64))
+    y = base.astype(F64) + corr
+    return tmp, y.astype(F32)
+
+
+# --------------------------------------------------------------------------------------------
+# Normalisation and Rayleigh step
+# --------------------------------------------------------------------------------------------
+
+def normalize(x):
+    """x / ‖x‖ with an FP64 sum of squares and an FP32 scale (common.h:156-183)."""
+    x = np.asarray(x, dtype=F32)
+    ss = float(np.dot(x.astype(F64), x.astype(F64)))
+    scale = F32(1.0 / np.sqrt(ss))
+    return (x * scale).astype(F32)
+
+
+def dot_product_and_generate_x(x, y, vstar=None):
+    """Rayleigh quotient, error, cosine and the next iterate (common.h:89-154).
+
+    λ = x·y, ‖y‖² and e = y·v* are FP64 sums; scale = 1/sqrt(‖y‖²) in FP64;
+    err = e·scale, cos = λ·scale; x_new = (float)scale · y in FP32.
+    Returns (lam, err, cos, x_new).
+    """
+    x64 = np.asarray(x, dtype=F32).astype(F64)
+    y32 = np.asarray(y, dtype=F32)
+    y64 = y32.astype(F64)
+    lam = float(np.dot(y64, x64))
+    yy = float(np.dot(y64, y64))
+    e = float(np.dot(y64, np.asarray(vstar, dtype=F64))) if vstar is not None else 0.0
+    scale = 1.0 / np.sqrt(yy)
+    x_new = (y32 * F32(scale)).astype(F32)
+    return lam, e * scale, lam * scale, x_new
+
+
+def reported_eigenvalue(lam, offset=0.0):
+    """The reference's printed eigenvalue max(0, sqrt(max(0, λ)) − offset)
+    (powerMethod_by_exact.cuh:83): an eigenvalue of its symmetric, diagonally shifted A."""
+    lam = np.asarray(lam, dtype=F64)
+    return np.maximum(0.0, np.sqrt(np.maximum(0.0, lam)) - offset)
+
+
+# --------------------------------------------------------------------------------------------
+# Drivers
+# --------------------------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class PowerTrace:
+    eigs: np.ndarray                     # λ per step (FP64)
+    errs: np.ndarray                     # (y·v*)/‖y‖ per step
+    coss: np.ndarray                     # cos∠(x_i, x_{i+1}) per step
+    modes: list                          # "exact", "exact_nomemo", "previous", "proposed"
+    indices: list                        # sorted sampled indices per AMM step (None otherwise)
+    x: np.ndarray                        # final iterate
+    y: np.ndarray                        # final product
+    states: np.ndarray                   # xorshift states after the run
+    cdf: dict                            # CDF per weighting ("norm", "normp") actually used
+
+
+def _sampling_tables(A, which, c, n, cdf_precision, sanity, cdf_override):
+    alpha, norm, normp = get_norms(A)
+    base = norm if which == "norm" else normp
+    f32 = cdf_precision == "f32"
+    if sanity and c == n:
+        weight = np.ones(n, dtype=F32 if f32 else F64)                 # device_memory.h:500-504
+    elif f32:
+        weight = set_weights(base)
+    else:
+        # FP64 mode: the exact square of the FP32 norm (no FP32 rounding of norm²)
+        weight = base.astype(F64) * base.astype(F64)
+    if cdf_override is not None and which in cdf_override:
+        cdf = np.asarray(cdf_override[which])
+    else:
+        cdf = cdf_f32(weight) if f32 else cdf_f64(weight)
+    w = update_weights(weight, float(cdf[n - 1]), c,
+                       precision="f32" if cdf.dtype == F32 else "f64")
+    return cdf, w
+
+
+def power_method(A, x0, *, method="exact", step=10, c=None, states=None, vr_period=0,
+                 vr_adaptive_threshold=0.0, sanity=False, cdf_precision="f64", vstar=None,
+                 cdf_override: Optional[dict] = None):
+    """One call of ``powerMethod_by_{exact,previous,proposed,proposed_v2}``.
+
+    exact       powerMethod_by_exact.cuh:4-100
+    previous    powerMethod_by_previous.cuh:100-210 (square_of_A_by_previous at :7-98)
+    proposed    powerMethod_by_proposed.cuh:317-447 (square_of_A_by_proposed at :7-103)
+    proposed_v2 powerMethod_by_proposed_v2.cuh:199-377
+
+    ``x0`` is the raw start vector (the reference draws it with ``curandGenerateNormal`` and
+    then calls ``normalize``); it is normalised here.  ``states`` are the xorshift states
+    (the reference's ``d_rnd``); they are advanced once per sample of every AMM step and the
+    advanced states are returned.  Variance reduction (VR) follows the reference:
+
+    * previous:    VR when ``(i+1) % vr_period == 0`` or ``cos > 1 − thr``  (:135-137)
+    * proposed:    the same, and only when ``i > last_exact + 1``             (:371-373)
+    * proposed_v2: phase 1 is ``vr_period − 1`` previous-AMM steps; step ``vr_period − 1``
+      is exact without a memo update; phase 2 is proposed AMM with periodic VR (:234-347).
+
+    A VR step computes the exact product and copies [x | y] into [x_memo | y_memo].
+    ``sanity`` (with c == n) is the reference's ``-sanity`` known-answer mode: all weights 1 and
+    indices 0..n−1, so every AMM step equals the exact product.
+    """
+    A = np.asarray(A)
+    m, n = A.shape
+    if c is None:
+        c = n
+    x = normalize(x0)
+    memo_x = np.zeros(m, dtype=F32)
+    memo_y = np.zeros(m, dtype=F32)
+    y = np.zeros(m, dtype=F32)
+    states = np.zeros(max(c, 1), dtype=U32) if states is None else np.array(states, dtype=U32)
+    variance_reduction = vr_period > 0 or vr_adaptive_threshold > 0.0
+    alpha, norm, normp = get_norms(A)
+    a2 = alpha_squared(alpha)
+    z, v = generate_zv(A, alpha, a2)
+    use_seq = sanity and c == n
+    cdfs = {}
+
+    eigs, errs, coss, modes, indices = [], [], [], [], []
+
+    def amm_step(which):
+        nonlocal states, y
+        if which not in cdfs:
+            cdfs[which] = _sampling_tables(A, which, c, n, cdf_precision, sanity, cdf_override)
+        cdf, w = cdfs[which]
+        if use_seq:
+            idx = np.arange(n, dtype=U32)                              # device_memory.h:547-551
+        else:
+            idx, states = sample_sorted(cdf, states, c)
+        if which == "norm":
+            _, y = previous_amm(A, x, memo_x, memo_y, idx, w)
+        else:
+            _, y = proposed_amm(A, alpha, x, memo_x, memo_y, idx, w, z, v)
+        indices.append(idx)
+
+    def rayleigh():
+        nonlocal x
+        lam, err, cos, x_new = dot_product_and_generate_x(x, y, vstar)
+        eigs.append(lam)
+        errs.append(err)
+        coss.append(cos)
+        x = x_new
+        return cos
+
+    dot = 0.0
+    if method == "exact":
+        for _ in range(step):
+            y = exact_product(A, x)
+            modes.append("exact_nomemo")
+            indices.append(None)
+            rayleigh()
+    elif method in ("previous", "proposed"):
+        which = "norm" if method == "previous" else "normp"
+        last_exact = 0
+        for i in range(step):
+            vr_now = variance_reduction and (
+                (vr_period > 0 and (i + 1) % vr_period == 0)
+                or (vr_adaptive_threshold > 0.0 and dot > 1.0 - vr_adaptive_threshold))
+            if method == "proposed":
+                vr_now = vr_now and i > last_exact + 1
+            if vr_now:
+                y = exact_product(A, x)
+                memo_x, memo_y = x.copy(), y.copy()
+                last_exact = i
+                modes.append("exact")
+                indices.append(None)
+            else:
+                amm_step(which)
+                modes.append(method)
+            dot = rayleigh()
+    elif method == "proposed_v2":
+        if vr_period < 1 or step < vr_period:
+            raise ValueError("proposed_v2 needs 1 <= vr_period <= step")
+        for _ in range(vr_period - 1):
+            amm_step("norm")
+            modes.append("previous")
+            rayleigh()
+        y = exact_product(A, x)                   # [z, tmp] = A·[α, x]; y = A·tmp (:255-294)
+        modes.append("exact_nomemo")
+        indices.append(None)
+        rayleigh()
+        for i in range(vr_period, step):
+            if variance_reduction and (i + 1) % vr_period == 0:
+                y = exact_product(A, x)
+                memo_x, memo_y = x.copy(), y.copy()
+                modes.append("exact")
+                indices.append(None)
+            else:
+                amm_step("normp")
+                modes.append("proposed")
+            rayleigh()
+    else:
+        raise ValueError(f"unknown method {method!r}")
+
+    return PowerTrace(np.array(eigs, dtype=F64), np.array(errs, dtype=F64),
+                      np.array(coss, dtype=F64), modes, indices, x, y, states,
+                      {k: v_[0] for k, v_ in cdfs.items()})
+
+
+# --------------------------------------------------------------------------------------------
+# Extensions: FP64 truth and the gradient of λ_max
+# --------------------------------------------------------------------------------------------
+
+def lambda_max_f64(A) -> float:
+    """λ_max(A·Aᵀ) by FP64 LAPACK ``syevd`` on C (the same call calculate_largest_eigenvalue.py:
+    1-13 makes on its matrix, via numpy ``eigh``)."""
+    A64 = np.asarray(A, dtype=F64)
+    C = A64 @ A64.T
+    return float(np.linalg.eigvalsh(C)[-1])
+
+
+def grad_lambda(A, v) -> np.ndarray:
+    """∂λ_max/∂A = 2·v·(vᵀA) for a unit top eigenvector v of A·Aᵀ (FP64)."""
+    A64 = np.asarray(A, dtype=F64)
+    v64 = np.asarray(v, dtype=F64)
+    v64 = v64 / np.linalg.norm(v64)
+    return 2.0 * np.outer(v64, v64 @ A64)

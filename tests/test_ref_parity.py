@@ -1,0 +1,152 @@
+"""GPU parity of libamm against the REFERENCE's own kernels and drivers, compiled for sm_100a
+from the reference sources (oracle/_ref/libamm_ref.so, built by oracle/Makefile).
+
+Inputs are square and symmetric because the reference only handles m x m (m % 128 == 0,
+c % 8 == 0, c <= m).  The reference builds its FP32 CDF with CUB; that array is imported into
+libamm (amm_set_cdf) so that "same seed and same probabilities" holds bit for bit, and the
+sampled index sets are then compared exactly.
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE / "golden"))
+
+import inputs as I  # noqa: E402
+import amm_oracle as O  # noqa: E402
+import ref_harness as R  # noqa: E402
+from helpers import RTOL_LAMBDA_F32, rel, vec_rel  # noqa: E402
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")]
+
+KERNEL_TO_METHOD = {"exact": "exact", "previousAMM": "previous", "proposedAMM": "proposed",
+                    "proposedAMM_v2": "proposed_v2"}
+
+
+def ctx_for(A, **kw):
+    from eigenvaluecomputation_by_amm_b200 import AMMContext, column_major
+    ctx = AMMContext(A.shape[0], A.shape[1], **kw)
+    ctx.set_matrix(column_major(torch.from_numpy(np.ascontiguousarray(A)).cuda()))
+    return ctx
+
+
+def tu32(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.uint32).view(np.int32)).cuda()
+
+
+def test_pick_index_bit_exact_vs_reference():
+    cdf, st = I.pick_inputs()
+    ridx, rst = R.pick_index(cdf, st)
+    A = np.ones((64, len(cdf)), np.float32)
+    ctx = ctx_for(A, c=len(st), cdf_precision="f32")
+    ctx.set_cdf(0, torch.from_numpy(cdf))
+    ctx.set_rng_state(tu32(st))
+    got = ctx.sample_indices(0).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, ridx)
+    oidx, ost = O.pick_index(cdf, st, len(st))
+    assert np.array_equal(oidx, ridx) and np.array_equal(ost, rst)
+
+
+def test_seeded_states_and_start_vectors_match_reference():
+    m = I.M
+    A = I.symmetric_matrix()
+    ctx = ctx_for(A, c=I.C)
+    ctx.seed_rng(42, count=m)
+    assert np.array_equal(ctx.get_rng_state(m).cpu().numpy().view(np.uint32), R.seed_states(m, 42))
+    ctx.seed_start_vectors(1276)
+    x0 = ctx.draw_start_vector().cpu().numpy()
+    assert np.array_equal(x0, R.draw_x0(m, 1276))
+
+
+@pytest.mark.parametrize("kernel", ["previousAMM", "proposedAMM"])
+def test_step_by_step_indices_and_lambda(kernel):
+    """Per step: the sorted sampled index set is bit-exact, y and λ within FP32 tolerance."""
+    A = I.symmetric_matrix()
+    st = I.states()
+    x0 = I.start_vector()
+    ref = R.amm_steps(kernel, A, x0, st, c=I.C, nsteps=I.NSTEPS)
+    ctx = ctx_for(A, c=I.C, cdf_precision="f32")
+    which = 0 if kernel == "previousAMM" else 1
+    ctx.set_cdf(which, torch.from_numpy(ref["cdf"]))
+    _, w = ctx.sampling_tables(which)
+    np.testing.assert_allclose(w.cpu().numpy(), ref["weight"], rtol=4e-7)
+    ctx.set_rng_state(tu32(st))
+    x = torch.from_numpy(x0).cuda()
+    ctx.normalize(x)
+    for i in range(I.NSTEPS):
+        if kernel == "previousAMM":
+            y, idx = ctx.core_previousAMM(x)
+        else:
+            y, idx = ctx.core_proposedAMM(x)
+        assert np.array_equal(idx.cpu().numpy().view(np.uint32), ref["sorted"][i]), f"step {i}"
+        assert vec_rel(y.cpu().numpy(), ref["y"][i]) < 1e-5
+        lam, _, _ = ctx.rayleigh_normalize(x, y)
+        assert rel(lam, ref["eigs"][i]) < RTOL_LAMBDA_F32
+    assert np.array_equal(ctx.get_rng_state(I.C).cpu().numpy().view(np.uint32), ref["states"][:I.C])
+
+
+RUNS = {
+    "exact": dict(vr_period=0),
+    "previousAMM": dict(vr_period=I.VR),
+    "proposedAMM": dict(vr_period=I.VR),
+    "proposedAMM_v2": dict(vr_period=I.VR),
+}
+
+
+@pytest.mark.parametrize("kernel", list(RUNS))
+def test_power_method_vs_reference_driver(kernel):
+    A = I.symmetric_matrix()
+    st = I.states()
+    vstar = I.top_eigenvector(A)
+    kw = RUNS[kernel]
+    ref = R.power_method(kernel, A, 1276, st, c=I.C, step=I.STEPS, vstar=vstar, **kw)
+    ctx = ctx_for(A, c=I.C, step=I.STEPS, cdf_precision="f32", **kw)
+    if kernel != "exact":
+        # the reference's CDF of the weighting its last AMM step used
+        ctx.set_cdf(1 if kernel != "previousAMM" else 0, torch.from_numpy(ref["cdf"]))
+    if kernel == "proposedAMM_v2":
+        # phase 1 samples with the ‖A_j‖² weighting: rebuild that CDF from the reference norms
+        ctx.set_cdf(0, torch.from_numpy(np.cumsum(
+            (ref["norm"].astype(np.float32) ** 2).astype(np.float64)).astype(np.float32)))
+    ctx.set_rng_state(tu32(st))
+    ctx.set_eigenvector(torch.from_numpy(vstar))
+    x0 = torch.from_numpy(R.draw_x0(I.M, 1276)).cuda()
+    ctx.power_method(KERNEL_TO_METHOD[kernel], x0)
+    tr = ctx.trace()
+    assert np.all(rel(tr["eigs"], ref["eigs"]) < 1e-4), (tr["eigs"], ref["eigs"])
+    assert np.all(np.abs(tr["errs"] - ref["errs"]) < 1e-4)
+    st_got = ctx.get_rng_state(I.C).cpu().numpy().view(np.uint32)
+    assert np.array_equal(st_got, ref["states"][:I.C])
+    stats = ctx.column_stats()
+    np.testing.assert_allclose(stats["norm"].cpu().numpy(), ref["norm"], rtol=1e-6)
+    np.testing.assert_allclose(stats["normp"].cpu().numpy(), ref["normp"], rtol=1e-5)
+    np.testing.assert_allclose(stats["alpha"].cpu().numpy(), ref["alpha"], rtol=1e-6, atol=1e-8)
+
+
+def test_reference_rectangular_embedding_previous():
+    """A 512 x 2048 matrix padded with zero rows to 2048 x 2048: the reference's AMM kernels
+    then compute A·Aᵀ restricted to the first 512 rows (no VR: its exact path assumes A = Aᵀ)."""
+    m, n, c, step = 512, 2048, 256, 10
+    rng = np.random.default_rng(5)
+    A = (rng.standard_normal((m, n)) * rng.lognormal(0, 1, n)).astype(np.float32)
+    Ap = np.zeros((n, n), np.float32)
+    Ap[:m] = A
+    st = rng.integers(1, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+    ref = R.power_method("previousAMM", Ap, 99, st, c=c, step=step)
+    x0 = R.draw_x0(n, 99)[:m]
+    ctx = ctx_for(A, c=c, step=step, cdf_precision="f32")
+    ctx.set_cdf(0, torch.from_numpy(ref["cdf"]))
+    ctx.set_rng_state(tu32(st[:c]))
+    # the reference normalises all n entries of x0; the padded rows stay in the norm only at
+    # step 0, so compare from the same normalised start: feed x0 scaled like the reference
+    full = R.draw_x0(n, 99).astype(np.float64)
+    x0s = (x0 / np.sqrt((full ** 2).sum())).astype(np.float32)
+    ctx_x = torch.from_numpy(x0s).cuda()
+    ctx.power_method("previous", ctx_x)
+    tr = ctx.trace()
+    assert np.all(rel(tr["eigs"][1:], ref["eigs"][1:]) < 1e-4)
