@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--max-exact-steps", type=int, default=80)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--trace-out", default=None, help="write the calibration λ traces (JSON)")
     return p.parse_args()
 
 
@@ -290,6 +291,7 @@ def run_ours(args, rank, world):
     cal.set_matrix(A32)
     cal.power_method("exact", x0)
     tr = cal.trace()
+    traces = {"lambda_fp64": lam_true, "exact_fp32": tr["eigs"].tolist()}
     k_exact = steps_to_tol(tr["eigs"], lam_true)
     cal.close()
     if k_exact is None:
@@ -309,6 +311,8 @@ def run_ours(args, rank, world):
         cal.power_method("proposed", x0)
         tr = cal.trace()
         cal.close()
+        traces[f"proposed_vr{P}"] = {"eigs": tr["eigs"].tolist(), "kinds": tr["kinds"],
+                                     "distinct": tr["distinct"].tolist()}
         k = steps_to_tol(tr["eigs"], lam_true)
         if k is None:
             continue
@@ -318,6 +322,8 @@ def run_ours(args, rank, world):
         t = timed_solve(ctx, A16, "proposed", 2, 1)
         kinds = ctx.trace()["kinds"]
         cands.append((statistics.median(t), P, steps, kinds.count("exact"), ctx))
+    if args.trace_out and rank == 0:
+        Path(args.trace_out).write_text(json.dumps(traces))
     if not cands:
         raise RuntimeError("proposed AMM did not reach 1e-3 for any VR period")
     cands.sort(key=lambda z: z[0])

@@ -115,6 +115,7 @@ struct PanelGeom {
   int gc;           // columns per stage
   int nstages;
   int stage_bytes;  // gc * colbytes
+  int stage_area;   // bytes reserved for the stages (also prologue scratch)
   int smem_bytes;   // dynamic shared memory
   int wl_cap;       // work-list capacity per CTA
 };

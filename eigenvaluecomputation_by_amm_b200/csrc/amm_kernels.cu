@@ -320,7 +320,7 @@ struct PanelArgs {
   int setup;
 };
 
-// Shared memory: [nstages * stage_bytes] | bars[8] | red (4 KB) | wl_idx | wl_mult | scan[40]
+// Shared memory: [stage_area >= nstages * stage_bytes] | bars[8] | red (4 KB) | wl_idx | wl_mult | scan[40]
 template <typename Elem, int R, bool SETUP>
 __global__ void __launch_bounds__(kMaxThreads, 1) panel_kernel(const __grid_constant__ PanelArgs a) {
   constexpr int E = 16 / static_cast<int>(sizeof(Elem));
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) panel_kernel(const __grid_cons
 
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* stage_base = smem;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)g.nstages * g.stage_bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)g.stage_area);
   float* red = reinterpret_cast<float*>(bars + 8);
   double* red64 = reinterpret_cast<double*>(red);
   uint32_t* wl_idx = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(red) + 4096);
@@ -577,10 +577,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) panel_kernel(const __grid_cons
       break;
     }
     // refill the stage consumed by the previous group (everyone has finished with it)
-    if (t == 0 && grp >= 1 && grp - 1 + NS < ngroups) {
-      fence_proxy_async_smem();
-      issue(grp - 1 + NS);
-    }
+    if (t == 0 && grp >= 1 && grp - 1 + NS < ngroups) issue(grp - 1 + NS);
     float coef[kGcMax];
 #pragma unroll
     for (int q = 0; q < kGcMax; ++q) {
@@ -1217,9 +1214,10 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   int maxlist = c < n ? c : n;
   int wl = (maxlist + nsm - 1) / nsm + 1;
   g->wl_cap = wl;
-  const int nchunk_scratch = 4 * 4096;  // prefix scratch lives in the stage area
-  if (ns * stage < nchunk_scratch) return false;
-  g->smem_bytes = ns * stage + 8 * 8 + 4096 + 2 * wl * 4 + 40 * 4;
+  // the stage area doubles as scratch for the per-chunk prefix (<= 4096 uint32) before the
+  // pipeline starts
+  g->stage_area = ns * stage > 4 * 4096 ? ns * stage : 4 * 4096;
+  g->smem_bytes = g->stage_area + 8 * 8 + 4096 + 2 * wl * 4 + 40 * 4;
   return g->smem_bytes <= 227 * 1024;
 }
 

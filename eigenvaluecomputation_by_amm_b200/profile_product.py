@@ -1,0 +1,50 @@
+"""Launch the fused product kernel in isolation, for profilers (ncu) and quick timing.
+
+    python -m eigenvaluecomputation_by_amm_b200.profile_product --m 16384 --n 8192 \
+        --dtype bf16 --kinds exact,proposed --reps 1
+
+Builds a context on a seeded N(0,1) x lognormal(0,1) matrix, runs one warm-up call (which also
+runs the set-up pass), then times `reps` launches of the product kernel per kind with CUDA
+events and prints the mean time and the algorithmic HBM rate per launch.
+"""
+from __future__ import annotations
+
+import argparse
+
+import torch
+
+from .api import AMMContext, column_major
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--m", type=int, default=16384)
+    p.add_argument("--n", type=int, default=8192)
+    p.add_argument("--c", type=int, default=4096)
+    p.add_argument("--dtype", default="bf16", choices=["f32", "bf16"])
+    p.add_argument("--kinds", default="exact,proposed")
+    p.add_argument("--reps", type=int, default=1)
+    p.add_argument("--seed", type=int, default=0)
+    a = p.parse_args()
+    g = torch.Generator(device="cuda").manual_seed(a.seed)
+    At = torch.randn(a.n, a.m, device="cuda", generator=g)
+    At *= torch.randn(a.n, 1, device="cuda", generator=g).exp()
+    A = At.t() if a.dtype == "f32" else At.to(torch.bfloat16).t()
+    del At
+    es = 4 if a.dtype == "f32" else 2
+    ctx = AMMContext(a.m, a.n, c=a.c, step=2, dtype=a.dtype)
+    ctx.set_matrix(A)
+    ctx.set_rng_state(torch.arange(1, a.c + 1, dtype=torch.int32, device="cuda") * 2654435761 % (2**31))
+    x0 = torch.randn(a.m, device="cuda", generator=g)
+    ctx.power_method("proposed", x0)
+    ctx.trace()
+    for kind in a.kinds.split(","):
+        ms, cd = ctx.benchmark_product(kind, reps=a.reps)
+        byts = a.m * cd * es + (0 if kind == "exact" else 8 * a.c) + 16 * a.m
+        print(f"{kind:9s} dtype={a.dtype} m={a.m} n={a.n} c={a.c}: {ms * 1e3:9.2f} us/launch, "
+              f"{cd} columns, {byts / ms / 1e6:8.1f} GB/s algorithmic")
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
