@@ -85,6 +85,7 @@ _SIGS = {
     "amm_sample_indices": [_P, C.c_int, _P, _P],
     "amm_benchmark_product": [_P, C.c_int, C.c_int, _P, _P, _P],
     "amm_grad_lambda": [_P, _P, _P, _I64, _P],
+    "amm_get_geometry": [_P, _P],
     "amm_status_string": [C.c_int],
     "amm_last_cuda_error": [],
     "amm_kernel_launch_count": [],

@@ -256,6 +256,13 @@ class AMMContext:
                                              _stream(stream)), "amm_benchmark_product")
         return float(ms.value), int(d.value)
 
+    def geometry(self) -> dict:
+        out = (C.c_int32 * 10)()
+        check(self.lib.amm_get_geometry(self._ctx, out), "amm_get_geometry")
+        keys = ("cluster", "rows_per_cta", "clusters", "threads", "slots", "cols_per_stage",
+                "stages", "stage_bytes", "smem_bytes", "worklist_cap")
+        return dict(zip(keys, list(out)))
+
     def grad_lambda(self, v: torch.Tensor, stream=None) -> torch.Tensor:
         """∂λ/∂A = 2·v·(vᵀA) as an (m, n) column-major FP32 tensor."""
         v = self._vec(v)

@@ -69,6 +69,8 @@ struct amm_ctx {
   float* y_final = nullptr;
   double* out3 = nullptr;
   cudaStream_t cap_stream = nullptr;
+  cudaStream_t side_stream = nullptr;  // the sampler runs here, concurrently with the product
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   curandGenerator_t x0_gen = nullptr;
   std::map<GraphKey, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
   int last_step = 0;
@@ -130,13 +132,15 @@ void layout(amm_ctx* ctx, Carver& cv) {
   }
   b.distinct_idx = cv.take<uint32_t>(c);
   b.distinct_mult = cv.take<uint32_t>(c);
-  b.partials = cv.take<float>((size_t)ctx->nsm * m);
-  b.spart = cv.take<float>(ctx->nsm);
-  b.spart64 = cv.take<double>(ctx->nsm);
+  b.partials = cv.take<float>((size_t)b.nsm * m);
+  b.spart = cv.take<float>(b.nsm);
+  b.spart64 = cv.take<double>(b.nsm);
   b.rpart = cv.take<double>(4 * ((m + 127) / 128));
   b.ticket = cv.take<uint32_t>(4);
   b.alpha2 = cv.take<double>(1);
   b.colvec = cv.take<float>(n);
+  b.cdf_tsum = cv.take<double>(2 * ((n + 4095) / 4096));
+  b.colsum = cv.take<double2>(n);
   b.st = cv.take<amm::IterState>(2);
   b.eigs = cv.take<double>(step);
   b.errs = cv.take<double>(step);
@@ -166,13 +170,29 @@ CallCfg make_cc(const amm_ctx* ctx, int method) {
 
 int ensure_setup(amm_ctx* ctx, cudaStream_t s);
 
-// The launch sequence of one call (captured into a graph or issued directly).
+// The launch sequence of one call (captured into a graph or issued directly):
+//   init, first draw | for each step: product || next draw (forked stream), reduce | finalize
 int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
                  cudaStream_t s) {
   const Buffers& b = ctx->b;
+  const bool draws = cc.uses_amm && !cc.sanity;
+  if (draws && !ctx->side_stream) {
+    AMM_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+    AMM_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    AMM_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
   AMM_CUDA(amm::launch_init(b, cc, x0, no_normalize, s));
+  if (draws) AMM_CUDA(amm::launch_sample(b, cc, -1, s));
   for (int i = 0; i < cc.step; ++i) {
+    const bool fork = draws && i + 1 < cc.step;
+    if (fork) {
+      AMM_CUDA(cudaEventRecord(ctx->ev_fork, s));
+      AMM_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0));
+      AMM_CUDA(amm::launch_sample(b, cc, i, ctx->side_stream));
+      AMM_CUDA(cudaEventRecord(ctx->ev_join, ctx->side_stream));
+    }
     AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, s));
+    if (fork) AMM_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
     AMM_CUDA(amm::launch_iter_reduce(b, cc, i, s));
   }
   AMM_CUDA(amm::launch_finalize(b, cc, ctx->x_final, ctx->y_final, s));
@@ -219,7 +239,7 @@ int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
     it = ctx->graphs.emplace(key, std::make_pair(g, ex)).first;
   }
   AMM_CUDA(cudaGraphLaunch(it->second.second, s));
-  amm::count_launch(2 + 2 * cc.step);
+  amm::count_launch(2 + 2 * cc.step + ((cc.uses_amm && !cc.sanity) ? cc.step : 0));
   return AMM_OK;
 }
 
@@ -347,6 +367,15 @@ const char* amm_status_string(int status) {
 
 const char* amm_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
 
+int amm_get_geometry(amm_ctx* ctx, int32_t* out10) {
+  if (!ctx || !out10) return AMM_ERR_INVALID_ARGUMENT;
+  const PanelGeom& g = ctx->geom;
+  const int32_t v[10] = {g.cluster, g.rows,  g.nclusters,   g.threads,    g.slots,
+                         g.gc,      g.nstages, g.stage_bytes, g.smem_bytes, g.wl_cap};
+  for (int i = 0; i < 10; ++i) out10[i] = v[i];
+  return AMM_OK;
+}
+
 int64_t amm_kernel_launch_count(void) { return amm::launch_count(); }
 
 int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
@@ -378,6 +407,7 @@ int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
   ctx->sanity_active = (cfg.sanity && cfg.c == cfg.n) ? 1 : 0;
   if (!amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm, &ctx->geom)) {
     delete ctx;
+    cudaGetLastError();
     return AMM_ERR_UNSUPPORTED;
   }
   Buffers& b = ctx->b;
@@ -386,7 +416,7 @@ int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
   b.c = (int32_t)cfg.c;
   b.dtype = cfg.dtype;
   b.cdf_f32 = cfg.cdf_precision == AMM_CDF_F32 ? 1 : 0;
-  b.nsm = ctx->nsm;
+  b.nsm = ctx->geom.nclusters;
   int seg = amm::kSeg;
   while (cfg.n / seg > amm::kCoarseMax) seg <<= 1;
   b.seg = seg;
@@ -424,6 +454,9 @@ int amm_destroy(amm_ctx* ctx) {
   DeviceGuard dg(ctx->device);
   drop_graphs(ctx);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->x0_gen) curandDestroyGenerator(ctx->x0_gen);
   if (ctx->pool) cudaFree(ctx->pool);
   delete ctx;
@@ -438,9 +471,10 @@ int amm_set_matrix(amm_ctx* ctx, const void* dA, int64_t ld, void* stream) {
   DeviceGuard dg(ctx->device);
   cudaStream_t s = as_stream(stream);
   (void)s;
+  // the captured graphs hold A and ld by value: keep them when the same matrix is rebound
+  if (ctx->b.A != dA || ctx->b.ld != ld) drop_graphs(ctx);
   ctx->b.A = dA;
   ctx->b.ld = ld;
-  drop_graphs(ctx);
   ctx->matrix_set = true;
   ctx->setup_done = false;
   return AMM_OK;
@@ -739,6 +773,7 @@ int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch
   cc.tol = 0.0;
   cc.step = 1;
   AMM_CUDA(amm::launch_init(ctx->b, cc, ctx->x0_buf, 0, s));
+  if (cc.uses_amm && !ctx->sanity_active) AMM_CUDA(amm::launch_sample(ctx->b, cc, -1, s));
   cudaEvent_t e0, e1;
   AMM_CUDA(cudaEventCreate(&e0));
   AMM_CUDA(cudaEventCreate(&e1));

@@ -57,7 +57,7 @@ struct Buffers {
   int32_t m, n, c;
   int32_t dtype;       // 0 FP32, 1 BF16
   int32_t cdf_f32;     // 1: FP32 CDF and target
-  int32_t nsm;         // panel-kernel CTAs (= partial sums)
+  int32_t nsm;         // partial sums written by the panel kernel (one per cluster)
   // per-column statistics (n)
   float* alpha;
   float* norm;
@@ -95,6 +95,8 @@ struct Buffers {
   uint32_t* ticket;    // last-CTA counters [0]: reduce, [1]: small kernels
   double* alpha2;      // ‖α‖²
   float* colvec;       // n floats of scratch (vᵀA for the gradient)
+  double* cdf_tsum;    // 2 x ceil(n/4096) tile sums of the CDF build
+  double2* colsum;     // n (Σa, Σa²) of each column from the set-up pass
   // iteration state and traces
   IterState* st;       // [2]
   double* eigs;
@@ -108,16 +110,20 @@ struct Buffers {
 
 // Launch geometry of the panel kernel for a given (m, dtype).
 struct PanelGeom {
-  int threads;      // block size
-  int slots;        // vector slots per thread (R)
+  int dtype;        // 0 FP32, 1 BF16
+  int cluster;      // CTAs per cluster (K); CTA rank r owns rows [r*rows, (r+1)*rows)
+  int rows;         // rows per CTA = m / cluster
+  int nclusters;    // clusters launched (= partial sums)
+  int threads;      // consumer threads (a producer warp is added)
+  int slots;        // 16-byte vector slots per consumer thread (R)
   int elems;        // elements per 16-byte vector (E)
-  int colbytes;     // m * elem_size
-  int gc;           // columns per stage
+  int colbytes;     // bytes of one column slice = rows * elem_size
+  int gc;           // columns per stage (group)
   int nstages;
   int stage_bytes;  // gc * colbytes
   int stage_area;   // bytes reserved for the stages (also prologue scratch)
-  int smem_bytes;   // dynamic shared memory
-  int wl_cap;       // work-list capacity per CTA
+  int smem_bytes;   // dynamic shared memory (set-up variant, the larger one)
+  int wl_cap;       // work-list capacity per cluster
 };
 
 bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g);
@@ -134,7 +140,10 @@ cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sani
 // no_normalize: use x0 as x_0 unscaled (single-product entry points).
 cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, int no_normalize,
                         cudaStream_t s);
-// One iteration: panel product and reduce/Rayleigh/next-picks.
+// Draw the picks of the first AMM step after step iter (iter = -1: start of a call); for
+// iter >= 0 it may run concurrently with the product of step iter.
+cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
+// One iteration: panel product and reduce/Rayleigh/clear.
 cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
                               cudaStream_t s);
 cudaError_t launch_iter_reduce(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);

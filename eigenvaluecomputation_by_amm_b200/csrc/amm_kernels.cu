@@ -16,6 +16,7 @@
 #include <atomic>
 #include <cstdint>
 
+#include "amm_device.cuh"
 #include "amm_internal.h"
 
 namespace amm {
@@ -23,103 +24,6 @@ namespace amm {
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
-
-// ------------------------------------------------------------------------------------------
-// Device helpers
-// ------------------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: gives up after ~2^22 polls (each try_wait may suspend briefly) and reports.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 22); ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-__device__ __forceinline__ uint64_t l2_evict_first_policy() {
-  uint64_t pol;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
-
-// 1-D bulk copy global -> shared, completion signalled on `bar` (transaction bytes).
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
-                                         uint64_t policy) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
-      "[%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
-      : "memory");
-}
-
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// 16-byte vector -> E floats.
-__device__ __forceinline__ void unpack(const uint4& v, float (&o)[4]) {
-  o[0] = __uint_as_float(v.x);
-  o[1] = __uint_as_float(v.y);
-  o[2] = __uint_as_float(v.z);
-  o[3] = __uint_as_float(v.w);
-}
-__device__ __forceinline__ void unpack(const uint4& v, float (&o)[8]) {
-  // bf16 -> fp32 is exact: the 16 bits become the high half of the float.
-  o[0] = __uint_as_float(v.x << 16);
-  o[1] = __uint_as_float(v.x & 0xffff0000u);
-  o[2] = __uint_as_float(v.y << 16);
-  o[3] = __uint_as_float(v.y & 0xffff0000u);
-  o[4] = __uint_as_float(v.z << 16);
-  o[5] = __uint_as_float(v.z & 0xffff0000u);
-  o[6] = __uint_as_float(v.w << 16);
-  o[7] = __uint_as_float(v.w & 0xffff0000u);
-}
 
 // Kind of the step that follows, as the reference's drivers decide it:
 //  previous    powerMethod_by_previous.cuh:135-137
@@ -248,416 +152,20 @@ __device__ void load_coarse(const Buffers& b, int which, F* coarse_s) {
     src = reinterpret_cast<const F*>(b.coarse64[which]);
   else
     src = reinterpret_cast<const F*>(b.coarse32[which]);
-  for (int k = threadIdx.x; k < b.ncoarse; k += blockDim.x) coarse_s[k] = src[k];
+  const F* __restrict__ csrc = src;
+  for (int k = threadIdx.x; k < b.ncoarse; k += blockDim.x) coarse_s[k] = __ldg(csrc + k);
   __syncthreads();
 }
 
-// Sampling role shared by the init and reduce kernels: clear the consumed picks (optional)
-// and draw the next ones.
-__device__ void sampling_role(const Buffers& b, int which, int clear_pb, int sb_in, int pb_out,
-                              int rank, int nranks, bool draw) {
-  __shared__ __align__(16) double coarse_s[kCoarseMax];
+// Clear the picks of buffer pb (consumed by the last product): every counted column and
+// every chunk total, so that the buffer is all-zero before its next draw.
+__device__ void clear_picks(const Buffers& b, int pb, int rank, int nranks) {
   const int tid = rank * blockDim.x + threadIdx.x;
   const int nthr = nranks * blockDim.x;
-  if (clear_pb >= 0) {
-    uint32_t* cnt = b.count[clear_pb];
-    const uint32_t* smp = b.samples[clear_pb];
-    for (int k = tid; k < b.c; k += nthr) cnt[smp[k]] = 0u;
-    for (int k = tid; k < b.nchunks; k += nthr) b.chunk[clear_pb][k] = 0u;
-  }
-  if (!draw) return;
-  if (b.cdf_f32) {
-    float* cs = reinterpret_cast<float*>(coarse_s);
-    load_coarse<float>(b, which, cs);
-    draw_samples<float>(b, which, b.states[sb_in], b.states[sb_in ^ 1], b.count[pb_out],
-                        b.chunk[pb_out], b.samples[pb_out], tid, nthr, cs);
-  } else {
-    load_coarse<double>(b, which, coarse_s);
-    draw_samples<double>(b, which, b.states[sb_in], b.states[sb_in ^ 1], b.count[pb_out],
-                         b.chunk[pb_out], b.samples[pb_out], tid, nthr, coarse_s);
-  }
-}
-
-// Block-wide exclusive scan of one uint32 per thread; returns the exclusive prefix and
-// writes the block total to *total.  `scratch` holds >= 33 uint32.
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* scratch,
-                                                         uint32_t* total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  uint32_t incl = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  if (lane == 31) scratch[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < nw ? scratch[lane] : 0u;
-    uint32_t wi = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += y;
-    }
-    if (lane < nw) scratch[lane] = wi - w;
-    if (lane == 31) scratch[32] = wi;
-  }
-  __syncthreads();
-  const uint32_t r = scratch[warp] + incl - v;
-  *total = scratch[32];
-  __syncthreads();
-  return r;
-}
-
-// ------------------------------------------------------------------------------------------
-// Panel kernel
-// ------------------------------------------------------------------------------------------
-struct PanelArgs {
-  Buffers b;
-  PanelGeom g;
-  CallCfg cc;
-  int iter;
-  int setup;
-};
-
-// Shared memory: [stage_area >= nstages * stage_bytes] | bars[8] | red (4 KB) | wl_idx | wl_mult | scan[40]
-template <typename Elem, int R, bool SETUP>
-__global__ void __launch_bounds__(kMaxThreads, 1) panel_kernel(const __grid_constant__ PanelArgs a) {
-  constexpr int E = 16 / static_cast<int>(sizeof(Elem));
-  const Buffers& b = a.b;
-  const PanelGeom& g = a.g;
-  const int T = blockDim.x, t = threadIdx.x, warp = t >> 5, lane = t & 31, nwarps = T >> 5;
-  const int m = b.m, nvec = m / E, G = gridDim.x, bid = blockIdx.x;
-
-  extern __shared__ __align__(128) unsigned char smem[];
-  unsigned char* stage_base = smem;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)g.stage_area);
-  float* red = reinterpret_cast<float*>(bars + 8);
-  double* red64 = reinterpret_cast<double*>(red);
-  uint32_t* wl_idx = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(red) + 4096);
-  uint32_t* wl_mult = wl_idx + g.wl_cap;
-  uint32_t* scan = wl_mult + g.wl_cap;
-
-  int mode = kExact, pb = 0;
-  float scale = 0.f;
-  if (!SETUP) {
-    const IterState& st = b.st[a.iter & 1];
-    if (st.done) return;
-    mode = st.mode;
-    pb = st.pb;
-    scale = st.scale;
-  }
-  const bool amm = !SETUP && (mode == kPrevious || mode == kProposed);
-  const bool centred = !SETUP && mode == kProposed;
-  const bool sampled = amm && !a.cc.sanity;
-  const int which = centred ? 1 : 0;
-
-  // ---- this CTA's column list -------------------------------------------------------
-  int64_t lo = 0, hi = 0;
-  if (!sampled) {
-    lo = (int64_t)bid * b.n / G;
-    hi = (int64_t)(bid + 1) * b.n / G;
-  } else {
-    // exclusive prefix of the distinct counts per chunk (stage area is scratch here)
-    uint32_t* cpre = reinterpret_cast<uint32_t*>(stage_base);
-    const uint32_t* chunk = b.chunk[pb];
-    uint32_t carry = 0;
-    for (int base = 0; base < b.nchunks; base += T) {
-      const int k = base + t;
-      const uint32_t v = k < b.nchunks ? chunk[k] : 0u;
-      uint32_t tot;
-      const uint32_t ex = block_exclusive_scan(v, scan, &tot);
-      if (k < b.nchunks) cpre[k] = carry + ex;
-      carry += tot;
-    }
-    __syncthreads();
-    const uint32_t cd = carry;
-    lo = (int64_t)bid * cd / G;
-    hi = (int64_t)(bid + 1) * cd / G;
-    if (bid == 0 && t == 0) b.distinct_hist[a.iter] = (int32_t)cd;
-    if (hi > lo) {
-      // chunk holding rank lo: the largest k with cpre[k] <= lo
-      int ka = 0, kb = b.nchunks - 1;
-      while (ka < kb) {
-        const int mid = (ka + kb + 1) >> 1;
-        if (cpre[mid] <= (uint32_t)lo)
-          ka = mid;
-        else
-          kb = mid - 1;
-      }
-      const uint32_t* cnt = b.count[pb];
-      const int CH = 1 << b.chunk_shift;
-      for (int kc = ka; kc < b.nchunks && cpre[kc] < (uint32_t)hi; ++kc) {
-        uint32_t rank0 = cpre[kc];
-        const int start = kc << b.chunk_shift;
-        const int len = min(CH, b.n - start);
-        for (int p0 = 0; p0 < len; p0 += T) {
-          const int p = p0 + t;
-          const uint32_t mult = p < len ? cnt[start + p] : 0u;
-          uint32_t tot;
-          const uint32_t ex = block_exclusive_scan(mult ? 1u : 0u, scan, &tot);
-          const int64_t r = (int64_t)rank0 + ex;
-          if (mult && r >= lo && r < hi) {
-            wl_idx[r - lo] = (uint32_t)(start + p);
-            wl_mult[r - lo] = mult;
-          }
-          rank0 += tot;
-        }
-      }
-    }
-    __syncthreads();
-    for (int k = t; k < (int)(hi - lo); k += T) {
-      b.distinct_idx[lo + k] = wl_idx[k];
-      b.distinct_mult[lo + k] = wl_mult[k];
-    }
-  }
-  const int nb = (int)(hi - lo);
-  const int gc = g.gc, NS = g.nstages;
-  const int ngroups = (nb + gc - 1) / gc;
-  const uint64_t policy = l2_evict_first_policy();
-  const size_t col_stride = (size_t)b.ld * sizeof(Elem);
-  const unsigned char* Abase = reinterpret_cast<const unsigned char*>(b.A);
-
-  auto column_of = [&](int k) -> uint32_t {
-    return sampled ? wl_idx[k] : (uint32_t)(lo + k);
-  };
-  auto issue = [&](int grp) {
-    const int s = grp % NS;
-    const int c0 = grp * gc;
-    const int cnt = min(gc, nb - c0);
-    mbar_arrive_expect_tx(&bars[s], (uint32_t)(cnt * g.colbytes));
-    for (int q = 0; q < cnt; ++q) {
-      const uint32_t col = column_of(c0 + q);
-      bulk_g2s(stage_base + (size_t)s * g.stage_bytes + (size_t)q * g.colbytes,
-               Abase + (size_t)col * col_stride, (uint32_t)g.colbytes, &bars[s], policy);
-    }
-  };
-
-  if (t == 0) {
-    for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  if (t == 0) {
-    fence_proxy_async_smem();
-    for (int grp = 0; grp < min(NS, ngroups); ++grp) issue(grp);
-  }
-
-  // ---- dx = x_i − x_memo in registers (x_i = scale * y_{i-1}, FP32) --------------------
-  float dx[R][E];
-  float yacc[R][E];
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      dx[r][e] = 0.f;
-      yacc[r][e] = 0.f;
-    }
-  double sum_dx = 0.0, zdx = 0.0;
-  if (!SETUP) {
-    const float* yprev = b.y[(a.iter + 1) & 1];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int vi = t + r * T;
-      if (vi < nvec) {
-#pragma unroll
-        for (int h = 0; h < E / 4; ++h) {
-          const float4 yp = reinterpret_cast<const float4*>(yprev)[vi * (E / 4) + h];
-          float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (amm) xm = reinterpret_cast<const float4*>(b.x_memo)[vi * (E / 4) + h];
-          dx[r][4 * h + 0] = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
-          dx[r][4 * h + 1] = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
-          dx[r][4 * h + 2] = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
-          dx[r][4 * h + 3] = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
-          if (centred) {
-            const float4 zz = reinterpret_cast<const float4*>(b.z)[vi * (E / 4) + h];
-            sum_dx += (double)dx[r][4 * h + 0] + (double)dx[r][4 * h + 1] +
-                      (double)dx[r][4 * h + 2] + (double)dx[r][4 * h + 3];
-            zdx = fma((double)dx[r][4 * h + 0], (double)zz.x, zdx);
-            zdx = fma((double)dx[r][4 * h + 1], (double)zz.y, zdx);
-            zdx = fma((double)dx[r][4 * h + 2], (double)zz.z, zdx);
-            zdx = fma((double)dx[r][4 * h + 3], (double)zz.w, zdx);
-          }
-        }
-      }
-    }
-    if (centred) {  // Σdx and z·dx (common.h:55-87), identical in every CTA
-      sum_dx = warp_sum(sum_dx);
-      zdx = warp_sum(zdx);
-      if (lane == 0) {
-        red64[2 * warp] = sum_dx;
-        red64[2 * warp + 1] = zdx;
-      }
-      __syncthreads();
-      sum_dx = 0.0;
-      zdx = 0.0;
-      for (int w = 0; w < nwarps; ++w) {
-        sum_dx += red64[2 * w];
-        zdx += red64[2 * w + 1];
-      }
-      __syncthreads();
-      if (bid == 0 && t == 0) {
-        b.st[a.iter & 1].sum_dx = sum_dx;
-        b.st[a.iter & 1].zdx = zdx;
-      }
-    }
-  }
-  const float sum_dx_f = (float)sum_dx;
-  const float* wts = b.wts[which];
-
-  float sacc = 0.f;     // Σ α_k t_k (proposed)
-  double a2acc = 0.0;   // Σ α_j² (set-up)
-  bool ok = true;
-
-  for (int grp = 0; grp < ngroups; ++grp) {
-    const int s = grp % NS;
-    const uint32_t parity = (uint32_t)((grp / NS) & 1);
-    const bool mbar_ok = mbar_wait_bounded(&bars[s], parity);
-    const int cnt = mbar_ok ? min(gc, nb - grp * gc) : 0;
-    const unsigned char* sbuf = stage_base + (size_t)s * g.stage_bytes;
-    const bool got = mbar_ok;
-    float d[kGcMax];
-    double s1[SETUP ? kGcMax : 1], s2[SETUP ? kGcMax : 1];
-#pragma unroll
-    for (int q = 0; q < kGcMax; ++q) d[q] = 0.f;
-#pragma unroll
-    for (int q = 0; q < (SETUP ? kGcMax : 1); ++q) {
-      s1[q] = 0.0;
-      s2[q] = 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < kGcMax; ++q) {
-      if (q < cnt) {
-        const uint4* col = reinterpret_cast<const uint4*>(sbuf + (size_t)q * g.colbytes);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int vi = t + r * T;
-          if (vi < nvec) {
-            float av[E];
-            unpack(col[vi], av);
-            if constexpr (SETUP) {
-#pragma unroll
-              for (int e = 0; e < E; ++e) {
-                s1[q] += (double)av[e];
-                s2[q] = fma((double)av[e], (double)av[e], s2[q]);
-              }
-            } else {
-#pragma unroll
-              for (int e = 0; e < E; ++e) d[q] = fmaf(av[e], dx[r][e], d[q]);
-            }
-          }
-        }
-      }
-    }
-    const int rb = grp & 1;
-    if constexpr (SETUP) {
-#pragma unroll
-      for (int q = 0; q < kGcMax; ++q) {
-        if (q < cnt) {
-          s1[q] = warp_sum(s1[q]);
-          s2[q] = warp_sum(s2[q]);
-          if (lane == 0) {
-            red64[((rb * 16 + warp) * kGcMax + q) * 2] = s1[q];
-            red64[((rb * 16 + warp) * kGcMax + q) * 2 + 1] = s2[q];
-          }
-        }
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < kGcMax; ++q) {
-        if (q < cnt) {
-          d[q] = warp_sum(d[q]);
-          if (lane == 0) red[(rb * 16 + warp) * kGcMax + q] = d[q];
-        }
-      }
-    }
-    // the barrier also makes a timed-out wait block-uniform
-    if (__syncthreads_or(got ? 0 : 1)) {
-      ok = false;
-      break;
-    }
-    // refill the stage consumed by the previous group (everyone has finished with it)
-    if (t == 0 && grp >= 1 && grp - 1 + NS < ngroups) issue(grp - 1 + NS);
-    float coef[kGcMax];
-#pragma unroll
-    for (int q = 0; q < kGcMax; ++q) {
-      coef[q] = 0.f;
-      if (q < cnt) {
-        const int k = grp * gc + q;
-        const uint32_t col = column_of(k);
-        if constexpr (SETUP) {
-          double ss = 0.0, qq = 0.0;
-          for (int w = 0; w < nwarps; ++w) {
-            ss += red64[((rb * 16 + w) * kGcMax + q) * 2];
-            qq += red64[((rb * 16 + w) * kGcMax + q) * 2 + 1];
-          }
-          const double mean = ss / (double)m;
-          const float af = (float)mean;
-          coef[q] = af;
-          a2acc = fma((double)af, (double)af, a2acc);
-          if (t == 0) {
-            b.alpha[col] = af;
-            b.norm[col] = (float)sqrt(qq);
-            b.normp[col] = (float)sqrt(fmax(qq - mean * mean * (double)m, 0.0));
-          }
-        } else {
-          float tot = 0.f;
-          for (int w = 0; w < nwarps; ++w) tot += red[(rb * 16 + w) * kGcMax + q];
-          if (!amm) {
-            coef[q] = tot;
-          } else {
-            const float wm = a.cc.sanity ? 1.0f : __fmul_rn(wts[col], (float)wl_mult[k]);
-            if (centred) {
-              const float al = b.alpha[col];
-              const float tq = __fmul_rn(__fsub_rn(tot, __fmul_rn(al, sum_dx_f)), wm);
-              coef[q] = tq;
-              sacc = fmaf(al, tq, sacc);
-            } else {
-              coef[q] = __fmul_rn(tot, wm);
-            }
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kGcMax; ++q) {
-      if (q < cnt) {
-        const uint4* col = reinterpret_cast<const uint4*>(sbuf + (size_t)q * g.colbytes);
-        const float cq = coef[q];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int vi = t + r * T;
-          if (vi < nvec) {
-            float av[E];
-            unpack(col[vi], av);
-#pragma unroll
-            for (int e = 0; e < E; ++e) yacc[r][e] = fmaf(cq, av[e], yacc[r][e]);
-          }
-        }
-      }
-    }
-  }
-
-  if (!ok) {
-    if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
-    return;
-  }
-
-  float* part = b.partials + (size_t)bid * m;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int vi = t + r * T;
-    if (vi < nvec) {
-#pragma unroll
-      for (int h = 0; h < E / 4; ++h)
-        reinterpret_cast<float4*>(part)[vi * (E / 4) + h] =
-            make_float4(yacc[r][4 * h], yacc[r][4 * h + 1], yacc[r][4 * h + 2], yacc[r][4 * h + 3]);
-    }
-  }
-  if (t == 0) {
-    b.spart[bid] = sacc;
-    b.spart64[bid] = a2acc;
-  }
+  uint32_t* cnt = b.count[pb];
+  const uint32_t* smp = b.samples[pb];
+  for (int k = tid; k < b.c; k += nthr) cnt[smp[k]] = 0u;
+  for (int k = tid; k < b.nchunks; k += nthr) b.chunk[pb][k] = 0u;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -672,13 +180,33 @@ __device__ __forceinline__ void reduce_rows(const Buffers& b, int row, double4 (
   const int rg = threadIdx.x & 31, ps = threadIdx.x >> 5;
   double4 acc = make_double4(0, 0, 0, 0);
   if (row < b.m) {
-    for (int k = ps; k < b.nsm; k += 8) {
-      const float4 p = *reinterpret_cast<const float4*>(b.partials + (size_t)k * b.m + row);
-      acc.x += p.x;
-      acc.y += p.y;
-      acc.z += p.z;
-      acc.w += p.w;
+    // two independent accumulators over partials ps, ps+8, ps+16, ... (a fixed order)
+    double4 acc1 = make_double4(0, 0, 0, 0);
+    const float* __restrict__ P = b.partials + row;
+    int k = ps;
+    for (; k + 8 < b.nsm; k += 16) {
+      const float4 p0 = __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * b.m));
+      const float4 p1 = __ldcg(reinterpret_cast<const float4*>(P + (size_t)(k + 8) * b.m));
+      acc.x += p0.x;
+      acc.y += p0.y;
+      acc.z += p0.z;
+      acc.w += p0.w;
+      acc1.x += p1.x;
+      acc1.y += p1.y;
+      acc1.z += p1.z;
+      acc1.w += p1.w;
     }
+    if (k < b.nsm) {
+      const float4 p0 = __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * b.m));
+      acc.x += p0.x;
+      acc.y += p0.y;
+      acc.z += p0.z;
+      acc.w += p0.w;
+    }
+    acc.x += acc1.x;
+    acc.y += acc1.y;
+    acc.z += acc1.z;
+    acc.w += acc1.w;
   }
   red[ps][rg] = acc;
   __syncthreads();
@@ -719,6 +247,19 @@ __global__ void __launch_bounds__(kRedThreads) setup_reduce_kernel(const __grid_
   if (blockIdx.x == 0 && t == 0) *b.alpha2 = a2;
 }
 
+// Per-column statistics from the set-up pass's FP64 column sums (get_norms,
+// device_memory.h:34-59): α = Σ/m, ‖A_j‖ = sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² − mean²·m) clamped
+// at 0 (the reference stores NaN when cancellation makes it negative).
+__global__ void __launch_bounds__(256) column_stats_kernel(const __grid_constant__ Buffers b) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < b.n; j += gridDim.x * blockDim.x) {
+    const double2 s = b.colsum[j];
+    const double mean = s.x / (double)b.m;
+    b.alpha[j] = (float)mean;
+    b.norm[j] = (float)sqrt(s.y);
+    b.normp[j] = (float)sqrt(fmax(s.y - mean * mean * (double)b.m, 0.0));
+  }
+}
+
 struct ReduceArgs {
   Buffers b;
   CallCfg cc;
@@ -739,12 +280,9 @@ __global__ void __launch_bounds__(kRedThreads) reduce_kernel(const __grid_consta
   const bool consumed = (st.mode == kPrevious || st.mode == kProposed);
 
   if ((int)blockIdx.x >= a.nred) {
-    // draw the picks of the next AMM step while the sums are reduced
-    if (consumed && !cc.sanity) {
-      const int which = next_amm_weighting(cc, a.iter);
-      sampling_role(b, which, st.pb, st.sb ^ 1, st.pb ^ 1, blockIdx.x - a.nred,
-                    gridDim.x - a.nred, a.iter + 1 < cc.step);
-    }
+    // the picks this step consumed are cleared while the sums are reduced (the next picks were
+    // drawn into the other buffer by sample_kernel, concurrently with the product)
+    if (consumed && !cc.sanity) clear_picks(b, st.pb, blockIdx.x - a.nred, gridDim.x - a.nred);
     return;
   }
 
@@ -819,16 +357,20 @@ __global__ void __launch_bounds__(kRedThreads) reduce_kernel(const __grid_consta
     }
   }
   __syncthreads();
-  if (!is_last || t != 0) return;
+  if (!is_last || t >= 32) return;
   __threadfence();
-  // last CTA: Rayleigh quotient and the next step (common.h:103-153)
+  // last CTA: Rayleigh quotient and the next step (common.h:103-153).  Warp 0 sums the CTA
+  // partials lane-strided and then by an xor butterfly: a fixed association order.
   double xy = 0.0, yy = 0.0, yv = 0.0;
-  const volatile double* rp = b.rpart;
-  for (int k = 0; k < a.nred; ++k) {
-    xy += rp[4 * k + 0];
-    yy += rp[4 * k + 1];
-    yv += rp[4 * k + 2];
+  for (int k = t; k < a.nred; k += 32) {
+    xy += __ldcg(b.rpart + 4 * k + 0);
+    yy += __ldcg(b.rpart + 4 * k + 1);
+    yv += __ldcg(b.rpart + 4 * k + 2);
   }
+  xy = warp_sum(xy);
+  yy = warp_sum(yy);
+  yv = warp_sum(yv);
+  if (t != 0) return;
   b.ticket[0] = 0u;
   const double scale = rsqrt(yy);
   const double lam = xy;
@@ -864,6 +406,42 @@ __global__ void __launch_bounds__(kRedThreads) reduce_kernel(const __grid_consta
 }
 
 // ------------------------------------------------------------------------------------------
+// Sampling (pick_index, device_memory.h:516-545), one sample per thread
+// ------------------------------------------------------------------------------------------
+struct SampleArgs {
+  Buffers b;
+  CallCfg cc;
+  int iter;     // draw the picks of the first AMM step after step `iter` (-1: start of a call)
+};
+
+// For iter >= 0 this runs concurrently with the product of step iter: if that step consumes
+// its picks (an AMM step), the next picks are drawn from the advanced states states[sb^1] into
+// the other buffer (count[pb^1], states[sb]); otherwise the pending picks stay valid and
+// nothing is drawn.  For iter = -1 the first picks are drawn from states[0].
+template <typename F>
+__global__ void __launch_bounds__(256) sample_kernel(const __grid_constant__ SampleArgs a) {
+  __shared__ __align__(16) F coarse_s[kCoarseMax];
+  const Buffers& b = a.b;
+  const CallCfg& cc = a.cc;
+  int sb_in, pb_out;
+  if (a.iter < 0) {
+    sb_in = 0;
+    pb_out = 0;
+  } else {
+    const IterState& st = b.st[a.iter & 1];
+    const bool consumes = st.mode == kPrevious || st.mode == kProposed;
+    if (st.done || !consumes || a.iter + 1 >= cc.step) return;  // uniform over the grid
+    sb_in = st.sb ^ 1;
+    pb_out = st.pb ^ 1;
+  }
+  const int which = next_amm_weighting(cc, a.iter);
+  load_coarse<F>(b, which, coarse_s);
+  draw_samples<F>(b, which, b.states[sb_in], b.states[sb_in ^ 1], b.count[pb_out],
+                  b.chunk[pb_out], b.samples[pb_out], blockIdx.x * blockDim.x + threadIdx.x,
+                  gridDim.x * blockDim.x, coarse_s);
+}
+
+// ------------------------------------------------------------------------------------------
 // Call start / end
 // ------------------------------------------------------------------------------------------
 struct InitArgs {
@@ -873,21 +451,29 @@ struct InitArgs {
   int no_normalize;
 };
 
-__global__ void __launch_bounds__(kRedThreads) init_kernel(const __grid_constant__ InitArgs a) {
+__global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ InitArgs a) {
   const Buffers& b = a.b;
   const CallCfg& cc = a.cc;
   const int t = threadIdx.x;
-  if (blockIdx.x > 0) {
-    if (cc.uses_amm && !cc.sanity)
-      sampling_role(b, next_amm_weighting(cc, -1), -1, 0, 0, blockIdx.x - 1, gridDim.x - 1, true);
-    return;
-  }
-  __shared__ double ws[kRedThreads / 32];
+  __shared__ double ws[32];
+  const float* __restrict__ x0 = a.x0;
+  float* __restrict__ y1 = b.y[1];
   double ss = 0.0;
-  for (int k = t; k < b.m; k += blockDim.x) {
-    const float v = a.x0[k];
-    b.y[1][k] = v;
-    ss = fma((double)v, (double)v, ss);
+  // a call starts from a zero memo pair, as the reference's zero_clear (device_memory.h:
+  // 345-355, called first by every powerMethod_by_*); the single-product entry points keep
+  // the memo their caller supplied
+  const bool clear_memo = !a.no_normalize;
+  for (int k0 = 4 * t; k0 < b.m; k0 += 4 * blockDim.x) {  // m % 4 == 0
+    const float4 v = __ldg(reinterpret_cast<const float4*>(x0 + k0));
+    *reinterpret_cast<float4*>(y1 + k0) = v;
+    if (clear_memo) {
+      *reinterpret_cast<float4*>(b.x_memo + k0) = make_float4(0.f, 0.f, 0.f, 0.f);
+      *reinterpret_cast<float4*>(b.y_memo + k0) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    ss = fma((double)v.x, (double)v.x, ss);
+    ss = fma((double)v.y, (double)v.y, ss);
+    ss = fma((double)v.z, (double)v.z, ss);
+    ss = fma((double)v.w, (double)v.w, ss);
   }
   ss = warp_sum(ss);
   if ((t & 31) == 0) ws[t >> 5] = ss;
@@ -945,82 +531,148 @@ __global__ void __launch_bounds__(kRedThreads) finalize_kernel(const __grid_cons
 }
 
 // ------------------------------------------------------------------------------------------
-// CDF construction (once per matrix)
+// CDF construction (once per matrix): tile sums, then tile scans with the ordered prefix of the
+// preceding tiles (deterministic association).  FP64 mode: weight_j = (double)norm_j²; FP32
+// mode: weight_j = fl32(norm_j²) as set_weights (common.h:34-40) and the CDF is fl32 of the
+// FP64 prefix.  Then w_j = total/(weight_j·c) (update_weights, common.h:42-53) and the coarse
+// table of the sampler.
 // ------------------------------------------------------------------------------------------
-constexpr int kCdfThreads = 1024;
-constexpr int kCdfTile = 4096;
+constexpr int kCdfThreads = 256;
+constexpr int kCdfPer = 16;
+constexpr int kCdfTile = kCdfThreads * kCdfPer;
 
-// blockIdx.x selects the weighting (or `which` when >= 0).  FP64 mode: weight_j =
-// (double)norm_j², CDF = FP64 inclusive prefix.  FP32 mode: weight_j = fl32(norm_j²) as
-// set_weights (common.h:34-40); CDF = fl32 of the FP64 prefix of those weights.  Then
-// w_j = total/(weight_j·c) (update_weights, common.h:42-53) and the coarse table.
-__global__ void __launch_bounds__(kCdfThreads) build_cdf_kernel(const __grid_constant__ Buffers b,
-                                                                int which_in, int keep_cdf,
-                                                                int sanity) {
-  __shared__ double tile[kCdfTile];
-  __shared__ double wsum[32];
-  __shared__ double carry_s;
-  const int which = which_in >= 0 ? which_in : (int)blockIdx.x;
-  const float* base = which == 0 ? b.norm : b.normp;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int n = b.n;
-  constexpr int PER = kCdfTile / kCdfThreads;
-  if (!keep_cdf) {
-    double carry = 0.0;
-    for (int t0 = 0; t0 < n; t0 += kCdfTile) {
-      for (int k = t; k < kCdfTile; k += kCdfThreads) {
-        const int j = t0 + k;
-        double w = 0.0;
-        if (j < n) {
-          const float nv = base[j];
-          w = sanity ? 1.0 : (b.cdf_f32 ? (double)__fmul_rn(nv, nv) : (double)nv * (double)nv);
-        }
-        tile[k] = w;
-      }
-      __syncthreads();
-      double loc = 0.0;
+
+// Block-wide exclusive scan of one double per thread (kCdfThreads threads); total in *total.
+__device__ double block_exclusive_scan_f64(double v, double* ws, double* total) {
+  // ws: >= 33 doubles
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int nw = kCdfThreads / 32;
+  double incl = v;
 #pragma unroll
-      for (int e = 0; e < PER; ++e) loc += tile[t * PER + e];
-      double incl = loc;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) ws[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const double w = lane < nw ? ws[lane] : 0.0;
+    double wi = w;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const double y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      if (lane == 31) wsum[warp] = incl;
-      __syncthreads();
-      if (warp == 0) {
-        const double w = wsum[lane];
-        double wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const double y = __shfl_up_sync(0xffffffffu, wi, o);
-          if (lane >= o) wi += y;
-        }
-        wsum[lane] = wi - w;
-        if (lane == 31) carry_s = wi;
-      }
-      __syncthreads();
-      double run = carry + wsum[warp] + (incl - loc);
-#pragma unroll
-      for (int e = 0; e < PER; ++e) {
-        const int j = t0 + t * PER + e;
-        run += tile[t * PER + e];
-        if (j < n) {
-          if (b.cdf_f32)
-            b.cdf32[which][j] = (float)run;
-          else
-            b.cdf64[which][j] = run;
-        }
-      }
-      carry += carry_s;
-      __syncthreads();
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
     }
+    if (lane < nw) ws[lane] = wi - w;
+    if (lane == nw - 1) ws[32] = wi;
   }
   __syncthreads();
-  const double total64 = b.cdf_f32 ? (double)b.cdf32[which][n - 1] : b.cdf64[which][n - 1];
-  const float total32 = b.cdf_f32 ? b.cdf32[which][n - 1] : (float)total64;
-  for (int j = t; j < n; j += kCdfThreads) {
+  const double r = ws[warp] + (incl - v);
+  *total = ws[32];
+  __syncthreads();
+  return r;
+}
+
+// Local (within-tile) inclusive prefix of this thread's kCdfPer weights and the tile total,
+// computed identically by both CDF kernels: a thread-sequential sum, a block scan of the thread
+// sums, then thread-sequential accumulation.  The tile total is the last local prefix value,
+// so cdf = pre_tile + local_prefix is non-decreasing across tile boundaries as well.
+__device__ void tile_local_prefix(const Buffers& b, const float* base, int t0, int sanity,
+                                  double (&lp)[kCdfPer], double* tile_total, double* ws,
+                                  float* tile) {
+  const float* __restrict__ src = base;
+#pragma unroll 4
+  for (int k = threadIdx.x; k < kCdfTile; k += kCdfThreads) {
+    const int j = t0 + k;
+    tile[k] = j < b.n ? __ldg(src + j) : 0.f;
+  }
+  __syncthreads();
+  double w[kCdfPer];
+  double loc = 0.0;
+#pragma unroll
+  for (int e = 0; e < kCdfPer; ++e) {
+    const int k = threadIdx.x * kCdfPer + e;
+    const float nv = tile[k];
+    w[e] = (t0 + k < b.n)
+               ? (sanity ? 1.0 : (b.cdf_f32 ? (double)__fmul_rn(nv, nv) : (double)nv * (double)nv))
+               : 0.0;
+    loc += w[e];
+  }
+  double unused;
+  double run = block_exclusive_scan_f64(loc, ws, &unused);
+#pragma unroll
+  for (int e = 0; e < kCdfPer; ++e) {
+    run += w[e];
+    lp[e] = run;
+  }
+  if (threadIdx.x == kCdfThreads - 1) ws[33] = run;
+  __syncthreads();
+  *tile_total = ws[33];
+  __syncthreads();
+}
+
+// grid (ntiles, weightings): the total of each tile
+__global__ void __launch_bounds__(kCdfThreads) cdf_tile_sums_kernel(const __grid_constant__ Buffers b,
+                                                                   int which0, int sanity) {
+  __shared__ double ws[34];
+  __shared__ float tile[kCdfTile];
+  const int which = which0 + blockIdx.y;
+  const float* base = which == 0 ? b.norm : b.normp;
+  double lp[kCdfPer], tot;
+  tile_local_prefix(b, base, blockIdx.x * kCdfTile, sanity, lp, &tot, ws, tile);
+  if (threadIdx.x == 0) b.cdf_tsum[which * gridDim.x + blockIdx.x] = tot;
+}
+
+// grid (ntiles, weightings): CDF of each tile (unless imported), weights w_j
+__global__ void __launch_bounds__(kCdfThreads) cdf_scan_kernel(const __grid_constant__ Buffers b,
+                                                               int which0, int keep_cdf, int sanity) {
+  __shared__ double ws[34];
+  __shared__ float tile[kCdfTile];
+  __shared__ double pre_s, total_s;
+  const int which = which0 + blockIdx.y;
+  const float* base = which == 0 ? b.norm : b.normp;
+  const int ntiles = gridDim.x;
+  const int t0 = blockIdx.x * kCdfTile;
+  const int n = b.n;
+  double total64;
+  if (!keep_cdf) {
+    // prefixes and the total summed sequentially in tile order (identical in every block);
+    // the tile sums are first staged in shared memory by all threads
+    double* ts = reinterpret_cast<double*>(tile);  // reused before the tile is loaded
+    const int nts = ntiles < kCdfTile / 2 ? ntiles : kCdfTile / 2;
+    for (int k = threadIdx.x; k < nts; k += kCdfThreads) ts[k] = __ldcg(b.cdf_tsum + which * ntiles + k);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double acc = 0.0, pre = 0.0;
+      for (int k = 0; k < ntiles; ++k) {
+        if (k == (int)blockIdx.x) pre = acc;
+        acc += k < nts ? ts[k] : __ldcg(b.cdf_tsum + which * ntiles + k);
+      }
+      pre_s = pre;
+      total_s = acc;
+    }
+    __syncthreads();
+    double lp[kCdfPer], tot;
+    tile_local_prefix(b, base, t0, sanity, lp, &tot, ws, tile);
+    const double pre = pre_s;
+#pragma unroll
+    for (int e = 0; e < kCdfPer; ++e) {
+      const int j = t0 + threadIdx.x * kCdfPer + e;
+      if (j < n) {
+        if (b.cdf_f32)
+          b.cdf32[which][j] = (float)(pre + lp[e]);
+        else
+          b.cdf64[which][j] = pre + lp[e];
+      }
+    }
+    total64 = total_s;
+  } else {
+    total64 = b.cdf_f32 ? (double)b.cdf32[which][n - 1] : b.cdf64[which][n - 1];
+  }
+  const float total32 = b.cdf_f32 ? (float)total64 : 0.f;
+  for (int k = threadIdx.x; k < kCdfTile; k += kCdfThreads) {
+    const int j = t0 + k;
+    if (j >= n) break;
     const float nv = base[j];
     float w;
     if (b.cdf_f32) {
@@ -1032,15 +684,21 @@ __global__ void __launch_bounds__(kCdfThreads) build_cdf_kernel(const __grid_con
     }
     b.wts[which][j] = w;
   }
-  for (int s = t; s < b.ncoarse; s += kCdfThreads) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (!(total64 > 0.0) || !isfinite(total64)))
+    atomicOr(b.status, (uint32_t)kDevNonFinite);
+}
+
+// coarse table (after the CDF is complete)
+__global__ void __launch_bounds__(256) cdf_coarse_kernel(const __grid_constant__ Buffers b,
+                                                         int which0) {
+  const int which = which0 + blockIdx.y;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.ncoarse; s += gridDim.x * blockDim.x) {
     const int j = (s + 1) * b.seg - 1;
     if (b.cdf_f32)
       b.coarse32[which][s] = b.cdf32[which][j];
     else
       b.coarse64[which][s] = b.cdf64[which][j];
   }
-  if (t == 0 && (!(total64 > 0.0) || !isfinite(total64)))
-    atomicOr(b.status, (uint32_t)kDevNonFinite);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1180,105 +838,34 @@ __global__ void __launch_bounds__(256) grad_outer_kernel(const float* v, const f
 // ------------------------------------------------------------------------------------------
 // Host launchers
 // ------------------------------------------------------------------------------------------
-bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
-  const int es = dtype == 1 ? 2 : 4;
-  const int E = 16 / es;
-  if (m <= 0 || m % E != 0) return false;
-  const int nvec = m / E;
-  int R = 1;
-  while (R < 8 && (nvec + R - 1) / R > kMaxThreads) R <<= 1;
-  if ((nvec + R - 1) / R > kMaxThreads) return false;
-  if (R * E > 32) return false;  // register budget: 32 rows per thread
-  int threads = ((nvec + R - 1) / R + 31) / 32 * 32;
-  g->threads = threads;
-  g->slots = R;
-  g->elems = E;
-  g->colbytes = m * es;
-  const int budget = 200 * 1024;
-  int target_stage = 48 * 1024;
-  int gc = target_stage / g->colbytes;
-  if (gc < 1) gc = 1;
-  if (gc > kGcMax) gc = kGcMax;
-  int stage = gc * g->colbytes;
-  int ns = budget / stage;
-  if (ns > 6) ns = 6;
-  if (ns < 2) {
-    ns = 2;
-    gc = 1;
-    stage = g->colbytes;
-    if (2 * stage > budget) return false;
-  }
-  g->gc = gc;
-  g->nstages = ns;
-  g->stage_bytes = stage;
-  int maxlist = c < n ? c : n;
-  int wl = (maxlist + nsm - 1) / nsm + 1;
-  g->wl_cap = wl;
-  // the stage area doubles as scratch for the per-chunk prefix (<= 4096 uint32) before the
-  // pipeline starts
-  g->stage_area = ns * stage > 4 * 4096 ? ns * stage : 4 * 4096;
-  g->smem_bytes = g->stage_area + 8 * 8 + 4096 + 2 * wl * 4 + 40 * 4;
-  return g->smem_bytes <= 227 * 1024;
-}
-
-template <typename Elem, int R>
-static cudaError_t launch_panel_t(const PanelArgs& a, cudaStream_t s) {
-  auto k = a.setup ? panel_kernel<Elem, R, true> : panel_kernel<Elem, R, false>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       a.g.smem_bytes);
-  if (e != cudaSuccess) return e;
-  k<<<a.b.nsm, a.g.threads, a.g.smem_bytes, s>>>(a);
-  count_launch();
-  return cudaGetLastError();
-}
-
-static cudaError_t launch_panel(const PanelArgs& a, cudaStream_t s) {
-  const bool bf = a.b.dtype == 1;
-  switch (a.g.slots) {
-    case 1: return bf ? launch_panel_t<__nv_bfloat16, 1>(a, s) : launch_panel_t<float, 1>(a, s);
-    case 2: return bf ? launch_panel_t<__nv_bfloat16, 2>(a, s) : launch_panel_t<float, 2>(a, s);
-    case 4: return bf ? launch_panel_t<__nv_bfloat16, 4>(a, s) : launch_panel_t<float, 4>(a, s);
-    case 8: return launch_panel_t<float, 8>(a, s);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-cudaError_t launch_setup_panel(const Buffers& b, const PanelGeom& g, cudaStream_t s) {
-  PanelArgs a{};
-  a.b = b;
-  a.g = g;
-  a.iter = 0;
-  a.setup = 1;
-  return launch_panel(a, s);
-}
-
-cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
-                              cudaStream_t s) {
-  PanelArgs a{};
-  a.b = b;
-  a.g = g;
-  a.cc = cc;
-  a.iter = iter;
-  a.setup = 0;
-  return launch_panel(a, s);
-}
-
 static int reduce_ctas(int m) { return (m + kRedRows - 1) / kRedRows; }
-static int sample_ctas(int c) {
+static int clear_ctas(int c) {
   int k = (c + kRedThreads * 4 - 1) / (kRedThreads * 4);
   return k < 1 ? 1 : (k > 64 ? 64 : k);
 }
 
 cudaError_t launch_setup_reduce(const Buffers& b, cudaStream_t s) {
   setup_reduce_kernel<<<reduce_ctas(b.m), kRedThreads, 0, s>>>(b);
-  count_launch();
+  int blocks = (b.n + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  column_stats_kernel<<<blocks, 256, 0, s>>>(b);
+  count_launch(2);
   return cudaGetLastError();
 }
 
 cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sanity,
                              cudaStream_t s) {
-  build_cdf_kernel<<<which >= 0 ? 1 : 2, kCdfThreads, 0, s>>>(b, which, keep_cdf, sanity);
-  count_launch();
+  const int ntiles = (b.n + kCdfTile - 1) / kCdfTile;
+  const dim3 grid(ntiles, which >= 0 ? 1 : 2);
+  const int w0 = which >= 0 ? which : 0;
+  if (!keep_cdf) {
+    cdf_tile_sums_kernel<<<grid, kCdfThreads, 0, s>>>(b, w0, sanity);
+    count_launch();
+  }
+  cdf_scan_kernel<<<grid, kCdfThreads, 0, s>>>(b, w0, keep_cdf, sanity);
+  const int cb = (b.ncoarse + 255) / 256;
+  cdf_coarse_kernel<<<dim3(cb > 0 ? cb : 1, grid.y), 256, 0, s>>>(b, w0);
+  count_launch(2);
   return cudaGetLastError();
 }
 
@@ -1289,8 +876,7 @@ cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, in
   a.cc = cc;
   a.x0 = x0;
   a.no_normalize = no_normalize;
-  const int ns = (cc.uses_amm && !cc.sanity) ? sample_ctas(b.c) : 0;
-  init_kernel<<<1 + ns, kRedThreads, 0, s>>>(a);
+  init_kernel<<<1, 1024, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }
@@ -1301,8 +887,23 @@ cudaError_t launch_iter_reduce(const Buffers& b, const CallCfg& cc, int iter, cu
   a.cc = cc;
   a.iter = iter;
   a.nred = reduce_ctas(b.m);
-  const int ns = (cc.uses_amm && !cc.sanity) ? sample_ctas(b.c) : 0;
+  const int ns = (cc.uses_amm && !cc.sanity) ? clear_ctas(b.c) : 0;
   reduce_kernel<<<a.nred + ns, kRedThreads, 0, s>>>(a);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s) {
+  SampleArgs a{};
+  a.b = b;
+  a.cc = cc;
+  a.iter = iter;
+  int blocks = (b.c + 255) / 256;
+  if (blocks > 1024) blocks = 1024;
+  if (b.cdf_f32)
+    sample_kernel<float><<<blocks, 256, 0, s>>>(a);
+  else
+    sample_kernel<double><<<blocks, 256, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }

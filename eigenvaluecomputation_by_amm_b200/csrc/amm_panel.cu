@@ -1,0 +1,671 @@
+// The fused single-pass product kernel of libamm (sm_100a):
+//
+//   y_part = Σ_{k in this CTA's columns} coef_k · A_k,   coef_k = f(A_kᵀ·dx)
+//
+// for one power-method step (all n columns for an exact step, the distinct sampled columns for
+// an AMM step) and for the set-up pass (coef_j = α_j, plus FP64 column statistics).
+//
+// One persistent CTA per SM owns a contiguous range of the column list and all m rows.  A
+// producer warp streams the columns, GC per group, into a ring of NS shared-memory stages with
+// 1-D TMA bulk copies (mbarrier complete_tx; measured on B200: >= 64 KB in flight per SM
+// saturates HBM).  The consumer warps hold dx and their share of y in registers; per group they
+//   1. form the coefficients of group g from the warp partials published at the last barrier,
+//   2. compute the partial dots of group g+1 (their rows),
+//   3. accumulate coef·A_k of group g into y (packed FP32x2 FMAs),
+//   4. warp-reduce and publish the dots of g+1, then meet at one named barrier,
+// so the reduction latency of a group hides behind the next group's math and there is one
+// barrier per group.  Each column is read from HBM once (the reference's kernel1/kernel2 read
+// it twice).  Each CTA writes one partial y; reduce_kernel sums them in a fixed order.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdlib>
+
+#include "amm_device.cuh"
+#include "amm_internal.h"
+
+namespace amm {
+
+struct PanelArgs {
+  Buffers b;
+  PanelGeom g;
+  CallCfg cc;
+  int iter;
+};
+
+template <bool SETUP>
+struct RedT {
+  using T = float;
+};
+template <>
+struct RedT<true> {
+  using T = double2;  // (Σa, Σa²)
+};
+
+__device__ __forceinline__ float red_add(float a, float b) { return a + b; }
+__device__ __forceinline__ double2 red_add(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ float red_zero(float) { return 0.f; }
+__device__ __forceinline__ double2 red_zero(double2) { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ float warp_red(float v) { return warp_sum(v); }
+__device__ __forceinline__ double2 warp_red(double2 v) {
+  return make_double2(warp_sum(v.x), warp_sum(v.y));
+}
+
+// Shared memory carve (byte offsets), identical on host and device.
+struct SmemLayout {
+  int stages, bars, redw, wl_idx, wl_w, wl_al, scan, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup) {
+  SmemLayout L{};
+  const int rsz = setup ? 16 : 4;
+  int o = 0;
+  L.stages = o;
+  o += g.stage_area;
+  L.bars = o;  // full[8] empty[8]
+  o += 8 * 16;
+  L.redw = o;  // [2][16 warps][GC]; also 16 x 2 doubles of prologue scratch
+  int rw = 2 * 16 * g.gc * rsz;
+  if (rw < 16 * 16) rw = 16 * 16;
+  o += rw;
+  L.wl_idx = o;
+  o += 4 * g.wl_cap;
+  L.wl_w = o;
+  o += 4 * g.wl_cap;
+  L.wl_al = o;
+  o += 4 * g.wl_cap;
+  L.scan = o;
+  o += 4 * 40;
+  L.total = (o + 127) & ~127;
+  return L;
+}
+
+// Packed FP32x2 arithmetic (Blackwell): two IEEE-rounded FMAs per instruction.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 xa, xb, xc;\n\t"
+      "mov.b64 xa, {%2, %3};\n\tmov.b64 xb, {%4, %5};\n\tmov.b64 xc, {%6, %7};\n\t"
+      "fma.rn.f32x2 xc, xa, xb, xc;\n\tmov.b64 {%0, %1}, xc;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+// 16-byte vector -> E/2 float2 (exact for BF16: the 16 bits become the high half).
+__device__ __forceinline__ void unpack2(const uint4& v, float2 (&o)[2]) {
+  o[0] = make_float2(__uint_as_float(v.x), __uint_as_float(v.y));
+  o[1] = make_float2(__uint_as_float(v.z), __uint_as_float(v.w));
+}
+__device__ __forceinline__ void unpack2(const uint4& v, float2 (&o)[4]) {
+  o[0] = make_float2(__uint_as_float(v.x << 16), __uint_as_float(v.x & 0xffff0000u));
+  o[1] = make_float2(__uint_as_float(v.y << 16), __uint_as_float(v.y & 0xffff0000u));
+  o[2] = make_float2(__uint_as_float(v.z << 16), __uint_as_float(v.z & 0xffff0000u));
+  o[3] = make_float2(__uint_as_float(v.w << 16), __uint_as_float(v.w & 0xffff0000u));
+}
+
+// Branch-free body of one full group: the axpy of group g (stage `cur`, coefficients `coef`)
+// interleaved, slot by slot, with the partial dots of group g+1 (stage `nxt`) when NEXT.  Used
+// when every column of both groups is present and every vector slot of every thread is valid.
+template <typename Elem, int R, int GC, bool NEXT>
+__device__ __forceinline__ void fused_block(const unsigned char* cur, const unsigned char* nxt,
+                                            uint32_t col_bytes, int t, int T,
+                                            const float (&coef)[GC],
+                                            const float2 (&dx)[R][8 / sizeof(Elem)],
+                                            float2 (&yacc)[R][8 / sizeof(Elem)], float (&dn)[GC]) {
+  constexpr int H = 8 / sizeof(Elem);
+  float2 p[GC];
+#pragma unroll
+  for (int qq = 0; qq < GC; ++qq) p[qq] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int vi = t + r * T;
+    uint4 vc[GC], vn[GC];
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      vc[qq] = reinterpret_cast<const uint4*>(cur + (size_t)qq * col_bytes)[vi];
+      if (NEXT) vn[qq] = reinterpret_cast<const uint4*>(nxt + (size_t)qq * col_bytes)[vi];
+    }
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      float2 ac[H];
+      unpack2(vc[qq], ac);
+      const float2 c2 = make_float2(coef[qq], coef[qq]);
+#pragma unroll
+      for (int h = 0; h < H; ++h) yacc[r][h] = fma2(c2, ac[h], yacc[r][h]);
+      if (NEXT) {
+        float2 an[H];
+        unpack2(vn[qq], an);
+#pragma unroll
+        for (int h = 0; h < H; ++h) p[qq] = fma2(an[h], dx[r][h], p[qq]);
+      }
+    }
+  }
+#pragma unroll
+  for (int qq = 0; qq < GC; ++qq) dn[qq] = p[qq].x + p[qq].y;
+}
+
+template <typename Elem, int R, int GC, bool SETUP>
+__global__ void __launch_bounds__(kMaxThreads + 32, 1)
+    panel_kernel(const __grid_constant__ PanelArgs a) {
+  using RT = typename RedT<SETUP>::T;
+  constexpr int E = 16 / static_cast<int>(sizeof(Elem));
+  constexpr int H = E / 2;  // float2 per vector
+  const Buffers& b = a.b;
+  const PanelGeom& g = a.g;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int T = blockDim.x - 32;              // consumer threads
+  const int ncw = T >> 5;                     // consumer warps
+  const int G = gridDim.x;
+  const int q = blockIdx.x;
+  const int m = b.m;
+  const int nvec = m / E;
+  const int NS = g.nstages;
+  const uint32_t col_bytes = (uint32_t)(m * sizeof(Elem));
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  const SmemLayout L = smem_layout(g, SETUP);
+  unsigned char* stages = smem + L.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
+  uint64_t* empty = full + 8;
+  RT* redw = reinterpret_cast<RT*>(smem + L.redw);
+  uint32_t* wl_idx = reinterpret_cast<uint32_t*>(smem + L.wl_idx);
+  float* wl_w = reinterpret_cast<float*>(smem + L.wl_w);
+  float* wl_al = reinterpret_cast<float*>(smem + L.wl_al);
+  uint32_t* scan = reinterpret_cast<uint32_t*>(smem + L.scan);
+
+  int mode = kExact, pb = 0, done = 0;
+  float scale = 0.f;
+  if (!SETUP) {
+    const IterState& st = b.st[a.iter & 1];
+    done = st.done;
+    mode = st.mode;
+    pb = st.pb;
+    scale = st.scale;
+  }
+  if (done) return;  // uniform over the grid
+  const bool amm = !SETUP && (mode == kPrevious || mode == kProposed);
+  const bool centred = !SETUP && mode == kProposed;
+  const bool sampled = amm && !a.cc.sanity;
+  const int which = centred ? 1 : 0;
+
+  if (t == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    fence_barrier_init();
+  }
+
+  // ---- this CTA's column list -------------------------------------------------------------
+  int64_t lo, hi;
+  if (!sampled) {
+    lo = (int64_t)q * b.n / G;
+    hi = (int64_t)(q + 1) * b.n / G;
+  } else {
+    uint32_t* cpre = reinterpret_cast<uint32_t*>(stages);  // scratch before the pipeline starts
+    const uint32_t* chunk = b.chunk[pb];
+    uint32_t carry = 0;
+    for (int base = 0; base < b.nchunks; base += blockDim.x) {
+      const int k = base + t;
+      const uint32_t v = k < b.nchunks ? chunk[k] : 0u;
+      uint32_t tot;
+      const uint32_t ex = block_exclusive_scan(v, scan, &tot);
+      if (k < b.nchunks) cpre[k] = carry + ex;
+      carry += tot;
+    }
+    __syncthreads();
+    const uint32_t cd = carry;
+    lo = (int64_t)q * cd / G;
+    hi = (int64_t)(q + 1) * cd / G;
+    if (q == 0 && t == 0) b.distinct_hist[a.iter] = (int32_t)cd;
+    if (hi > lo) {
+      int ka = 0, kb = b.nchunks - 1;  // largest k with cpre[k] <= lo
+      while (ka < kb) {
+        const int mid = (ka + kb + 1) >> 1;
+        if (cpre[mid] <= (uint32_t)lo)
+          ka = mid;
+        else
+          kb = mid - 1;
+      }
+      const uint32_t* cnt = b.count[pb];
+      const float* wts = b.wts[which];
+      const int CH = 1 << b.chunk_shift;
+      for (int kc = ka; kc < b.nchunks && cpre[kc] < (uint32_t)hi; ++kc) {
+        uint32_t rank0 = cpre[kc];
+        const int start = kc << b.chunk_shift;
+        const int len = min(CH, b.n - start);
+        for (int p0 = 0; p0 < len; p0 += blockDim.x) {
+          const int p = p0 + t;
+          const uint32_t mult = p < len ? cnt[start + p] : 0u;
+          uint32_t tot;
+          const uint32_t ex = block_exclusive_scan(mult ? 1u : 0u, scan, &tot);
+          const int64_t r = (int64_t)rank0 + ex;
+          if (mult && r >= lo && r < hi) {
+            const int col = start + p;
+            wl_idx[r - lo] = (uint32_t)col;
+            wl_w[r - lo] = __fmul_rn(wts[col], (float)mult);
+            wl_al[r - lo] = b.alpha[col];
+            b.distinct_idx[r] = (uint32_t)col;
+            b.distinct_mult[r] = mult;
+          }
+          rank0 += tot;
+        }
+      }
+    }
+  }
+  if (amm && !sampled) {  // sanity mode: identity list, weight 1
+    for (int k = t; k < (int)(hi - lo); k += blockDim.x) {
+      wl_w[k] = 1.0f;
+      wl_al[k] = b.alpha[lo + k];
+    }
+  }
+  const int nb = (int)(hi - lo);
+  const int ngroups = (nb + GC - 1) / GC;
+  __syncthreads();
+  fence_proxy_async_smem();  // the stage area was written through the generic proxy
+
+  if (warp == ncw) {
+    // ================================ producer warp ================================
+    if (lane == 0) {
+      const uint64_t policy = l2_evict_first_policy();
+      const size_t col_stride = (size_t)b.ld * sizeof(Elem);
+      const unsigned char* Abase = reinterpret_cast<const unsigned char*>(b.A);
+      for (int grp = 0; grp < ngroups; ++grp) {
+        const int s = grp % NS;
+        const int use = grp / NS;
+        if (use >= 1 && !mbar_wait_bounded(&empty[s], (uint32_t)((use - 1) & 1))) {
+          atomicOr(b.status, (uint32_t)kDevTimeout);
+          break;
+        }
+        const int c0 = grp * GC;
+        const int cnt = min(GC, nb - c0);
+        mbar_arrive_expect_tx(&full[s], (uint32_t)cnt * col_bytes);
+        for (int qq = 0; qq < cnt; ++qq) {
+          const uint32_t col = sampled ? wl_idx[c0 + qq] : (uint32_t)(lo + c0 + qq);
+          bulk_g2s(stages + ((size_t)s * GC + qq) * col_bytes, Abase + (size_t)col * col_stride,
+                   col_bytes, &full[s], policy);
+        }
+      }
+    }
+    return;
+  }
+
+  // ================================= consumer warps ==================================
+  // dx = x_i − x_memo on this thread's rows, x_i = scale·y_{i−1} (FP32 multiply)
+  float2 dx[R][H];
+  float2 yacc[R][H];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      dx[r][h] = make_float2(0.f, 0.f);
+      yacc[r][h] = make_float2(0.f, 0.f);
+    }
+  double sum_dx = 0.0, zdx = 0.0;
+  if (!SETUP) {
+    const float* yprev = b.y[(a.iter + 1) & 1];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int vi = t + r * T;
+      if (vi < nvec) {
+#pragma unroll
+        for (int h4 = 0; h4 < E / 4; ++h4) {
+          const int o4 = vi * (E / 4) + h4;
+          const float4 yp = reinterpret_cast<const float4*>(yprev)[o4];
+          float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (amm) xm = reinterpret_cast<const float4*>(b.x_memo)[o4];
+          const float d0 = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
+          const float d1 = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
+          const float d2 = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
+          const float d3 = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
+          dx[r][2 * h4] = make_float2(d0, d1);
+          dx[r][2 * h4 + 1] = make_float2(d2, d3);
+          if (centred) {
+            const float4 z4 = reinterpret_cast<const float4*>(b.z)[o4];
+            sum_dx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
+            zdx = fma((double)d0, (double)z4.x, zdx);
+            zdx = fma((double)d1, (double)z4.y, zdx);
+            zdx = fma((double)d2, (double)z4.z, zdx);
+            zdx = fma((double)d3, (double)z4.w, zdx);
+          }
+        }
+      }
+    }
+  }
+  if (centred) {  // Σdx and z·dx over all m rows (common.h:55-87), identical in every CTA
+    sum_dx = warp_sum(sum_dx);
+    zdx = warp_sum(zdx);
+    double* wtmp = reinterpret_cast<double*>(redw);
+    if (lane == 0) {
+      wtmp[2 * warp] = sum_dx;
+      wtmp[2 * warp + 1] = zdx;
+    }
+    named_barrier_or(1, T, false);
+    sum_dx = 0.0;
+    zdx = 0.0;
+    for (int w = 0; w < ncw; ++w) {
+      sum_dx += wtmp[2 * w];
+      zdx += wtmp[2 * w + 1];
+    }
+    named_barrier_or(1, T, false);  // wtmp (= redw) is reused below
+    if (q == 0 && t == 0) {
+      b.st[a.iter & 1].sum_dx = sum_dx;
+      b.st[a.iter & 1].zdx = zdx;
+    }
+  }
+  const float sum_dx_f = (float)sum_dx;
+
+  // partial dots of group grp over this thread's rows, warp-reduced into redw[grp & 1]
+  auto wait_group = [&](int grp) -> bool {
+    return mbar_wait_bounded(&full[grp % NS], (uint32_t)((grp / NS) & 1));
+  };
+  // guarded partial dots of group grp (tail groups, partial slots, the set-up statistics)
+  auto dot_group = [&](int grp, RT (&d)[GC], bool got) -> bool {
+    const int s = grp % NS;
+    const int cnt = got ? min(GC, nb - grp * GC) : 0;
+    const unsigned char* sb = stages + (size_t)s * GC * col_bytes;
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      if constexpr (SETUP) {
+        d[qq] = make_double2(0.0, 0.0);
+      } else {
+        d[qq] = 0.f;
+      }
+      if (qq < cnt) {
+        const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
+        if constexpr (SETUP) {
+          // per 16-byte vector: FP32 partial sums of <= 8 values (the BF16 squares are exact in
+          // FP32), folded into FP64 accumulators
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int vi = t + r * T;
+            if (vi < nvec) {
+              float2 av[H];
+              unpack2(col[vi], av);
+              float2 s2 = av[0];
+              float2 q2 = make_float2(__fmul_rn(av[0].x, av[0].x), __fmul_rn(av[0].y, av[0].y));
+#pragma unroll
+              for (int h = 1; h < H; ++h) {
+                s2 = make_float2(s2.x + av[h].x, s2.y + av[h].y);
+                q2 = fma2(av[h], av[h], q2);
+              }
+              d[qq].x += (double)s2.x + (double)s2.y;
+              d[qq].y += (double)q2.x + (double)q2.y;
+            }
+          }
+        } else {
+          float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int vi = t + r * T;
+            if (vi < nvec) {
+              float2 av[H];
+              unpack2(col[vi], av);
+#pragma unroll
+              for (int h = 0; h < H; h += 2) {
+                p0 = fma2(av[h], dx[r][h], p0);
+                if (h + 1 < H) p1 = fma2(av[h + 1], dx[r][h + 1], p1);
+              }
+            }
+          }
+          d[qq] = (p0.x + p0.y) + (p1.x + p1.y);
+        }
+      }
+    }
+    return got;
+  };
+  auto publish = [&](int grp, RT (&d)[GC]) {
+    const int cnt = min(GC, nb - grp * GC);
+    RT* slot = redw + ((grp & 1) * 16 + warp) * GC;
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      if (qq < cnt) {
+        const RT v = warp_red(d[qq]);
+        if (lane == 0) slot[qq] = v;
+      }
+    }
+  };
+
+  float sacc = 0.f;    // Σ α_k t_k (proposed)
+  double a2acc = 0.0;  // Σ α_j² (set-up)
+  bool ok = true;
+  const bool full_slots = (T * R == nvec);  // every vector slot of every thread is a real row
+  RT dn[GC];
+  if (ngroups > 0) {
+    ok = wait_group(0);
+    dot_group(0, dn, ok);
+    publish(0, dn);
+  }
+  if (named_barrier_or(1, T, !ok)) ok = false;
+  for (int grp = 0; ok && grp < ngroups; ++grp) {
+    const int cnt = min(GC, nb - grp * GC);
+    // coefficients of this group (every thread sums the warp partials in the same order)
+    float coef[GC];
+    const RT* rs = redw + (grp & 1) * 16 * GC;
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      coef[qq] = 0.f;
+      if (qq < cnt) {
+        const int k = grp * GC + qq;
+        if constexpr (SETUP) {
+          // α_j needs only Σa; the column sums go to global memory for the statistics kernel
+          double sx = rs[qq].x;
+          for (int w = 1; w < ncw; ++w) sx += rs[w * GC + qq].x;
+          const float af = (float)(sx / (double)m);
+          coef[qq] = af;
+          a2acc = fma((double)af, (double)af, a2acc);
+          if (t == qq) {
+            double sy = rs[qq].y;
+            for (int w = 1; w < ncw; ++w) sy += rs[w * GC + qq].y;
+            b.colsum[lo + k] = make_double2(sx, sy);
+          }
+        } else {
+          float tot = rs[qq];
+          for (int w = 1; w < ncw; ++w) tot += rs[w * GC + qq];
+          if (!amm) {
+            coef[qq] = tot;
+          } else if (centred) {
+            const float al = wl_al[k];
+            const float tq = __fmul_rn(__fsub_rn(tot, __fmul_rn(al, sum_dx_f)), wl_w[k]);
+            coef[qq] = tq;
+            sacc = fmaf(al, tq, sacc);
+          } else {
+            coef[qq] = __fmul_rn(tot, wl_w[k]);
+          }
+        }
+      }
+    }
+    const bool more = grp + 1 < ngroups;
+    const int cnt_n = more ? min(GC, nb - (grp + 1) * GC) : 0;
+    bool got = true;
+    if (more) got = wait_group(grp + 1);
+    ok = ok && got;
+    const int s = grp % NS;
+    const unsigned char* sb = stages + (size_t)s * GC * col_bytes;
+    bool fused = false;
+    if constexpr (!SETUP) {
+      if (full_slots && cnt == GC && got) {
+        if (more && cnt_n == GC) {
+          fused_block<Elem, R, GC, true>(sb, stages + (size_t)((grp + 1) % NS) * GC * col_bytes,
+                                         col_bytes, t, T, coef, dx, yacc, dn);
+          fused = true;
+        } else if (!more) {
+          fused_block<Elem, R, GC, false>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
+          fused = true;
+        }
+      }
+    }
+    if (!fused) {
+      // partial dots of the next group (its reduction latency overlaps this group's axpy)
+      if (more) dot_group(grp + 1, dn, got);
+      // y += coef · A over this thread's rows
+#pragma unroll
+      for (int qq = 0; qq < GC; ++qq) {
+        if (qq < cnt) {
+          const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
+          const float2 c2 = make_float2(coef[qq], coef[qq]);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int vi = t + r * T;
+            if (vi < nvec) {
+              float2 av[H];
+              unpack2(col[vi], av);
+#pragma unroll
+              for (int h = 0; h < H; ++h) yacc[r][h] = fma2(c2, av[h], yacc[r][h]);
+            }
+          }
+        }
+      }
+    }
+    if (more) publish(grp + 1, dn);
+    // partials of grp+1 published; every consumer is done with stage s
+    if (named_barrier_or(1, T, !ok)) ok = false;
+    if (t == 0) mbar_arrive_local(&empty[s]);
+  }
+
+  if (!ok) {
+    if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
+    return;
+  }
+  float* part = b.partials + (size_t)q * m;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int vi = t + r * T;
+    if (vi < nvec) {
+#pragma unroll
+      for (int h4 = 0; h4 < E / 4; ++h4)
+        reinterpret_cast<float4*>(part)[vi * (E / 4) + h4] =
+            make_float4(yacc[r][2 * h4].x, yacc[r][2 * h4].y, yacc[r][2 * h4 + 1].x,
+                        yacc[r][2 * h4 + 1].y);
+    }
+  }
+  if (t == 0) {
+    b.spart[q] = sacc;
+    b.spart64[q] = a2acc;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Geometry and launch
+// ------------------------------------------------------------------------------------------
+
+using KernelFn = void (*)(PanelArgs);
+
+// Supported (R, GC) instantiations; rows per thread = R*E.
+static KernelFn pick_kernel(int dtype, int R, int GC, bool setup) {
+#define AMM_PICK(EL, RR, GG)                                                     \
+  if (R == RR && GC == GG)                                                       \
+    return setup ? panel_kernel<EL, RR, GG, true> : panel_kernel<EL, RR, GG, false>;
+  if (dtype == 1) {
+    AMM_PICK(__nv_bfloat16, 1, 8)
+    AMM_PICK(__nv_bfloat16, 1, 4)
+    AMM_PICK(__nv_bfloat16, 2, 4)
+    AMM_PICK(__nv_bfloat16, 2, 2)
+    AMM_PICK(__nv_bfloat16, 4, 2)
+    AMM_PICK(__nv_bfloat16, 4, 1)
+  } else {
+    AMM_PICK(float, 1, 8)
+    AMM_PICK(float, 1, 4)
+    AMM_PICK(float, 2, 4)
+    AMM_PICK(float, 2, 2)
+    AMM_PICK(float, 4, 2)
+    AMM_PICK(float, 4, 1)
+    AMM_PICK(float, 8, 1)
+  }
+#undef AMM_PICK
+  return nullptr;
+}
+
+static cudaError_t configure(const PanelGeom& g, bool setup, KernelFn* fn, int* smem) {
+  *fn = pick_kernel(g.dtype, g.slots, g.gc, setup);
+  if (!*fn) return cudaErrorInvalidValue;
+  *smem = smem_layout(g, setup).total;
+  return cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem);
+}
+
+static int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return (v && *v) ? atoi(v) : dflt;
+}
+
+// Rows per thread, columns per group and stages for (m, dtype): one persistent CTA per SM
+// (grid = number of SMs).  Tuning overrides: AMM_PANEL_GC, AMM_PANEL_STAGES (0 = automatic).
+bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
+  const int es = dtype == 1 ? 2 : 4;
+  const int E = 16 / es;
+  if (m <= 0 || m % E != 0) return false;
+  const int nvec = m / E;
+  const int rmax = dtype == 1 ? 4 : 8;  // 32 rows per thread at most (register budget)
+  int R = 1;
+  while ((nvec + R - 1) / R > kMaxThreads && R < rmax) R <<= 1;
+  if ((nvec + R - 1) / R > kMaxThreads) return false;
+  // prefer >= 4 rows per thread so that small matrices still use few warps efficiently
+  const int T = ((nvec + R - 1) / R + 31) / 32 * 32;
+  const int colb = m * es;
+  // ~64 KB per stage, 3 stages (one in flight while two are in use)
+  int gc = 65536 / colb;
+  if (gc < 1) gc = 1;
+  if (gc > 8) gc = 8;
+  int p2 = 1;
+  while (p2 * 2 <= gc) p2 <<= 1;
+  gc = p2;
+  const int fgc = env_int("AMM_PANEL_GC", 0);
+  if (fgc > 0) gc = fgc;
+  const int stage = gc * colb;
+  int ns = (192 * 1024) / stage;
+  if (ns > 8) ns = 8;
+  const int fns = env_int("AMM_PANEL_STAGES", 0);
+  if (fns > 0 && fns < ns) ns = fns;
+  if (ns < 3 || !pick_kernel(dtype, R, gc, false)) return false;
+  PanelGeom b{};
+  b.dtype = dtype;
+  b.cluster = 1;
+  b.rows = m;
+  b.nclusters = nsm;
+  b.threads = T;
+  b.slots = R;
+  b.elems = E;
+  b.colbytes = colb;
+  b.gc = gc;
+  b.nstages = ns;
+  b.stage_bytes = stage;
+  b.stage_area = ns * stage > 4 * 4096 ? ns * stage : 4 * 4096;
+  const int maxlist = c < n ? c : n;
+  b.wl_cap = (maxlist + nsm - 1) / nsm + 1;
+  b.smem_bytes = smem_layout(b, true).total;
+  *g = b;
+  return b.smem_bytes <= 227 * 1024;
+}
+
+static cudaError_t launch_panel(const PanelArgs& a, bool setup, cudaStream_t s) {
+  KernelFn fn;
+  int smem = 0;
+  cudaError_t e = configure(a.g, setup, &fn, &smem);
+  if (e != cudaSuccess) return e;
+  fn<<<a.g.nclusters, a.g.threads + 32, smem, s>>>(a);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_setup_panel(const Buffers& b, const PanelGeom& g, cudaStream_t s) {
+  PanelArgs a{};
+  a.b = b;
+  a.g = g;
+  a.iter = 0;
+  return launch_panel(a, true, s);
+}
+
+cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
+                              cudaStream_t s) {
+  PanelArgs a{};
+  a.b = b;
+  a.g = g;
+  a.cc = cc;
+  a.iter = iter;
+  return launch_panel(a, false, s);
+}
+
+}  // namespace amm

@@ -25,6 +25,10 @@ def main():
     p.add_argument("--kinds", default="exact,proposed")
     p.add_argument("--reps", type=int, default=1)
     p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--solve", default=None, choices=[None, "exact", "previous", "proposed"],
+                   help="instead of single launches: one warm-up and one timed solve")
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--vr", type=int, default=4)
     a = p.parse_args()
     g = torch.Generator(device="cuda").manual_seed(a.seed)
     At = torch.randn(a.n, a.m, device="cuda", generator=g)
@@ -32,7 +36,25 @@ def main():
     A = At.t() if a.dtype == "f32" else At.to(torch.bfloat16).t()
     del At
     es = 4 if a.dtype == "f32" else 2
+    if a.solve:
+        ctx = AMMContext(a.m, a.n, c=a.c, step=a.steps, vr_period=a.vr, dtype=a.dtype)
+        x0 = torch.randn(a.m, device="cuda", generator=g)
+        for rep in range(2):
+            ctx.set_rng_state(torch.arange(1, a.c + 1, dtype=torch.int32, device="cuda"))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            ctx.set_matrix(A)
+            ctx.power_method(a.solve, x0)
+            e1.record()
+            e1.synchronize()
+            tr = ctx.trace()
+            print(f"solve {a.solve} rep {rep}: {e0.elapsed_time(e1):.3f} ms, kinds {tr['kinds']}")
+        ctx.close()
+        return
     ctx = AMMContext(a.m, a.n, c=a.c, step=2, dtype=a.dtype)
+    print("geometry", ctx.geometry())
     ctx.set_matrix(A)
     ctx.set_rng_state(torch.arange(1, a.c + 1, dtype=torch.int32, device="cuda") * 2654435761 % (2**31))
     x0 = torch.randn(a.m, device="cuda", generator=g)

@@ -195,6 +195,11 @@ int amm_benchmark_product(amm_ctx *ctx, int kind, int reps, float *ms_per_launch
 int amm_grad_lambda(amm_ctx *ctx, const float *d_v, float *d_grad, int64_t ld_grad,
                     void *stream);
 
+/* Launch geometry of the fused product kernel chosen for this context, 10 values:
+ * {cluster size, rows per CTA, clusters, consumer threads, vector slots per thread,
+ *  columns per stage, stages, stage bytes, shared memory bytes, work-list capacity}. */
+int amm_get_geometry(amm_ctx *ctx, int32_t *out10);
+
 /* Human-readable name of a status code; the last CUDA error string of this thread. */
 const char *amm_status_string(int status);
 const char *amm_last_cuda_error(void);

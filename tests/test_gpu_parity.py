@@ -49,7 +49,7 @@ def test_column_stats(m, n):
     np.testing.assert_allclose(st["norm"].cpu().numpy(), norm, rtol=1e-6)
     np.testing.assert_allclose(st["normp"].cpu().numpy(), normp, rtol=1e-5)
     a2 = O.alpha_squared(alpha)
-    assert abs(st["alpha2"] - a2) <= 1e-9 * a2
+    assert abs(st["alpha2"] - a2) <= 1e-6 * a2  # FP32 α_j, accumulated in FP64
     z, v = O.generate_zv(A, alpha, a2)
     assert vec_rel(st["z"].cpu().numpy(), z) < 1e-5
     assert vec_rel(st["v"].cpu().numpy(), v) < 1e-5
@@ -60,7 +60,10 @@ def test_cdf_and_weights(cdf):
     A = scaled_gaussian(256, 3000, seed=3, shift=0.1)
     c = 200
     ctx = ctx_for(A, c=c, cdf=cdf)
-    alpha, norm, normp = O.get_norms(A)
+    # the tables are a function of the library's own column norms (checked against the oracle
+    # in test_column_stats); FP32 norms may differ from the oracle's in the last bit
+    stats = ctx.column_stats()
+    norm, normp = stats["norm"].cpu().numpy(), stats["normp"].cpu().numpy()
     for which, base in ((0, norm), (1, normp)):
         gcdf, gw = ctx.sampling_tables(which)
         gcdf = gcdf.cpu().numpy()
@@ -258,13 +261,14 @@ def test_exact_fp32_lambda_matches_fp64_eigvalsh():
     assert rel(tr["eigs"][-1], lam) < 1e-5
 
 
-def test_runs_are_deterministic():
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_runs_are_deterministic(use_graph):
     m, n, c, step = 512, 4096, 300, 10
     A = scaled_gaussian(m, n, seed=81)
     x0 = t32(np.random.default_rng(82).standard_normal(m))
     out = []
     for _ in range(2):
-        ctx = ctx_for(A, c=c, step=step, vr_period=3)
+        ctx = ctx_for(A, c=c, step=step, vr_period=3, use_graph=use_graph)
         ctx.set_rng_state(tu32(states(c, 83)))
         ctx.power_method("proposed", x0)
         out.append(ctx.trace()["eigs"])
@@ -272,6 +276,26 @@ def test_runs_are_deterministic():
         out.append(ctx.trace()["eigs"])
     assert np.array_equal(out[0], out[2]) and np.array_equal(out[1], out[3])
     assert not np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("method", ["previous", "proposed", "proposed_v2"])
+def test_every_call_starts_from_a_zero_memo(method):
+    """Each call restarts like the reference (zero_clear): repeated calls on one context with
+    the same states and start vector give the same trace, equal to the oracle's."""
+    m, n, c, step = 512, 4096, 256, 9
+    A = scaled_gaussian(m, n, seed=85)
+    x0 = np.random.default_rng(86).standard_normal(m).astype(np.float32)
+    st = states(c, 87)
+    ctx = ctx_for(A, c=c, step=step, vr_period=3)
+    traces = []
+    for _ in range(4):
+        ctx.set_rng_state(tu32(st))
+        ctx.power_method(method, t32(x0))
+        traces.append(ctx.trace()["eigs"])
+    for tr in traces[1:]:
+        assert np.array_equal(tr, traces[0])
+    ref = O.power_method(A, x0, method=method, step=step, c=c, states=st, vr_period=3)
+    assert np.all(rel(traces[0], ref.eigs) < RTOL_LAMBDA_F32)
 
 
 def test_grad_lambda_kernel():
