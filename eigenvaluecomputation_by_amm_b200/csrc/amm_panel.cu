@@ -83,16 +83,9 @@ __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup
   return L;
 }
 
-// Packed FP32x2 arithmetic (Blackwell): two IEEE-rounded FMAs per instruction.
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-  float2 d;
-  asm("{\n\t.reg .b64 xa, xb, xc;\n\t"
-      "mov.b64 xa, {%2, %3};\n\tmov.b64 xb, {%4, %5};\n\tmov.b64 xc, {%6, %7};\n\t"
-      "fma.rn.f32x2 xc, xa, xb, xc;\n\tmov.b64 {%0, %1}, xc;\n\t}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
-}
+// Packed FP32x2 arithmetic (Blackwell): two IEEE-rounded FMAs per instruction (the sm_100
+// builtin, so the compiler allocates the register pairs itself).
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 // 16-byte vector -> E/2 float2 (exact for BF16: the 16 bits become the high half).
 __device__ __forceinline__ void unpack2(const uint4& v, float2 (&o)[2]) {
@@ -109,24 +102,28 @@ __device__ __forceinline__ void unpack2(const uint4& v, float2 (&o)[4]) {
 // Branch-free body of one full group: the axpy of group g (stage `cur`, coefficients `coef`)
 // interleaved, slot by slot, with the partial dots of group g+1 (stage `nxt`) when NEXT.  Used
 // when every column of both groups is present and every vector slot of every thread is valid.
-template <typename Elem, int R, int GC, bool NEXT>
+template <typename Elem, int R, int GC, bool NEXT, int TC>
 __device__ __forceinline__ void fused_block(const unsigned char* cur, const unsigned char* nxt,
-                                            uint32_t col_bytes, int t, int T,
+                                            uint32_t col_bytes, int t, int T_rt,
                                             const float (&coef)[GC],
                                             const float2 (&dx)[R][8 / sizeof(Elem)],
                                             float2 (&yacc)[R][8 / sizeof(Elem)], float (&dn)[GC]) {
   constexpr int H = 8 / sizeof(Elem);
+  // with a compile-time thread count (TC > 0) every shared-memory load uses an immediate offset
+  const int T = TC > 0 ? TC : T_rt;
+  const int colv = TC > 0 ? R * TC : (int)(col_bytes >> 4);  // vectors per column
+  const uint4* c4 = reinterpret_cast<const uint4*>(cur) + t;
+  const uint4* n4 = reinterpret_cast<const uint4*>(nxt) + t;
   float2 p[GC];
 #pragma unroll
   for (int qq = 0; qq < GC; ++qq) p[qq] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int vi = t + r * T;
     uint4 vc[GC], vn[GC];
 #pragma unroll
     for (int qq = 0; qq < GC; ++qq) {
-      vc[qq] = reinterpret_cast<const uint4*>(cur + (size_t)qq * col_bytes)[vi];
-      if (NEXT) vn[qq] = reinterpret_cast<const uint4*>(nxt + (size_t)qq * col_bytes)[vi];
+      vc[qq] = c4[qq * colv + r * T];
+      if (NEXT) vn[qq] = n4[qq * colv + r * T];
     }
 #pragma unroll
     for (int qq = 0; qq < GC; ++qq) {
@@ -145,6 +142,101 @@ __device__ __forceinline__ void fused_block(const unsigned char* cur, const unsi
   }
 #pragma unroll
   for (int qq = 0; qq < GC; ++qq) dn[qq] = p[qq].x + p[qq].y;
+}
+
+// Sum over the 16 warps of NC partial values per warp (element (w, c) at base[w * stride + c]),
+// computed identically by every warp: lane groups of L lanes own one value each and reduce by a
+// fixed xor tree (deterministic).
+template <typename V, int NC>
+__device__ __forceinline__ void warp_partials_sum(const V* base, int stride, int lane,
+                                                  V (&tot)[NC]) {
+  constexpr int L = (32 / NC) < 16 ? (32 / NC) : 16;  // lanes per value
+  constexpr int PER = 16 / L;                          // warp partials per lane
+  constexpr int CPR = 32 / L;                          // values per round
+  constexpr int ROUNDS = (NC + CPR - 1) / CPR;
+#pragma unroll
+  for (int rr = 0; rr < ROUNDS; ++rr) {
+    const int q = rr * CPR + lane / L;
+    const int w0 = lane % L;
+    V v = V(0);
+    if (q < NC) {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) v += base[(w0 + j * L) * stride + q];
+    }
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+#pragma unroll
+    for (int c = 0; c < CPR; ++c)
+      if (rr * CPR + c < NC) tot[rr * CPR + c] = __shfl_sync(0xffffffffu, v, c * L);
+  }
+}
+
+// Warp reduction of N values at once (multi-value butterfly): lane l ends with the full sum of
+// value l / (32/N); returns it (a fixed tree, deterministic).
+template <typename V, int N>
+__device__ __forceinline__ V warp_reduce_multi(V (&v)[N], int lane) {
+  int off = 16;
+#pragma unroll
+  for (int n = N / 2; n >= 1; n >>= 1, off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      const V send = upper ? v[i] : v[i + n];
+      const V keep = upper ? v[i + n] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  V r = v[0];
+  for (; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+  return r;
+}
+
+// Set-up variant of fused_block: the axpy uses coef = α_j; the next group's statistics are
+// per-vector FP32 partial sums of <= 8 values (BF16 squares are exact in FP32) folded into
+// FP64 accumulators (Σa, Σa²).
+template <typename Elem, int R, int GC, bool NEXT, int TC>
+__device__ __forceinline__ void fused_block_setup(const unsigned char* cur, const unsigned char* nxt,
+                                                  uint32_t col_bytes, int t, int T_rt,
+                                                  const float (&coef)[GC],
+                                                  float2 (&yacc)[R][8 / sizeof(Elem)],
+                                                  double2 (&dn)[GC]) {
+  constexpr int H = 8 / sizeof(Elem);
+  const int T = TC > 0 ? TC : T_rt;
+  const int colv = TC > 0 ? R * TC : (int)(col_bytes >> 4);
+  const uint4* c4 = reinterpret_cast<const uint4*>(cur) + t;
+  const uint4* n4 = reinterpret_cast<const uint4*>(nxt) + t;
+#pragma unroll
+  for (int qq = 0; qq < GC; ++qq) dn[qq] = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    uint4 vc[GC], vn[GC];
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      vc[qq] = c4[qq * colv + r * T];
+      if (NEXT) vn[qq] = n4[qq * colv + r * T];
+    }
+#pragma unroll
+    for (int qq = 0; qq < GC; ++qq) {
+      float2 ac[H];
+      unpack2(vc[qq], ac);
+      const float2 c2 = make_float2(coef[qq], coef[qq]);
+#pragma unroll
+      for (int h = 0; h < H; ++h) yacc[r][h] = fma2(c2, ac[h], yacc[r][h]);
+      if (NEXT) {
+        float2 an[H];
+        unpack2(vn[qq], an);
+        float2 s2 = an[0];
+        float2 q2 = __fmul2_rn(an[0], an[0]);
+#pragma unroll
+        for (int h = 1; h < H; ++h) {
+          s2 = __fadd2_rn(s2, an[h]);
+          q2 = fma2(an[h], an[h], q2);
+        }
+        dn[qq].x += (double)s2.x + (double)s2.y;
+        dn[qq].y += (double)q2.x + (double)q2.y;
+      }
+    }
+  }
 }
 
 template <typename Elem, int R, int GC, bool SETUP>
@@ -386,10 +478,10 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
               float2 av[H];
               unpack2(col[vi], av);
               float2 s2 = av[0];
-              float2 q2 = make_float2(__fmul_rn(av[0].x, av[0].x), __fmul_rn(av[0].y, av[0].y));
+              float2 q2 = __fmul2_rn(av[0], av[0]);
 #pragma unroll
               for (int h = 1; h < H; ++h) {
-                s2 = make_float2(s2.x + av[h].x, s2.y + av[h].y);
+                s2 = __fadd2_rn(s2, av[h]);
                 q2 = fma2(av[h], av[h], q2);
               }
               d[qq].x += (double)s2.x + (double)s2.y;
@@ -420,11 +512,35 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
   auto publish = [&](int grp, RT (&d)[GC]) {
     const int cnt = min(GC, nb - grp * GC);
     RT* slot = redw + ((grp & 1) * 16 + warp) * GC;
+    if constexpr (!SETUP && GC >= 2) {
+      float v[GC];
 #pragma unroll
-    for (int qq = 0; qq < GC; ++qq) {
-      if (qq < cnt) {
-        const RT v = warp_red(d[qq]);
-        if (lane == 0) slot[qq] = v;
+      for (int qq = 0; qq < GC; ++qq) v[qq] = d[qq];
+      const float r = warp_reduce_multi<float, GC>(v, lane);
+      constexpr int L = 32 / GC;
+      const int q = lane / L;
+      if (lane % L == 0 && q < cnt) slot[q] = r;
+    } else if constexpr (SETUP && 2 * GC <= 32) {
+      double v[2 * GC];
+#pragma unroll
+      for (int qq = 0; qq < GC; ++qq) {
+        v[2 * qq] = d[qq].x;
+        v[2 * qq + 1] = d[qq].y;
+      }
+      const double r = warp_reduce_multi<double, 2 * GC>(v, lane);
+      constexpr int L = 32 / (2 * GC);
+      const int idx = lane / L;
+      if (lane % L == 0 && (idx >> 1) < cnt) {
+        double* sd = reinterpret_cast<double*>(slot);
+        sd[idx] = r;  // (Σa, Σa²) of column idx/2
+      }
+    } else {
+#pragma unroll
+      for (int qq = 0; qq < GC; ++qq) {
+        if (qq < cnt) {
+          const RT v = warp_red(d[qq]);
+          if (lane == 0) slot[qq] = v;
+        }
       }
     }
   };
@@ -445,6 +561,32 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
     // coefficients of this group (every thread sums the warp partials in the same order)
     float coef[GC];
     const RT* rs = redw + (grp & 1) * 16 * GC;
+    float tots[GC];
+    double sxy[2 * GC];
+    if constexpr (SETUP) {
+      const double* rsd = reinterpret_cast<const double*>(rs);
+      if (ncw == 16) {
+        warp_partials_sum<double, 2 * GC>(rsd, 2 * GC, lane, sxy);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 2 * GC; ++i) {
+          double tt = rsd[i];
+          for (int w = 1; w < ncw; ++w) tt += rsd[w * 2 * GC + i];
+          sxy[i] = tt;
+        }
+      }
+    } else {
+      if (ncw == 16) {
+        warp_partials_sum<float, GC>(reinterpret_cast<const float*>(rs), GC, lane, tots);
+      } else {
+#pragma unroll
+        for (int qq = 0; qq < GC; ++qq) {
+          float tt = rs[qq];
+          for (int w = 1; w < ncw; ++w) tt += rs[w * GC + qq];
+          tots[qq] = tt;
+        }
+      }
+    }
 #pragma unroll
     for (int qq = 0; qq < GC; ++qq) {
       coef[qq] = 0.f;
@@ -452,19 +594,13 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
         const int k = grp * GC + qq;
         if constexpr (SETUP) {
           // α_j needs only Σa; the column sums go to global memory for the statistics kernel
-          double sx = rs[qq].x;
-          for (int w = 1; w < ncw; ++w) sx += rs[w * GC + qq].x;
+          const double sx = sxy[2 * qq];
           const float af = (float)(sx / (double)m);
           coef[qq] = af;
           a2acc = fma((double)af, (double)af, a2acc);
-          if (t == qq) {
-            double sy = rs[qq].y;
-            for (int w = 1; w < ncw; ++w) sy += rs[w * GC + qq].y;
-            b.colsum[lo + k] = make_double2(sx, sy);
-          }
+          if (t == qq) b.colsum[lo + k] = make_double2(sx, sxy[2 * qq + 1]);
         } else {
-          float tot = rs[qq];
-          for (int w = 1; w < ncw; ++w) tot += rs[w * GC + qq];
+          const float tot = tots[qq];
           if (!amm) {
             coef[qq] = tot;
           } else if (centred) {
@@ -486,14 +622,34 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
     const int s = grp % NS;
     const unsigned char* sb = stages + (size_t)s * GC * col_bytes;
     bool fused = false;
-    if constexpr (!SETUP) {
-      if (full_slots && cnt == GC && got) {
+    if (full_slots && cnt == GC && got) {
+      const unsigned char* sn = stages + (size_t)((grp + 1) % NS) * GC * col_bytes;
+      if constexpr (SETUP) {
         if (more && cnt_n == GC) {
-          fused_block<Elem, R, GC, true>(sb, stages + (size_t)((grp + 1) % NS) * GC * col_bytes,
-                                         col_bytes, t, T, coef, dx, yacc, dn);
+          if (T == 512)
+            fused_block_setup<Elem, R, GC, true, 512>(sb, sn, col_bytes, t, T, coef, yacc, dn);
+          else
+            fused_block_setup<Elem, R, GC, true, 0>(sb, sn, col_bytes, t, T, coef, yacc, dn);
           fused = true;
         } else if (!more) {
-          fused_block<Elem, R, GC, false>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
+          if (T == 512)
+            fused_block_setup<Elem, R, GC, false, 512>(sb, sb, col_bytes, t, T, coef, yacc, dn);
+          else
+            fused_block_setup<Elem, R, GC, false, 0>(sb, sb, col_bytes, t, T, coef, yacc, dn);
+          fused = true;
+        }
+      } else {
+        if (more && cnt_n == GC) {
+          if (T == 512)
+            fused_block<Elem, R, GC, true, 512>(sb, sn, col_bytes, t, T, coef, dx, yacc, dn);
+          else
+            fused_block<Elem, R, GC, true, 0>(sb, sn, col_bytes, t, T, coef, dx, yacc, dn);
+          fused = true;
+        } else if (!more) {
+          if (T == 512)
+            fused_block<Elem, R, GC, false, 512>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
+          else
+            fused_block<Elem, R, GC, false, 0>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
           fused = true;
         }
       }
