@@ -248,8 +248,9 @@ class AMMContext:
         return idx
 
     def benchmark_product(self, kind: str, reps: int = 10, stream=None):
-        """Mean CUDA-event time (ms) of one fused product launch and its distinct columns."""
-        k = {"exact": 1, "previous": 2, "proposed": 3}[kind]
+        """Mean CUDA-event time (ms) of one fused product launch (or of the set-up pass, kind
+        "setup") and the distinct columns it reads."""
+        k = {"exact": 1, "previous": 2, "proposed": 3, "setup": 16}[kind]
         ms = C.c_float(0.0)
         d = C.c_int64(0)
         check(self.lib.amm_benchmark_product(self._ctx, k, int(reps), C.byref(ms), C.byref(d),

@@ -132,6 +132,12 @@ void layout(amm_ctx* ctx, Carver& cv) {
   }
   b.distinct_idx = cv.take<uint32_t>(c);
   b.distinct_mult = cv.take<uint32_t>(c);
+  for (int w = 0; w < 2; ++w) {
+    b.wl_col[w] = cv.take<uint32_t>(c);
+    b.wl_wm[w] = cv.take<float>(c);
+    b.wl_al[w] = cv.take<float>(c);
+    b.wl_count[w] = cv.take<uint32_t>(1);
+  }
   b.partials = cv.take<float>((size_t)b.nsm * m);
   b.spart = cv.take<float>(b.nsm);
   b.spart64 = cv.take<double>(b.nsm);
@@ -182,13 +188,17 @@ int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normal
     AMM_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   }
   AMM_CUDA(amm::launch_init(b, cc, x0, no_normalize, s));
-  if (draws) AMM_CUDA(amm::launch_sample(b, cc, -1, s));
+  if (draws) {
+    AMM_CUDA(amm::launch_sample(b, cc, -1, s));
+    AMM_CUDA(amm::launch_compact(b, cc, -1, s));
+  }
   for (int i = 0; i < cc.step; ++i) {
     const bool fork = draws && i + 1 < cc.step;
     if (fork) {
       AMM_CUDA(cudaEventRecord(ctx->ev_fork, s));
       AMM_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0));
       AMM_CUDA(amm::launch_sample(b, cc, i, ctx->side_stream));
+      AMM_CUDA(amm::launch_compact(b, cc, i, ctx->side_stream));
       AMM_CUDA(cudaEventRecord(ctx->ev_join, ctx->side_stream));
     }
     AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, s));
@@ -239,7 +249,7 @@ int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
     it = ctx->graphs.emplace(key, std::make_pair(g, ex)).first;
   }
   AMM_CUDA(cudaGraphLaunch(it->second.second, s));
-  amm::count_launch(2 + 2 * cc.step + ((cc.uses_amm && !cc.sanity) ? cc.step : 0));
+  amm::count_launch(2 + 2 * cc.step + ((cc.uses_amm && !cc.sanity) ? 2 * cc.step : 0));
   return AMM_OK;
 }
 
@@ -746,6 +756,26 @@ int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch
   if (rc) return rc;
   if (reps < 1 || !ms_per_launch) return AMM_ERR_INVALID_ARGUMENT;
   int method;
+  if (kind == AMM_PASS_SETUP) {
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = as_stream(stream);
+    rc = ensure_setup(ctx, s);  // buffers and geometry; the timed launches redo the pass
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    AMM_CUDA(cudaEventCreate(&e0));
+    AMM_CUDA(cudaEventCreate(&e1));
+    AMM_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) AMM_CUDA(amm::launch_setup_panel(ctx->b, ctx->geom, s));
+    AMM_CUDA(cudaEventRecord(e1, s));
+    AMM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    AMM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_per_launch = ms / (float)reps;
+    if (distinct) *distinct = ctx->cfg.n;
+    return read_status(ctx, s);
+  }
   if (kind == AMM_STEP_EXACT || kind == AMM_STEP_EXACT_MEMO)
     method = amm::kMethodExact;
   else if (kind == AMM_STEP_PREVIOUS)
@@ -773,7 +803,10 @@ int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch
   cc.tol = 0.0;
   cc.step = 1;
   AMM_CUDA(amm::launch_init(ctx->b, cc, ctx->x0_buf, 0, s));
-  if (cc.uses_amm && !ctx->sanity_active) AMM_CUDA(amm::launch_sample(ctx->b, cc, -1, s));
+  if (cc.uses_amm && !ctx->sanity_active) {
+    AMM_CUDA(amm::launch_sample(ctx->b, cc, -1, s));
+    AMM_CUDA(amm::launch_compact(ctx->b, cc, -1, s));
+  }
   cudaEvent_t e0, e1;
   AMM_CUDA(cudaEventCreate(&e0));
   AMM_CUDA(cudaEventCreate(&e1));

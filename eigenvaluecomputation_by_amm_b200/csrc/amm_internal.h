@@ -87,6 +87,12 @@ struct Buffers {
   uint32_t* samples[2];  // raw picks in draw order (c)
   uint32_t* distinct_idx;   // sorted distinct indices of the last AMM product (c)
   uint32_t* distinct_mult;  // their multiplicities (c)
+  // work list of the pending picks (per pick buffer): sorted distinct columns with their
+  // coefficient data, built by compact_kernel
+  uint32_t* wl_col[2];      // c
+  float* wl_wm[2];          // c: w_j · multiplicity
+  float* wl_al[2];          // c: α_j
+  uint32_t* wl_count[2];    // 1: number of distinct columns
   // partial sums
   float* partials;     // nsm x m
   float* spart;        // nsm  (Σ α_k t_k of each CTA, proposed)
@@ -121,7 +127,7 @@ struct PanelGeom {
   int gc;           // columns per stage (group)
   int nstages;
   int stage_bytes;  // gc * colbytes
-  int stage_area;   // bytes reserved for the stages (also prologue scratch)
+  int stage_area;   // bytes reserved for the stages
   int smem_bytes;   // dynamic shared memory (set-up variant, the larger one)
   int wl_cap;       // work-list capacity per cluster
 };
@@ -143,6 +149,8 @@ cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, in
 // Draw the picks of the first AMM step after step iter (iter = -1: start of a call); for
 // iter >= 0 it may run concurrently with the product of step iter.
 cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
+// Build the sorted distinct work list of the picks just drawn (same decision as sample_kernel).
+cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
 // One iteration: panel product and reduce/Rayleigh/clear.
 cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
                               cudaStream_t s);

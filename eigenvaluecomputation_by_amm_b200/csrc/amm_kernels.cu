@@ -174,45 +174,40 @@ __device__ void clear_picks(const Buffers& b, int pb, int rank, int nranks) {
 constexpr int kRedThreads = 256;
 constexpr int kRedRows = 128;  // rows per reduce CTA: 32 float4 groups x 8 partial slices
 
-// Deterministic sum over the nsm partials of 4 rows starting at row (FP64, fixed order).
+// Deterministic sum over the nsm partials of 4 rows starting at row (FP64, fixed order).  Slice
+// ps of the 8 owns partials ps, ps+8, ps+16, ...; every load of a slice is issued before the
+// first add, so a reduce costs about one L2 round trip instead of one per partial.
+constexpr int kRedSlices = 8;
+constexpr int kRedUnroll = 19;  // 8 x 19 = 152 partials per round (one round for 148 SMs)
+
 __device__ __forceinline__ void reduce_rows(const Buffers& b, int row, double4 (*red)[32],
                                             double4* out) {
   const int rg = threadIdx.x & 31, ps = threadIdx.x >> 5;
   double4 acc = make_double4(0, 0, 0, 0);
   if (row < b.m) {
-    // two independent accumulators over partials ps, ps+8, ps+16, ... (a fixed order)
-    double4 acc1 = make_double4(0, 0, 0, 0);
     const float* __restrict__ P = b.partials + row;
-    int k = ps;
-    for (; k + 8 < b.nsm; k += 16) {
-      const float4 p0 = __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * b.m));
-      const float4 p1 = __ldcg(reinterpret_cast<const float4*>(P + (size_t)(k + 8) * b.m));
-      acc.x += p0.x;
-      acc.y += p0.y;
-      acc.z += p0.z;
-      acc.w += p0.w;
-      acc1.x += p1.x;
-      acc1.y += p1.y;
-      acc1.z += p1.z;
-      acc1.w += p1.w;
+    for (int k0 = ps; k0 < b.nsm; k0 += kRedSlices * kRedUnroll) {
+      float4 v[kRedUnroll];
+#pragma unroll
+      for (int u = 0; u < kRedUnroll; ++u) {
+        const int k = k0 + u * kRedSlices;
+        v[u] = k < b.nsm ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * b.m))
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < kRedUnroll; ++u) {
+        acc.x += v[u].x;
+        acc.y += v[u].y;
+        acc.z += v[u].z;
+        acc.w += v[u].w;
+      }
     }
-    if (k < b.nsm) {
-      const float4 p0 = __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * b.m));
-      acc.x += p0.x;
-      acc.y += p0.y;
-      acc.z += p0.z;
-      acc.w += p0.w;
-    }
-    acc.x += acc1.x;
-    acc.y += acc1.y;
-    acc.z += acc1.z;
-    acc.w += acc1.w;
   }
   red[ps][rg] = acc;
   __syncthreads();
   if (ps == 0) {
     double4 s = red[0][rg];
-    for (int k = 1; k < 8; ++k) {
+    for (int k = 1; k < kRedSlices; ++k) {
       s.x += red[k][rg].x;
       s.y += red[k][rg].y;
       s.z += red[k][rg].z;
@@ -439,6 +434,80 @@ __global__ void __launch_bounds__(256) sample_kernel(const __grid_constant__ Sam
   draw_samples<F>(b, which, b.states[sb_in], b.states[sb_in ^ 1], b.count[pb_out],
                   b.chunk[pb_out], b.samples[pb_out], blockIdx.x * blockDim.x + threadIdx.x,
                   gridDim.x * blockDim.x, coarse_s);
+}
+
+// Sorted distinct work list of the picks just drawn (the product kernel's column list): one CTA
+// per kCompactSpan columns counts the picked columns below its range, scans its own range in
+// column order and writes (column, w_j · multiplicity, α_j) at each picked column's rank; CTA 0
+// also writes the list length.  It makes the same decision as sample_kernel and runs after it on
+// the same stream, so it too overlaps the product of step `iter`.  The picks of the first product
+// of a call are also kept as (index, multiplicity) for the single-product entry points.
+constexpr int kCompactThreads = 256;
+constexpr int kCompactPer = 4;
+constexpr int kCompactSpan = kCompactThreads * kCompactPer;
+
+__global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_constant__ SampleArgs a) {
+  __shared__ uint32_t scan[40];
+  const Buffers& b = a.b;
+  const CallCfg& cc = a.cc;
+  int pb_out;
+  if (a.iter < 0) {
+    pb_out = 0;
+  } else {
+    const IterState& st = b.st[a.iter & 1];
+    const bool consumes = st.mode == kPrevious || st.mode == kProposed;
+    if (st.done || !consumes || a.iter + 1 >= cc.step) return;  // uniform over the grid
+    pb_out = st.pb ^ 1;
+  }
+  const int which = next_amm_weighting(cc, a.iter);
+  const uint32_t* __restrict__ cnt = b.count[pb_out];
+  const uint32_t* __restrict__ chunk = b.chunk[pb_out];
+  const int t = threadIdx.x;
+  const int start = blockIdx.x * kCompactSpan;
+  // picked columns below `start`: the whole chunks, then the columns of the chunk `start` is in
+  const int c_lo = start >> b.chunk_shift;
+  uint32_t below = 0;
+  for (int k = t; k < c_lo; k += kCompactThreads) below += __ldg(chunk + k);
+  for (int j = (c_lo << b.chunk_shift) + t; j < start; j += kCompactThreads)
+    below += (__ldg(cnt + j) != 0u) ? 1u : 0u;
+  uint32_t base;
+  block_exclusive_scan(below, scan, &base);
+  if (blockIdx.x == 0) {
+    uint32_t all = 0;
+    for (int k = t; k < b.nchunks; k += kCompactThreads) all += __ldg(chunk + k);
+    uint32_t total;
+    block_exclusive_scan(all, scan, &total);
+    if (t == 0) *b.wl_count[pb_out] = total;
+  }
+  uint32_t mult[kCompactPer];
+  uint32_t nz = 0;
+  const int j0 = start + t * kCompactPer;
+#pragma unroll
+  for (int e = 0; e < kCompactPer; ++e) {
+    const int j = j0 + e;
+    mult[e] = j < b.n ? __ldg(cnt + j) : 0u;
+    nz += mult[e] ? 1u : 0u;
+  }
+  uint32_t unused;
+  uint32_t r = base + block_exclusive_scan(nz, scan, &unused);
+  const float* __restrict__ wts = b.wts[which];
+  uint32_t* __restrict__ wl_col = b.wl_col[pb_out];
+  float* __restrict__ wl_wm = b.wl_wm[pb_out];
+  float* __restrict__ wl_al = b.wl_al[pb_out];
+#pragma unroll
+  for (int e = 0; e < kCompactPer; ++e) {
+    if (mult[e]) {
+      const int j = j0 + e;
+      wl_col[r] = (uint32_t)j;
+      wl_wm[r] = __fmul_rn(__ldg(wts + j), (float)mult[e]);
+      wl_al[r] = __ldg(b.alpha + j);
+      if (a.iter < 0) {
+        b.distinct_idx[r] = (uint32_t)j;
+        b.distinct_mult[r] = mult[e];
+      }
+      ++r;
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -904,6 +973,17 @@ cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStr
     sample_kernel<float><<<blocks, 256, 0, s>>>(a);
   else
     sample_kernel<double><<<blocks, 256, 0, s>>>(a);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s) {
+  SampleArgs a{};
+  a.b = b;
+  a.cc = cc;
+  a.iter = iter;
+  const int blocks = (b.n + kCompactSpan - 1) / kCompactSpan;
+  compact_kernel<<<blocks, kCompactThreads, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }

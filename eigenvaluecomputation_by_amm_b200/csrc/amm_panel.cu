@@ -56,7 +56,7 @@ __device__ __forceinline__ double2 warp_red(double2 v) {
 
 // Shared memory carve (byte offsets), identical on host and device.
 struct SmemLayout {
-  int stages, bars, redw, wl_idx, wl_w, wl_al, scan, total;
+  int stages, bars, redw, wl_idx, wl_w, wl_al, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup) {
@@ -77,8 +77,6 @@ __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup
   o += 4 * g.wl_cap;
   L.wl_al = o;
   o += 4 * g.wl_cap;
-  L.scan = o;
-  o += 4 * 40;
   L.total = (o + 127) & ~127;
   return L;
 }
@@ -205,8 +203,14 @@ __device__ __forceinline__ void fused_block_setup(const unsigned char* cur, cons
   const int colv = TC > 0 ? R * TC : (int)(col_bytes >> 4);
   const uint4* c4 = reinterpret_cast<const uint4*>(cur) + t;
   const uint4* n4 = reinterpret_cast<const uint4*>(nxt) + t;
+  // FP32 partial sums over this thread's R vectors of a column (the BF16 squares are exact in
+  // FP32), folded into FP64 once per column
+  float2 s2[GC], q2[GC];
 #pragma unroll
-  for (int qq = 0; qq < GC; ++qq) dn[qq] = make_double2(0.0, 0.0);
+  for (int qq = 0; qq < GC; ++qq) {
+    s2[qq] = make_float2(0.f, 0.f);
+    q2[qq] = make_float2(0.f, 0.f);
+  }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     uint4 vc[GC], vn[GC];
@@ -225,18 +229,18 @@ __device__ __forceinline__ void fused_block_setup(const unsigned char* cur, cons
       if (NEXT) {
         float2 an[H];
         unpack2(vn[qq], an);
-        float2 s2 = an[0];
-        float2 q2 = __fmul2_rn(an[0], an[0]);
 #pragma unroll
-        for (int h = 1; h < H; ++h) {
-          s2 = __fadd2_rn(s2, an[h]);
-          q2 = fma2(an[h], an[h], q2);
+        for (int h = 0; h < H; ++h) {
+          s2[qq] = __fadd2_rn(s2[qq], an[h]);
+          q2[qq] = fma2(an[h], an[h], q2[qq]);
         }
-        dn[qq].x += (double)s2.x + (double)s2.y;
-        dn[qq].y += (double)q2.x + (double)q2.y;
       }
     }
   }
+#pragma unroll
+  for (int qq = 0; qq < GC; ++qq)
+    dn[qq] = make_double2((double)s2[qq].x + (double)s2[qq].y,
+                          (double)q2[qq].x + (double)q2[qq].y);
 }
 
 template <typename Elem, int R, int GC, bool SETUP>
@@ -266,7 +270,6 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
   uint32_t* wl_idx = reinterpret_cast<uint32_t*>(smem + L.wl_idx);
   float* wl_w = reinterpret_cast<float*>(smem + L.wl_w);
   float* wl_al = reinterpret_cast<float*>(smem + L.wl_al);
-  uint32_t* scan = reinterpret_cast<uint32_t*>(smem + L.scan);
 
   int mode = kExact, pb = 0, done = 0;
   float scale = 0.f;
@@ -291,73 +294,38 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
     fence_barrier_init();
   }
 
-  // ---- this CTA's column list -------------------------------------------------------------
+  // ---- this CTA's column list: a contiguous slice of the sorted work list ------------------
   int64_t lo, hi;
   if (!sampled) {
     lo = (int64_t)q * b.n / G;
     hi = (int64_t)(q + 1) * b.n / G;
   } else {
-    uint32_t* cpre = reinterpret_cast<uint32_t*>(stages);  // scratch before the pipeline starts
-    const uint32_t* chunk = b.chunk[pb];
-    uint32_t carry = 0;
-    for (int base = 0; base < b.nchunks; base += blockDim.x) {
-      const int k = base + t;
-      const uint32_t v = k < b.nchunks ? chunk[k] : 0u;
-      uint32_t tot;
-      const uint32_t ex = block_exclusive_scan(v, scan, &tot);
-      if (k < b.nchunks) cpre[k] = carry + ex;
-      carry += tot;
-    }
-    __syncthreads();
-    const uint32_t cd = carry;
+    const uint32_t cd = __ldg(b.wl_count[pb]);
     lo = (int64_t)q * cd / G;
     hi = (int64_t)(q + 1) * cd / G;
     if (q == 0 && t == 0) b.distinct_hist[a.iter] = (int32_t)cd;
-    if (hi > lo) {
-      int ka = 0, kb = b.nchunks - 1;  // largest k with cpre[k] <= lo
-      while (ka < kb) {
-        const int mid = (ka + kb + 1) >> 1;
-        if (cpre[mid] <= (uint32_t)lo)
-          ka = mid;
-        else
-          kb = mid - 1;
-      }
-      const uint32_t* cnt = b.count[pb];
-      const float* wts = b.wts[which];
-      const int CH = 1 << b.chunk_shift;
-      for (int kc = ka; kc < b.nchunks && cpre[kc] < (uint32_t)hi; ++kc) {
-        uint32_t rank0 = cpre[kc];
-        const int start = kc << b.chunk_shift;
-        const int len = min(CH, b.n - start);
-        for (int p0 = 0; p0 < len; p0 += blockDim.x) {
-          const int p = p0 + t;
-          const uint32_t mult = p < len ? cnt[start + p] : 0u;
-          uint32_t tot;
-          const uint32_t ex = block_exclusive_scan(mult ? 1u : 0u, scan, &tot);
-          const int64_t r = (int64_t)rank0 + ex;
-          if (mult && r >= lo && r < hi) {
-            const int col = start + p;
-            wl_idx[r - lo] = (uint32_t)col;
-            wl_w[r - lo] = __fmul_rn(wts[col], (float)mult);
-            wl_al[r - lo] = b.alpha[col];
-            b.distinct_idx[r] = (uint32_t)col;
-            b.distinct_mult[r] = mult;
-          }
-          rank0 += tot;
-        }
-      }
-    }
-  }
-  if (amm && !sampled) {  // sanity mode: identity list, weight 1
-    for (int k = t; k < (int)(hi - lo); k += blockDim.x) {
-      wl_w[k] = 1.0f;
-      wl_al[k] = b.alpha[lo + k];
-    }
   }
   const int nb = (int)(hi - lo);
   const int ngroups = (nb + GC - 1) / GC;
-  __syncthreads();
-  fence_proxy_async_smem();  // the stage area was written through the generic proxy
+  __syncthreads();  // barrier initialisation visible to every thread
+  if (warp == ncw) {
+    if (sampled) {
+      for (int k = lane; k < nb; k += 32) wl_idx[k] = __ldg(b.wl_col[pb] + lo + k);
+      __syncwarp();
+    }
+  } else if (amm) {
+    // coefficient data of the slice; published to the consumer warps by the named barrier
+    // ahead of the first group
+    for (int k = t; k < nb; k += T) {
+      if (sampled) {
+        wl_w[k] = __ldg(b.wl_wm[pb] + lo + k);
+        wl_al[k] = __ldg(b.wl_al[pb] + lo + k);
+      } else {  // sanity mode: identity list, weight 1
+        wl_w[k] = 1.0f;
+        wl_al[k] = __ldg(b.alpha + lo + k);
+      }
+    }
+  }
 
   if (warp == ncw) {
     // ================================ producer warp ================================
@@ -469,25 +437,23 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
       if (qq < cnt) {
         const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
         if constexpr (SETUP) {
-          // per 16-byte vector: FP32 partial sums of <= 8 values (the BF16 squares are exact in
-          // FP32), folded into FP64 accumulators
+          // FP32 partial sums over this thread's vectors, folded into FP64 once (as
+          // fused_block_setup)
+          float2 s2 = make_float2(0.f, 0.f), q2 = make_float2(0.f, 0.f);
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int vi = t + r * T;
             if (vi < nvec) {
               float2 av[H];
               unpack2(col[vi], av);
-              float2 s2 = av[0];
-              float2 q2 = __fmul2_rn(av[0], av[0]);
 #pragma unroll
-              for (int h = 1; h < H; ++h) {
+              for (int h = 0; h < H; ++h) {
                 s2 = __fadd2_rn(s2, av[h]);
                 q2 = fma2(av[h], av[h], q2);
               }
-              d[qq].x += (double)s2.x + (double)s2.y;
-              d[qq].y += (double)q2.x + (double)q2.y;
             }
           }
+          d[qq] = make_double2((double)s2.x + (double)s2.y, (double)q2.x + (double)q2.y);
         } else {
           float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);
 #pragma unroll
@@ -788,7 +754,7 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   b.gc = gc;
   b.nstages = ns;
   b.stage_bytes = stage;
-  b.stage_area = ns * stage > 4 * 4096 ? ns * stage : 4 * 4096;
+  b.stage_area = ns * stage;
   const int maxlist = c < n ? c : n;
   b.wl_cap = (maxlist + nsm - 1) / nsm + 1;
   b.smem_bytes = smem_layout(b, true).total;

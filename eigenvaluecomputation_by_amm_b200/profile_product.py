@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import argparse
 
+import numpy as np
 import torch
 
 from .api import AMMContext, column_major
@@ -39,8 +40,11 @@ def main():
     if a.solve:
         ctx = AMMContext(a.m, a.n, c=a.c, step=a.steps, vr_period=a.vr, dtype=a.dtype)
         x0 = torch.randn(a.m, device="cuda", generator=g)
+        gs = torch.Generator().manual_seed(a.seed + 7)
+        states = torch.randint(1, 2**31 - 1, (a.c,), generator=gs, dtype=torch.int64)
+        states = states.to(torch.int32).cuda()
         for rep in range(2):
-            ctx.set_rng_state(torch.arange(1, a.c + 1, dtype=torch.int32, device="cuda"))
+            ctx.set_rng_state(states)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
@@ -50,7 +54,10 @@ def main():
             e1.record()
             e1.synchronize()
             tr = ctx.trace()
-            print(f"solve {a.solve} rep {rep}: {e0.elapsed_time(e1):.3f} ms, kinds {tr['kinds']}")
+            steps_us = np.diff(np.concatenate([[0.0], tr["t_ns"]])) / 1e3
+            print(f"solve {a.solve} rep {rep}: {e0.elapsed_time(e1):.3f} ms, kinds {tr['kinds']}, "
+                  f"distinct {tr['distinct'].tolist()}, step us (device clock) "
+                  f"{np.round(steps_us, 1).tolist()}")
         ctx.close()
         return
     ctx = AMMContext(a.m, a.n, c=a.c, step=2, dtype=a.dtype)
@@ -62,7 +69,7 @@ def main():
     ctx.trace()
     for kind in a.kinds.split(","):
         ms, cd = ctx.benchmark_product(kind, reps=a.reps)
-        byts = a.m * cd * es + (0 if kind == "exact" else 8 * a.c) + 16 * a.m
+        byts = a.m * cd * es + (0 if kind in ("exact", "setup") else 8 * a.c) + 16 * a.m
         print(f"{kind:9s} dtype={a.dtype} m={a.m} n={a.n} c={a.c}: {ms * 1e3:9.2f} us/launch, "
               f"{cd} columns, {byts / ms / 1e6:8.1f} GB/s algorithmic")
     ctx.close()

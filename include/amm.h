@@ -65,6 +65,8 @@ enum amm_step_kind {
   AMM_STEP_PREVIOUS = 2,     /* previous AMM (norm-proportional sampling)                  */
   AMM_STEP_PROPOSED = 3      /* proposed AMM (centred sampling + rank-one correction)      */
 };
+/* amm_benchmark_product: time the set-up pass (not a step kind). */
+#define AMM_PASS_SETUP 16
 
 /* Parameters (the reference's host_memory fields, host_memory.h:26-50, plus n, ld, dtype). */
 typedef struct amm_config {
@@ -183,8 +185,10 @@ int amm_sample_indices(amm_ctx *ctx, int which, uint32_t *d_idx, void *stream);
  * step kind (AMM_STEP_EXACT, AMM_STEP_PREVIOUS or AMM_STEP_PROPOSED) on the bound matrix,
  * with CUDA events on `stream`, from the start vector of the last call (ones before any
  * call).  AMM kinds draw one set of picks from the current states without advancing them.
+ * AMM_PASS_SETUP times the set-up pass instead (column sums, sums of squares and z = A·α in
+ * one read of A; it rewrites the same statistics each time).
  * *ms_per_launch receives the mean time per launch and *distinct the distinct columns read
- * per launch (n for an exact launch).  Synchronises `stream`.  No counterpart in the
+ * per launch (n for an exact launch or the set-up pass).  Synchronises `stream`.  No counterpart in the
  * reference (its per-step timing is cudaEventElapsedTime around whole steps,
  * powerMethod_by_exact.cuh:60-64). */
 int amm_benchmark_product(amm_ctx *ctx, int kind, int reps, float *ms_per_launch,
