@@ -83,6 +83,7 @@ _SIGS = {
     "amm_get_column_stats": [_P, _P, _P, _P, _P, _P, _P, _P],
     "amm_get_sampling_tables": [_P, C.c_int, _P, _P, _P],
     "amm_sample_indices": [_P, C.c_int, _P, _P],
+    "amm_pick_sorted_noalloc": [_P, _P, _I64, _P, C.c_int, _I64, _P, _P, _P],
     "amm_benchmark_product": [_P, C.c_int, C.c_int, _P, _P, _P],
     "amm_grad_lambda": [_P, _P, _P, _I64, _P],
     "amm_get_geometry": [_P, _P],

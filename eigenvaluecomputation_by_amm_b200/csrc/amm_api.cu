@@ -52,6 +52,10 @@ using GraphKey = std::tuple<int, int, double, double, int, int, int, int>;
 
 }  // namespace
 
+namespace amm {
+int record_cuda_failure(cudaError_t e, const char* what) { return cuda_fail(e, what); }
+}  // namespace amm
+
 struct amm_ctx {
   amm_config cfg{};
   int device = 0;

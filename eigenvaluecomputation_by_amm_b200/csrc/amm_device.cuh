@@ -218,4 +218,16 @@ __device__ __forceinline__ bool named_barrier_or(int id, int nthreads, bool pred
   return r != 0;
 }
 
+// ---- the reference's random draw (get_rand, device_memory.h:506-514) ----
+__device__ __forceinline__ uint32_t xorshift32(uint32_t y) {
+  y ^= (y << 13);
+  y ^= (y >> 17);
+  y ^= (y << 5);
+  return y;
+}
+// exact: 1.mantissa - 1 (device_memory.h:513)
+__device__ __forceinline__ float uniform_from(uint32_t y) {
+  return __fsub_rn(__uint_as_float((y & 0x007FFFFFu) | 0x3f800000u), 1.0f);
+}
+
 }  // namespace amm

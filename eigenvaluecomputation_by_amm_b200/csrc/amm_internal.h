@@ -149,6 +149,8 @@ cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, in
 // Draw the picks of the first AMM step after step iter (iter = -1: start of a call); for
 // iter >= 0 it may run concurrently with the product of step iter.
 cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
+// Record a CUDA failure for amm_last_cuda_error and return AMM_ERR_CUDA.
+int record_cuda_failure(cudaError_t e, const char* what);
 // Build the sorted distinct work list of the picks just drawn (same decision as sample_kernel).
 cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
 // One iteration: panel product and reduce/Rayleigh/clear.

@@ -60,16 +60,6 @@ __device__ __forceinline__ int next_amm_weighting(const CallCfg& cc, int i) {
   return 0;
 }
 
-__device__ __forceinline__ uint32_t xorshift32(uint32_t y) {
-  y ^= (y << 13);
-  y ^= (y >> 17);
-  y ^= (y << 5);
-  return y;
-}
-__device__ __forceinline__ float uniform_from(uint32_t y) {
-  // exact: 1.mantissa - 1 (device_memory.h:513)
-  return __fsub_rn(__uint_as_float((y & 0x007FFFFFu) | 0x3f800000u), 1.0f);
-}
 
 // First index i in [0, n) with cdf[i] > target, else n-1 (device_memory.h:529-543).
 // The coarse table (in shared memory) holds cdf[(s+1)*seg - 1] for the ncoarse full segments;

@@ -181,6 +181,21 @@ int amm_get_sampling_tables(amm_ctx *ctx, int which, void *d_cdf, float *d_weigh
  * (pick_index, device_memory.h:516-545) into d_idx (length c, in draw order). */
 int amm_sample_indices(amm_ctx *ctx, int which, uint32_t *d_idx, void *stream);
 
+/* Allocation-free draw and sort (no amm_ctx): advances the c xorshift32 states d_states_in into
+ * d_states_out (may alias), draws one index per state from the inclusive CDF d_cdf (length n,
+ * FP64 or FP32 per cdf_precision) as pick_index does (device_memory.h:506-545), and writes the
+ * c indices in ascending order, repeats included, to d_idx_sorted (as the CUB SortKeys of
+ * powerMethod_by_previous.cuh:63-70) and the number of distinct indices to the device int32
+ * *d_distinct.  No counterpart in the reference: it exists for callers that may not allocate
+ * device memory (a process whose device memory belongs to its own pool, or a loop where an
+ * allocator call is not acceptable); it allocates nothing and works in a fixed 1 MiB static
+ * device array, so n is limited to 262144 (larger n returns AMM_ERR_UNSUPPORTED).  The first
+ * call on each device resolves that array's address and should come before any stream capture.
+ * Calls that overlap in time on one device race on the array: serialise them. */
+int amm_pick_sorted_noalloc(const uint32_t *d_states_in, uint32_t *d_states_out, int64_t c,
+                            const void *d_cdf, int cdf_precision, int64_t n,
+                            uint32_t *d_idx_sorted, int32_t *d_distinct, void *stream);
+
 /* Measurement hook: time `reps` back-to-back launches of the fused product kernel for one
  * step kind (AMM_STEP_EXACT, AMM_STEP_PREVIOUS or AMM_STEP_PROPOSED) on the bound matrix,
  * with CUDA events on `stream`, from the start vector of the last call (ones before any
