@@ -145,12 +145,11 @@ void layout(amm_ctx* ctx, Carver& cv) {
   b.partials = cv.take<float>((size_t)b.nsm * m);
   b.spart = cv.take<float>(b.nsm);
   b.spart64 = cv.take<double>(b.nsm);
-  b.rpart = cv.take<double>(4 * ((m + 127) / 128));
+  b.rpart = cv.take<double>(4 * b.nsm);
   b.ticket = cv.take<uint32_t>(4);
   b.alpha2 = cv.take<double>(1);
   b.colvec = cv.take<float>(n);
   b.cdf_tsum = cv.take<double>(2 * ((n + 4095) / 4096));
-  b.colsum = cv.take<double2>(n);
   b.st = cv.take<amm::IterState>(2);
   b.eigs = cv.take<double>(step);
   b.errs = cv.take<double>(step);
@@ -181,7 +180,8 @@ CallCfg make_cc(const amm_ctx* ctx, int method) {
 int ensure_setup(amm_ctx* ctx, cudaStream_t s);
 
 // The launch sequence of one call (captured into a graph or issued directly):
-//   init, first draw | for each step: product || next draw (forked stream), reduce | finalize
+//   init, first draw + work list | for each step: step kernel (product, reduction, Rayleigh)
+//   || next draw + work list (forked stream) | finalize
 int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
                  cudaStream_t s) {
   const Buffers& b = ctx->b;
@@ -206,8 +206,8 @@ int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normal
       AMM_CUDA(cudaEventRecord(ctx->ev_join, ctx->side_stream));
     }
     AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, s));
+    // the next step reads the work list built on the side stream
     if (fork) AMM_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
-    AMM_CUDA(amm::launch_iter_reduce(b, cc, i, s));
   }
   AMM_CUDA(amm::launch_finalize(b, cc, ctx->x_final, ctx->y_final, s));
   return AMM_OK;
@@ -253,7 +253,7 @@ int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
     it = ctx->graphs.emplace(key, std::make_pair(g, ex)).first;
   }
   AMM_CUDA(cudaGraphLaunch(it->second.second, s));
-  amm::count_launch(2 + 2 * cc.step + ((cc.uses_amm && !cc.sanity) ? 2 * cc.step : 0));
+  amm::count_launch(2 + cc.step + ((cc.uses_amm && !cc.sanity) ? 2 * cc.step : 0));
   return AMM_OK;
 }
 
@@ -267,8 +267,8 @@ int check_ready(amm_ctx* ctx) {
 // accessors; exact calls never need it.
 int ensure_setup(amm_ctx* ctx, cudaStream_t s) {
   if (ctx->setup_done) return AMM_OK;
+  AMM_CUDA(cudaMemsetAsync(ctx->b.ticket, 0, sizeof(uint32_t) * 4, s));
   AMM_CUDA(amm::launch_setup_panel(ctx->b, ctx->geom, s));
-  AMM_CUDA(amm::launch_setup_reduce(ctx->b, s));
   AMM_CUDA(amm::launch_build_cdf(ctx->b, -1, 0, ctx->sanity_active, s));
   ctx->setup_done = true;
   return AMM_OK;

@@ -230,4 +230,96 @@ __device__ __forceinline__ float uniform_from(uint32_t y) {
   return __fsub_rn(__uint_as_float((y & 0x007FFFFFu) | 0x3f800000u), 1.0f);
 }
 
+// Kind of the step that follows, as the reference's drivers decide it:
+//  previous    powerMethod_by_previous.cuh:135-137
+//  proposed    powerMethod_by_proposed.cuh:371-373 (no VR right after a VR step)
+//  proposed_v2 powerMethod_by_proposed_v2.cuh:234-305
+__device__ __forceinline__ int decide_mode(const CallCfg& cc, int i, double cos_prev, int last_exact,
+                           int* le_out) {
+  *le_out = last_exact;
+  const bool periodic = cc.vr_period > 0 && (i + 1) % cc.vr_period == 0;
+  const bool adaptive = cc.vr_thr > 0.0 && cos_prev > 1.0 - cc.vr_thr;
+  switch (cc.method) {
+    case kMethodPrevious:
+      return (cc.variance_reduction && (periodic || adaptive)) ? kExactMemo : kPrevious;
+    case kMethodProposed:
+      if (i > last_exact + 1 && cc.variance_reduction && (periodic || adaptive)) {
+        *le_out = i;
+        return kExactMemo;
+      }
+      return kProposed;
+    case kMethodProposedV2:
+      if (i < cc.vr_period - 1) return kPrevious;
+      if (i == cc.vr_period - 1) return kExact;
+      return (cc.variance_reduction && periodic) ? kExactMemo : kProposed;
+    default:
+      return kExact;
+  }
+}
+
+// The step's scalars from the summed x·y, y·y and y·v* (dotProduct_and_generate_x,
+// common.h:103-153): λ = x·y, err = y·v*/‖y‖, cos = λ/‖y‖, the trace entries and the state of
+// the next step (its kind, the tolerance stop).  Run by one thread once the sums are final.
+__device__ __forceinline__ void finish_step(const Buffers& b, const CallCfg& cc, int i,
+                                            const IterState& st, double xy, double yy,
+                                            double yv) {
+  const bool consumed = st.mode == kPrevious || st.mode == kProposed;
+  const double scale = rsqrt(yy);
+  const double lam = xy;
+  const double err = yv * scale;
+  const double cosv = lam * scale;
+  b.eigs[i] = lam;
+  b.errs[i] = err;
+  b.coss[i] = cosv;
+  b.kinds[i] = st.mode;
+  if (!consumed || cc.sanity) b.distinct_hist[i] = b.n;
+  b.tstamp[i + 1] = globaltimer_now();
+  IterState nx = st;
+  nx.scale = (float)scale;
+  nx.cos_prev = cosv;
+  nx.lam_prev = lam;
+  nx.steps_run = i + 1;
+  if (consumed && !cc.sanity) {
+    nx.sb = st.sb ^ 1;
+    nx.pb = st.pb ^ 1;
+  }
+  bool done = false;
+  if (!isfinite(lam) || !isfinite(scale)) {
+    atomicOr(b.status, (uint32_t)kDevNonFinite);
+    done = true;
+  }
+  if (cc.tol > 0.0 && i >= 1 && fabs(lam - st.lam_prev) <= cc.tol * fabs(lam)) done = true;
+  nx.done = done ? 1 : 0;
+  int le;
+  nx.mode = decide_mode(cc, i + 1, cosv, st.last_exact, &le);
+  nx.last_exact = le;
+  b.st[(i + 1) & 1] = nx;
+}
+
+// ---- grid-wide barrier over co-resident CTAs ----
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Called by one thread per CTA after the CTA's own writes are ordered before it (a CTA barrier).
+// bar counts arrivals without reset (a call's first kernel zeroes it); every launch adds exactly
+// nblocks arrivals, so a barrier completes when the count reaches the next multiple of nblocks.
+// Every CTA of the grid must be resident at once (one per SM).  Bounded: returns false if the
+// count did not reach the target within kWaitLimitNs.
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t nblocks) {
+  __threadfence();
+  const uint32_t old = atomicAdd(bar, 1u);
+  const uint32_t target = (old / nblocks + 1u) * nblocks;
+  const unsigned long long t0 = globaltimer_now();
+  for (uint32_t it = 0;; ++it) {
+    if ((int32_t)(ld_acquire_gpu(bar) - target) >= 0) break;
+    if ((it & 31u) == 31u && globaltimer_now() - t0 > kWaitLimitNs) return false;
+    __nanosleep(20);
+  }
+  __threadfence();
+  return true;
+}
+
 }  // namespace amm

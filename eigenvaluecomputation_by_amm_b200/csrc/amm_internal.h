@@ -19,7 +19,7 @@ constexpr int kSeg = 32;           // fine-search window of the sampler (element
 constexpr int kCoarseMax = 2048;   // coarse CDF table entries held in shared memory
 
 // Iteration state, double-buffered by iteration parity: kernels of iteration i read
-// st[i & 1]; the last CTA of the reduce kernel of iteration i writes st[(i + 1) & 1].
+// st[i & 1]; the last CTA of the step kernel of iteration i writes st[(i + 1) & 1].
 struct IterState {
   int32_t mode;        // StepKind of this iteration
   int32_t last_exact;  // proposed AMM: index of the last VR step
@@ -33,8 +33,6 @@ struct IterState {
   float pad2;
   double cos_prev;     // cos of the previous step (adaptive VR)
   double lam_prev;     // λ of the previous step (tolerance stop)
-  double sum_dx;       // Σ(x_i − x_memo)    (proposed)
-  double zdx;          // z·(x_i − x_memo)   (proposed)
 };
 
 // Static description of one power-method call, passed by value to the kernels.
@@ -97,12 +95,12 @@ struct Buffers {
   float* partials;     // nsm x m
   float* spart;        // nsm  (Σ α_k t_k of each CTA, proposed)
   double* spart64;     // nsm  (Σ α_j² of each CTA, set-up)
-  double* rpart;       // reduce CTAs x 4 (x·y, y·y, y·v*, spare)
-  uint32_t* ticket;    // last-CTA counters [0]: reduce, [1]: small kernels
+  double* rpart;       // nsm x 4 (x·y, y·y, y·v*, z·dx) of each CTA
+  uint32_t* ticket;    // [0]: last-CTA ticket of a step, [2]: grid-barrier arrivals,
+                       // [1], [3]: spare
   double* alpha2;      // ‖α‖²
   float* colvec;       // n floats of scratch (vᵀA for the gradient)
   double* cdf_tsum;    // 2 x ceil(n/4096) tile sums of the CDF build
-  double2* colsum;     // n (Σa, Σa²) of each column from the set-up pass
   // iteration state and traces
   IterState* st;       // [2]
   double* eigs;
@@ -135,10 +133,9 @@ struct PanelGeom {
 bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g);
 
 // ---- launchers (amm_kernels.cu); each returns the cudaError_t of the launch ----
-// Set-up pass over A: column statistics and per-CTA partial sums of z = A·α.
+// Set-up pass over A (amm_panel.cu): column statistics (α, ‖A_j‖, ‖A_j − α_j‖), z = A·α,
+// v = z − ‖α‖² and ‖α‖², in one read of A.
 cudaError_t launch_setup_panel(const Buffers& b, const PanelGeom& g, cudaStream_t s);
-// Reduce the set-up partials into z and v = z − ‖α‖².
-cudaError_t launch_setup_reduce(const Buffers& b, cudaStream_t s);
 // Build the CDFs, weights and coarse tables of both weightings (or one if which >= 0,
 // keeping an imported CDF when keep_cdf is set).
 cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sanity, cudaStream_t s);
@@ -153,10 +150,10 @@ cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStr
 int record_cuda_failure(cudaError_t e, const char* what);
 // Build the sorted distinct work list of the picks just drawn (same decision as sample_kernel).
 cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
-// One iteration: panel product and reduce/Rayleigh/clear.
+// One step (amm_panel.cu): the product, the grid-wide reduction of the partials into y, the
+// Rayleigh quotient and the next step's state.
 cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
                               cudaStream_t s);
-cudaError_t launch_iter_reduce(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
 // x_final = scale * y_last into dst (length m); y_last into ydst (optional); commits the
 // sampling states to states[0] and clears any pending picks.
 cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, float* ydst,

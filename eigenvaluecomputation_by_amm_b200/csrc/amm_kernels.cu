@@ -25,33 +25,6 @@ static std::atomic<int64_t> g_launches{0};
 void count_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
-// Kind of the step that follows, as the reference's drivers decide it:
-//  previous    powerMethod_by_previous.cuh:135-137
-//  proposed    powerMethod_by_proposed.cuh:371-373 (no VR right after a VR step)
-//  proposed_v2 powerMethod_by_proposed_v2.cuh:234-305
-__device__ int decide_mode(const CallCfg& cc, int i, double cos_prev, int last_exact,
-                           int* le_out) {
-  *le_out = last_exact;
-  const bool periodic = cc.vr_period > 0 && (i + 1) % cc.vr_period == 0;
-  const bool adaptive = cc.vr_thr > 0.0 && cos_prev > 1.0 - cc.vr_thr;
-  switch (cc.method) {
-    case kMethodPrevious:
-      return (cc.variance_reduction && (periodic || adaptive)) ? kExactMemo : kPrevious;
-    case kMethodProposed:
-      if (i > last_exact + 1 && cc.variance_reduction && (periodic || adaptive)) {
-        *le_out = i;
-        return kExactMemo;
-      }
-      return kProposed;
-    case kMethodProposedV2:
-      if (i < cc.vr_period - 1) return kPrevious;
-      if (i == cc.vr_period - 1) return kExact;
-      return (cc.variance_reduction && periodic) ? kExactMemo : kProposed;
-    default:
-      return kExact;
-  }
-}
-
 // Weighting (0 = ‖A_j‖², 1 = ‖A_j − α_j‖²) of the first AMM step after step i.
 __device__ __forceinline__ int next_amm_weighting(const CallCfg& cc, int i) {
   if (cc.method == kMethodPrevious) return 0;
@@ -145,249 +118,6 @@ __device__ void load_coarse(const Buffers& b, int which, F* coarse_s) {
   const F* __restrict__ csrc = src;
   for (int k = threadIdx.x; k < b.ncoarse; k += blockDim.x) coarse_s[k] = __ldg(csrc + k);
   __syncthreads();
-}
-
-// Clear the picks of buffer pb (consumed by the last product): every counted column and
-// every chunk total, so that the buffer is all-zero before its next draw.
-__device__ void clear_picks(const Buffers& b, int pb, int rank, int nranks) {
-  const int tid = rank * blockDim.x + threadIdx.x;
-  const int nthr = nranks * blockDim.x;
-  uint32_t* cnt = b.count[pb];
-  const uint32_t* smp = b.samples[pb];
-  for (int k = tid; k < b.c; k += nthr) cnt[smp[k]] = 0u;
-  for (int k = tid; k < b.nchunks; k += nthr) b.chunk[pb][k] = 0u;
-}
-
-// ------------------------------------------------------------------------------------------
-// Reduce kernels
-// ------------------------------------------------------------------------------------------
-constexpr int kRedThreads = 256;
-constexpr int kRedRows = 128;  // rows per reduce CTA: 32 float4 groups x 8 partial slices
-
-// Deterministic sum over the nsm partials of 4 rows starting at row (FP64, fixed order).  Slice
-// ps of the 8 owns partials ps, ps+8, ps+16, ...; every load of a slice is issued before the
-// first add, so a reduce costs about one L2 round trip instead of one per partial.
-constexpr int kRedSlices = 8;
-constexpr int kRedUnroll = 19;  // 8 x 19 = 152 partials per round (one round for 148 SMs)
-
-__device__ __forceinline__ void reduce_rows(const Buffers& b, int row, double4 (*red)[32],
-                                            double4* out) {
-  const int rg = threadIdx.x & 31, ps = threadIdx.x >> 5;
-  double4 acc = make_double4(0, 0, 0, 0);
-  if (row < b.m) {
-    const float* __restrict__ P = b.partials + row;
-    for (int k0 = ps; k0 < b.nsm; k0 += kRedSlices * kRedUnroll) {
-      float4 v[kRedUnroll];
-#pragma unroll
-      for (int u = 0; u < kRedUnroll; ++u) {
-        const int k = k0 + u * kRedSlices;
-        v[u] = k < b.nsm ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * b.m))
-                         : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int u = 0; u < kRedUnroll; ++u) {
-        acc.x += v[u].x;
-        acc.y += v[u].y;
-        acc.z += v[u].z;
-        acc.w += v[u].w;
-      }
-    }
-  }
-  red[ps][rg] = acc;
-  __syncthreads();
-  if (ps == 0) {
-    double4 s = red[0][rg];
-    for (int k = 1; k < kRedSlices; ++k) {
-      s.x += red[k][rg].x;
-      s.y += red[k][rg].y;
-      s.z += red[k][rg].z;
-      s.w += red[k][rg].w;
-    }
-    *out = s;
-  }
-}
-
-__global__ void __launch_bounds__(kRedThreads) setup_reduce_kernel(const __grid_constant__ Buffers b) {
-  __shared__ double4 red[8][32];
-  __shared__ double a2s;
-  const int t = threadIdx.x;
-  if (t < 32) {
-    double s = 0.0;
-    for (int k = t; k < b.nsm; k += 32) s += b.spart64[k];
-    s = warp_sum(s);
-    if (t == 0) a2s = s;
-  }
-  const int row = blockIdx.x * kRedRows + (t & 31) * 4;
-  double4 z;
-  reduce_rows(b, row, red, &z);
-  __syncthreads();
-  const double a2 = a2s;
-  if (t < 32 && row < b.m) {
-    const float4 zf = make_float4((float)z.x, (float)z.y, (float)z.z, (float)z.w);
-    *reinterpret_cast<float4*>(b.z + row) = zf;
-    *reinterpret_cast<float4*>(b.v + row) =
-        make_float4((float)((double)zf.x - a2), (float)((double)zf.y - a2),
-                    (float)((double)zf.z - a2), (float)((double)zf.w - a2));
-  }
-  if (blockIdx.x == 0 && t == 0) *b.alpha2 = a2;
-}
-
-// Per-column statistics from the set-up pass's FP64 column sums (get_norms,
-// device_memory.h:34-59): α = Σ/m, ‖A_j‖ = sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² − mean²·m) clamped
-// at 0 (the reference stores NaN when cancellation makes it negative).
-__global__ void __launch_bounds__(256) column_stats_kernel(const __grid_constant__ Buffers b) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < b.n; j += gridDim.x * blockDim.x) {
-    const double2 s = b.colsum[j];
-    const double mean = s.x / (double)b.m;
-    b.alpha[j] = (float)mean;
-    b.norm[j] = (float)sqrt(s.y);
-    b.normp[j] = (float)sqrt(fmax(s.y - mean * mean * (double)b.m, 0.0));
-  }
-}
-
-struct ReduceArgs {
-  Buffers b;
-  CallCfg cc;
-  int iter;
-  int nred;
-};
-
-__global__ void __launch_bounds__(kRedThreads) reduce_kernel(const __grid_constant__ ReduceArgs a) {
-  const Buffers& b = a.b;
-  const CallCfg& cc = a.cc;
-  const int t = threadIdx.x;
-  const IterState st = b.st[a.iter & 1];
-  IterState* st_next = &b.st[(a.iter + 1) & 1];
-  if (st.done) {
-    if (blockIdx.x == 0 && t == 0) *st_next = st;
-    return;
-  }
-  const bool consumed = (st.mode == kPrevious || st.mode == kProposed);
-
-  if ((int)blockIdx.x >= a.nred) {
-    // the picks this step consumed are cleared while the sums are reduced (the next picks were
-    // drawn into the other buffer by sample_kernel, concurrently with the product)
-    if (consumed && !cc.sanity) clear_picks(b, st.pb, blockIdx.x - a.nred, gridDim.x - a.nred);
-    return;
-  }
-
-  __shared__ double4 red[8][32];
-  __shared__ double s_shared;
-  __shared__ int is_last;
-  if (t < 32) {
-    double s = 0.0;
-    if (st.mode == kProposed)
-      for (int k = t; k < b.nsm; k += 32) s += (double)b.spart[k];
-    s = warp_sum(s);
-    if (t == 0) s_shared = s;
-  }
-  const int row = blockIdx.x * kRedRows + (t & 31) * 4;
-  double4 tot;
-  reduce_rows(b, row, red, &tot);
-  __syncthreads();
-  if (t < 32) {
-    double xy = 0.0, yy = 0.0, yv = 0.0;
-    if (row < b.m) {
-      const float* yprev = b.y[(a.iter + 1) & 1];
-      const float4 yp = *reinterpret_cast<const float4*>(yprev + row);
-      const float4 xi = make_float4(__fmul_rn(st.scale, yp.x), __fmul_rn(st.scale, yp.y),
-                                    __fmul_rn(st.scale, yp.z), __fmul_rn(st.scale, yp.w));
-      double tv[4] = {tot.x, tot.y, tot.z, tot.w};
-      float yo[4];
-      const float xa[4] = {xi.x, xi.y, xi.z, xi.w};
-      if (st.mode == kExact || st.mode == kExactMemo) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) yo[e] = (float)tv[e];
-      } else {
-        const float4 ym = *reinterpret_cast<const float4*>(b.y_memo + row);
-        const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
-        if (st.mode == kPrevious) {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) yo[e] = (float)((double)ymv[e] + tv[e]);
-        } else {
-          // y_memo + Σdx·v + z·dx in FP64, rounded (core_proposedAMM.cuh:198-212)
-          const float4 vv = *reinterpret_cast<const float4*>(b.v + row);
-          const float va[4] = {vv.x, vv.y, vv.z, vv.w};
-          const double S = s_shared;
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const float base = (float)(fma(st.sum_dx, (double)va[e], st.zdx) + (double)ymv[e]);
-            yo[e] = (float)((double)base + (tv[e] - S));
-          }
-        }
-      }
-      *reinterpret_cast<float4*>(b.y[a.iter & 1] + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
-      if (st.mode == kExactMemo) {
-        *reinterpret_cast<float4*>(b.x_memo + row) = xi;
-        *reinterpret_cast<float4*>(b.y_memo + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
-      }
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const double yd = (double)yo[e];
-        xy = fma(yd, (double)xa[e], xy);
-        yy = fma(yd, yd, yy);
-        if (b.has_vstar) yv = fma(yd, b.vstar[row + e], yv);
-      }
-    }
-    xy = warp_sum(xy);
-    yy = warp_sum(yy);
-    yv = warp_sum(yv);
-    if (t == 0) {
-      b.rpart[4 * blockIdx.x + 0] = xy;
-      b.rpart[4 * blockIdx.x + 1] = yy;
-      b.rpart[4 * blockIdx.x + 2] = yv;
-      __threadfence();
-      const uint32_t old = atomicAdd(&b.ticket[0], 1u);
-      is_last = (old == (uint32_t)(a.nred - 1));
-    }
-  }
-  __syncthreads();
-  if (!is_last || t >= 32) return;
-  __threadfence();
-  // last CTA: Rayleigh quotient and the next step (common.h:103-153).  Warp 0 sums the CTA
-  // partials lane-strided and then by an xor butterfly: a fixed association order.
-  double xy = 0.0, yy = 0.0, yv = 0.0;
-  for (int k = t; k < a.nred; k += 32) {
-    xy += __ldcg(b.rpart + 4 * k + 0);
-    yy += __ldcg(b.rpart + 4 * k + 1);
-    yv += __ldcg(b.rpart + 4 * k + 2);
-  }
-  xy = warp_sum(xy);
-  yy = warp_sum(yy);
-  yv = warp_sum(yv);
-  if (t != 0) return;
-  b.ticket[0] = 0u;
-  const double scale = rsqrt(yy);
-  const double lam = xy;
-  const double err = yv * scale;
-  const double cosv = lam * scale;
-  const int i = a.iter;
-  b.eigs[i] = lam;
-  b.errs[i] = err;
-  b.coss[i] = cosv;
-  b.kinds[i] = st.mode;
-  if (!consumed || cc.sanity) b.distinct_hist[i] = b.n;
-  b.tstamp[i + 1] = globaltimer_ns();
-  IterState nx = st;
-  nx.scale = (float)scale;
-  nx.cos_prev = cosv;
-  nx.lam_prev = lam;
-  nx.steps_run = i + 1;
-  if (consumed && !cc.sanity) {
-    nx.sb = st.sb ^ 1;
-    nx.pb = st.pb ^ 1;
-  }
-  bool done = false;
-  if (!isfinite(lam) || !isfinite(scale)) {
-    atomicOr(b.status, (uint32_t)kDevNonFinite);
-    done = true;
-  }
-  if (cc.tol > 0.0 && i >= 1 && fabs(lam - st.lam_prev) <= cc.tol * fabs(lam)) done = true;
-  nx.done = done ? 1 : 0;
-  int le;
-  nx.mode = decide_mode(cc, i + 1, cosv, st.last_exact, &le);
-  nx.last_exact = le;
-  *st_next = nx;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -538,6 +268,8 @@ __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ Init
   if ((t & 31) == 0) ws[t >> 5] = ss;
   __syncthreads();
   if (t == 0) {
+    b.ticket[0] = 0u;  // the step kernels' last-CTA ticket and grid-barrier count
+    b.ticket[2] = 0u;
     double s = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += ws[w];
     IterState st{};
@@ -560,6 +292,8 @@ __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ Init
   }
 }
 
+constexpr int kFinalThreads = 256;
+
 struct FinalArgs {
   Buffers b;
   CallCfg cc;
@@ -567,7 +301,7 @@ struct FinalArgs {
   float* ydst;
 };
 
-__global__ void __launch_bounds__(kRedThreads) finalize_kernel(const __grid_constant__ FinalArgs a) {
+__global__ void __launch_bounds__(kFinalThreads) finalize_kernel(const __grid_constant__ FinalArgs a) {
   const Buffers& b = a.b;
   const IterState st = b.st[a.cc.step & 1];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
@@ -897,21 +631,6 @@ __global__ void __launch_bounds__(256) grad_outer_kernel(const float* v, const f
 // ------------------------------------------------------------------------------------------
 // Host launchers
 // ------------------------------------------------------------------------------------------
-static int reduce_ctas(int m) { return (m + kRedRows - 1) / kRedRows; }
-static int clear_ctas(int c) {
-  int k = (c + kRedThreads * 4 - 1) / (kRedThreads * 4);
-  return k < 1 ? 1 : (k > 64 ? 64 : k);
-}
-
-cudaError_t launch_setup_reduce(const Buffers& b, cudaStream_t s) {
-  setup_reduce_kernel<<<reduce_ctas(b.m), kRedThreads, 0, s>>>(b);
-  int blocks = (b.n + 255) / 256;
-  if (blocks > 4096) blocks = 4096;
-  column_stats_kernel<<<blocks, 256, 0, s>>>(b);
-  count_launch(2);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sanity,
                              cudaStream_t s) {
   const int ntiles = (b.n + kCdfTile - 1) / kCdfTile;
@@ -936,18 +655,6 @@ cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, in
   a.x0 = x0;
   a.no_normalize = no_normalize;
   init_kernel<<<1, 1024, 0, s>>>(a);
-  count_launch();
-  return cudaGetLastError();
-}
-
-cudaError_t launch_iter_reduce(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s) {
-  ReduceArgs a{};
-  a.b = b;
-  a.cc = cc;
-  a.iter = iter;
-  a.nred = reduce_ctas(b.m);
-  const int ns = (cc.uses_amm && !cc.sanity) ? clear_ctas(b.c) : 0;
-  reduce_kernel<<<a.nred + ns, kRedThreads, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }
@@ -985,9 +692,9 @@ cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, fl
   a.cc = cc;
   a.xdst = xdst;
   a.ydst = ydst;
-  int blocks = (b.m + kRedThreads - 1) / kRedThreads;
+  int blocks = (b.m + kFinalThreads - 1) / kFinalThreads;
   if (blocks > 256) blocks = 256;
-  finalize_kernel<<<blocks, kRedThreads, 0, s>>>(a);
+  finalize_kernel<<<blocks, kFinalThreads, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }

@@ -65,7 +65,7 @@ __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup
   int o = 0;
   L.stages = o;
   o += g.stage_area;
-  L.bars = o;  // full[8] empty[8]
+  L.bars = o;  // full[8]
   o += 8 * 16;
   L.redw = o;  // [2][16 warps][GC]; also 16 x 2 doubles of prologue scratch
   int rw = 2 * 16 * g.gc * rsz;
@@ -244,7 +244,7 @@ __device__ __forceinline__ void fused_block_setup(const unsigned char* cur, cons
 }
 
 template <typename Elem, int R, int GC, bool SETUP>
-__global__ void __launch_bounds__(kMaxThreads + 32, 1)
+__global__ void __launch_bounds__(kMaxThreads, 1)
     panel_kernel(const __grid_constant__ PanelArgs a) {
   using RT = typename RedT<SETUP>::T;
   constexpr int E = 16 / static_cast<int>(sizeof(Elem));
@@ -252,8 +252,8 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
   const Buffers& b = a.b;
   const PanelGeom& g = a.g;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int T = blockDim.x - 32;              // consumer threads
-  const int ncw = T >> 5;                     // consumer warps
+  const int T = blockDim.x;  // threads: all consume; thread 0 also issues the copies
+  const int ncw = T >> 5;    // warps
   const int G = gridDim.x;
   const int q = blockIdx.x;
   const int m = b.m;
@@ -265,34 +265,36 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
   const SmemLayout L = smem_layout(g, SETUP);
   unsigned char* stages = smem + L.stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
-  uint64_t* empty = full + 8;
   RT* redw = reinterpret_cast<RT*>(smem + L.redw);
   uint32_t* wl_idx = reinterpret_cast<uint32_t*>(smem + L.wl_idx);
   float* wl_w = reinterpret_cast<float*>(smem + L.wl_w);
   float* wl_al = reinterpret_cast<float*>(smem + L.wl_al);
+  __shared__ IterState st_s;  // the step state, for the last CTA's epilogue
 
+  if (t == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();  // barrier initialisation visible to every thread
+
+  // The loads of the prologue are issued together, before anything depends on them: the step
+  // state, both work-list lengths (the pick buffer is known only with the state) and this
+  // thread's rows of y_{i-1} and x_memo.
   int mode = kExact, pb = 0, done = 0;
   float scale = 0.f;
+  uint32_t cd_buf[2] = {0u, 0u};
   if (!SETUP) {
     const IterState& st = b.st[a.iter & 1];
     done = st.done;
     mode = st.mode;
     pb = st.pb;
     scale = st.scale;
+    cd_buf[0] = __ldg(b.wl_count[0]);
+    cd_buf[1] = __ldg(b.wl_count[1]);
   }
-  if (done) return;  // uniform over the grid
   const bool amm = !SETUP && (mode == kPrevious || mode == kProposed);
   const bool centred = !SETUP && mode == kProposed;
   const bool sampled = amm && !a.cc.sanity;
-  const int which = centred ? 1 : 0;
-
-  if (t == 0) {
-    for (int s = 0; s < NS; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
-    }
-    fence_barrier_init();
-  }
 
   // ---- this CTA's column list: a contiguous slice of the sorted work list ------------------
   int64_t lo, hi;
@@ -300,24 +302,89 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
     lo = (int64_t)q * b.n / G;
     hi = (int64_t)(q + 1) * b.n / G;
   } else {
-    const uint32_t cd = __ldg(b.wl_count[pb]);
+    const uint32_t cd = pb ? cd_buf[1] : cd_buf[0];
     lo = (int64_t)q * cd / G;
     hi = (int64_t)(q + 1) * cd / G;
-    if (q == 0 && t == 0) b.distinct_hist[a.iter] = (int32_t)cd;
+    if (q == 0 && t == 0 && !done) b.distinct_hist[a.iter] = (int32_t)cd;
   }
   const int nb = (int)(hi - lo);
   const int ngroups = (nb + GC - 1) / GC;
-  __syncthreads();  // barrier initialisation visible to every thread
-  if (warp == ncw) {
-    if (sampled) {
-      for (int k = lane; k < nb; k += 32) wl_idx[k] = __ldg(b.wl_col[pb] + lo + k);
-      __syncwarp();
+
+  // Stage s of group grp is refilled by thread 0 once every thread is past the group that
+  // last used it (the CTA barrier at the end of each group): there is no producer warp.
+  const uint64_t policy = l2_evict_first_policy();
+  const size_t col_stride = (size_t)b.ld * sizeof(Elem);
+  const unsigned char* Abase = reinterpret_cast<const unsigned char*>(b.A);
+  auto issue = [&](int grp, const uint32_t* cols) {
+    const int s = grp % NS;
+    const int c0 = grp * GC;
+    const int cnt = min(GC, nb - c0);
+    mbar_arrive_expect_tx(&full[s], (uint32_t)cnt * col_bytes);
+    for (int qq = 0; qq < cnt; ++qq) {
+      const uint32_t col = sampled ? cols[c0 + qq] : (uint32_t)(lo + c0 + qq);
+      bulk_g2s(stages + ((size_t)s * GC + qq) * col_bytes, Abase + (size_t)col * col_stride,
+               col_bytes, &full[s], policy);
     }
-  } else if (amm) {
-    // coefficient data of the slice; published to the consumer warps by the named barrier
-    // ahead of the first group
+  };
+
+  // ---- dx = x_i − x_memo on this thread's rows, x_i = scale·y_{i−1} (FP32 multiply) ----
+  // The loads are issued before the first copies, the arithmetic after them.
+  float4 ypv[R][E / 4], xmv[R][E / 4];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int vi = t + r * T;
+#pragma unroll
+    for (int h4 = 0; h4 < E / 4; ++h4) {
+      ypv[r][h4] = make_float4(0.f, 0.f, 0.f, 0.f);
+      xmv[r][h4] = ypv[r][h4];
+      if (!SETUP && vi < nvec) {
+        const int o4 = vi * (E / 4) + h4;
+        ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(a.iter + 1) & 1]) + o4);
+        // x_memo is read only by calls that draw samples (it is zero for exact steps, whose
+        // kind is not known before the state arrives)
+        if (a.cc.uses_amm) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
+      }
+    }
+  }
+  if (t == 0 && !done && ngroups > 0) {  // the first NS groups
+    uint32_t first[8 * 8];
+    const int nf = min(NS * GC, nb);
+    if (sampled)
+      for (int k = 0; k < nf; ++k) first[k] = __ldg(b.wl_col[pb] + lo + k);
+    for (int grp = 0; grp < NS && grp < ngroups; ++grp) issue(grp, first);
+  }
+  if (!SETUP && t == 0) st_s = b.st[a.iter & 1];
+  float2 dx[R][H];
+  float2 yacc[R][H];
+  double sum_dx = 0.0, zdx = 0.0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+#pragma unroll
+    for (int h4 = 0; h4 < E / 4; ++h4) {
+      const float4 yp = ypv[r][h4];
+      const float4 xm = amm ? xmv[r][h4] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float d0 = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
+      const float d1 = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
+      const float d2 = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
+      const float d3 = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
+      dx[r][2 * h4] = make_float2(d0, d1);
+      dx[r][2 * h4 + 1] = make_float2(d2, d3);
+      if (centred) sum_dx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int h = 0; h < H; ++h) yacc[r][h] = make_float2(0.f, 0.f);
+  if (done) {  // uniform over the grid: the state passes on unchanged
+    if (q == 0 && t == 0) b.st[(a.iter + 1) & 1] = b.st[a.iter & 1];
+    return;
+  }
+  if (amm) {
+    // coefficient data of the slice; published by the CTA barrier ahead of the first group
     for (int k = t; k < nb; k += T) {
       if (sampled) {
+        wl_idx[k] = __ldg(b.wl_col[pb] + lo + k);
         wl_w[k] = __ldg(b.wl_wm[pb] + lo + k);
         wl_al[k] = __ldg(b.wl_al[pb] + lo + k);
       } else {  // sanity mode: identity list, weight 1
@@ -326,95 +393,14 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
       }
     }
   }
-
-  if (warp == ncw) {
-    // ================================ producer warp ================================
-    if (lane == 0) {
-      const uint64_t policy = l2_evict_first_policy();
-      const size_t col_stride = (size_t)b.ld * sizeof(Elem);
-      const unsigned char* Abase = reinterpret_cast<const unsigned char*>(b.A);
-      for (int grp = 0; grp < ngroups; ++grp) {
-        const int s = grp % NS;
-        const int use = grp / NS;
-        if (use >= 1 && !mbar_wait_bounded(&empty[s], (uint32_t)((use - 1) & 1))) {
-          atomicOr(b.status, (uint32_t)kDevTimeout);
-          break;
-        }
-        const int c0 = grp * GC;
-        const int cnt = min(GC, nb - c0);
-        mbar_arrive_expect_tx(&full[s], (uint32_t)cnt * col_bytes);
-        for (int qq = 0; qq < cnt; ++qq) {
-          const uint32_t col = sampled ? wl_idx[c0 + qq] : (uint32_t)(lo + c0 + qq);
-          bulk_g2s(stages + ((size_t)s * GC + qq) * col_bytes, Abase + (size_t)col * col_stride,
-                   col_bytes, &full[s], policy);
-        }
-      }
-    }
-    return;
-  }
-
-  // ================================= consumer warps ==================================
-  // dx = x_i − x_memo on this thread's rows, x_i = scale·y_{i−1} (FP32 multiply)
-  float2 dx[R][H];
-  float2 yacc[R][H];
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int h = 0; h < H; ++h) {
-      dx[r][h] = make_float2(0.f, 0.f);
-      yacc[r][h] = make_float2(0.f, 0.f);
-    }
-  double sum_dx = 0.0, zdx = 0.0;
-  if (!SETUP) {
-    const float* yprev = b.y[(a.iter + 1) & 1];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int vi = t + r * T;
-      if (vi < nvec) {
-#pragma unroll
-        for (int h4 = 0; h4 < E / 4; ++h4) {
-          const int o4 = vi * (E / 4) + h4;
-          const float4 yp = reinterpret_cast<const float4*>(yprev)[o4];
-          float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (amm) xm = reinterpret_cast<const float4*>(b.x_memo)[o4];
-          const float d0 = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
-          const float d1 = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
-          const float d2 = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
-          const float d3 = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
-          dx[r][2 * h4] = make_float2(d0, d1);
-          dx[r][2 * h4 + 1] = make_float2(d2, d3);
-          if (centred) {
-            const float4 z4 = reinterpret_cast<const float4*>(b.z)[o4];
-            sum_dx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
-            zdx = fma((double)d0, (double)z4.x, zdx);
-            zdx = fma((double)d1, (double)z4.y, zdx);
-            zdx = fma((double)d2, (double)z4.z, zdx);
-            zdx = fma((double)d3, (double)z4.w, zdx);
-          }
-        }
-      }
-    }
-  }
-  if (centred) {  // Σdx and z·dx over all m rows (common.h:55-87), identical in every CTA
+  if (centred) {  // Σdx over all m rows (dots, common.h:55-87), identical in every CTA
     sum_dx = warp_sum(sum_dx);
-    zdx = warp_sum(zdx);
     double* wtmp = reinterpret_cast<double*>(redw);
-    if (lane == 0) {
-      wtmp[2 * warp] = sum_dx;
-      wtmp[2 * warp + 1] = zdx;
-    }
+    if (lane == 0) wtmp[warp] = sum_dx;
     named_barrier_or(1, T, false);
     sum_dx = 0.0;
-    zdx = 0.0;
-    for (int w = 0; w < ncw; ++w) {
-      sum_dx += wtmp[2 * w];
-      zdx += wtmp[2 * w + 1];
-    }
+    for (int w = 0; w < ncw; ++w) sum_dx += wtmp[w];
     named_barrier_or(1, T, false);  // wtmp (= redw) is reused below
-    if (q == 0 && t == 0) {
-      b.st[a.iter & 1].sum_dx = sum_dx;
-      b.st[a.iter & 1].zdx = zdx;
-    }
   }
   const float sum_dx_f = (float)sum_dx;
 
@@ -564,7 +550,16 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
           const float af = (float)(sx / (double)m);
           coef[qq] = af;
           a2acc = fma((double)af, (double)af, a2acc);
-          if (t == qq) b.colsum[lo + k] = make_double2(sx, sxy[2 * qq + 1]);
+          if (t == qq) {
+            // the column statistics (get_norms, device_memory.h:34-59): α = Σa/m, ‖A_j‖ =
+            // sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² − mean²·m) clamped at 0 (the reference
+            // stores NaN when cancellation makes it negative)
+            const double sy = sxy[2 * qq + 1];
+            const double mean = sx / (double)m;
+            b.alpha[lo + k] = (float)mean;
+            b.norm[lo + k] = (float)sqrt(sy);
+            b.normp[lo + k] = (float)sqrt(fmax(sy - mean * mean * (double)m, 0.0));
+          }
         } else {
           const float tot = tots[qq];
           if (!amm) {
@@ -643,14 +638,24 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
       }
     }
     if (more) publish(grp + 1, dn);
-    // partials of grp+1 published; every consumer is done with stage s
+    // partials of grp+1 published; every thread is done with stage s: thread 0 refills it
     if (named_barrier_or(1, T, !ok)) ok = false;
-    if (t == 0) mbar_arrive_local(&empty[s]);
+    if (t == 0 && ok && grp + NS < ngroups) issue(grp + NS, wl_idx);
   }
 
   if (!ok) {
     if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
     return;
+  }
+  if (sampled) {
+    // The picks are consumed: their histogram entries and chunk totals are cleared for the
+    // next draw into this buffer (several CTAs may zero one chunk total: the same value).
+    const int cs = b.chunk_shift;
+    for (int k = t; k < nb; k += T) {
+      const uint32_t col = wl_idx[k];
+      b.count[pb][col] = 0u;
+      b.chunk[pb][col >> cs] = 0u;
+    }
   }
   float* part = b.partials + (size_t)q * m;
 #pragma unroll
@@ -667,6 +672,205 @@ __global__ void __launch_bounds__(kMaxThreads + 32, 1)
   if (t == 0) {
     b.spart[q] = sacc;
     b.spart64[q] = a2acc;
+  }
+
+  // ======================= the step's epilogue, fused (grid-wide) =======================
+  // Every CTA is resident (one per SM), so after a grid barrier the nsm partials are summed
+  // where they sit in L2: CTA q owns float4 row groups [g0, g1) and sums them over the CTAs in
+  // a fixed order (FP64); then the new y rows, and the Rayleigh quotient by the last CTA to
+  // finish (dotProduct_and_generate_x, common.h:103-153).
+  const int RG = m >> 2;
+  const int g0 = (int)((int64_t)q * RG / G), g1 = (int)((int64_t)(q + 1) * RG / G);
+  const float* yprev = b.y[(a.iter + 1) & 1];
+  float* ynew = b.y[a.iter & 1];
+  // the epilogue's own inputs for the first row chunk, fetched before the barrier
+  float4 pre_yp = make_float4(0.f, 0.f, 0.f, 0.f), pre_ym = pre_yp, pre_v = pre_yp;
+  double pre_vs[4] = {0.0, 0.0, 0.0, 0.0};
+  if (!SETUP && warp == 0 && g0 + lane < g1) {
+    const int row = 4 * (g0 + lane);
+    pre_yp = __ldcg(reinterpret_cast<const float4*>(yprev + row));
+    pre_ym = __ldcg(reinterpret_cast<const float4*>(b.y_memo + row));
+    pre_v = __ldcg(reinterpret_cast<const float4*>(b.v + row));
+    if (b.has_vstar)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) pre_vs[e] = __ldcg(b.vstar + row + e);
+  }
+  // z·dx (dots, common.h:55-87) is needed only here: each CTA sums it over its own rows into
+  // rpart[4q+3]; after the barrier the CTA partials are summed in a fixed order
+  if (centred && warp == 0) {
+    for (int c0 = g0; c0 < g1; c0 += 32) {
+      const int gi = c0 + lane;
+      if (gi < g1) {
+        const int row = 4 * gi;
+        const float4 yp =
+            c0 == g0 ? pre_yp : __ldcg(reinterpret_cast<const float4*>(yprev + row));
+        const float4 xm = __ldcg(reinterpret_cast<const float4*>(b.x_memo + row));
+        const float4 z4 = __ldcg(reinterpret_cast<const float4*>(b.z + row));
+        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.x), xm.x), (double)z4.x, zdx);
+        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.y), xm.y), (double)z4.y, zdx);
+        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.z), xm.z), (double)z4.z, zdx);
+        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.w), xm.w), (double)z4.w, zdx);
+      }
+    }
+    zdx = warp_sum(zdx);
+    if (lane == 0) b.rpart[4 * q + 3] = zdx;
+  }
+  named_barrier_or(1, T, false);  // this CTA's partials are written
+  bool bar_ok = true;
+  if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
+  if (named_barrier_or(1, T, !bar_ok)) {
+    if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
+    return;
+  }
+  double4* red = reinterpret_cast<double4*>(stages);  // [warps][32]; the stages are drained
+  double S = 0.0;  // Σ over the CTAs of the per-CTA scalar (fixed order, the same everywhere)
+  double xy = 0.0, yy = 0.0, yv = 0.0;
+  constexpr int kU = 10;
+  for (int c0 = g0; c0 < g1; c0 += 32) {
+    const int gi = c0 + lane;
+    const bool first = (c0 == g0);
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (gi < g1) {
+      const float* P = b.partials + 4 * (size_t)gi;
+      for (int k0 = warp; k0 < G; k0 += ncw * kU) {
+        float4 v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int k = k0 + u * ncw;
+          v[u] = k < G ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * m))
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (first && k0 == warp && warp == 0 && (SETUP || centred)) {
+          zdx = 0.0;
+          for (int k = lane; k < G; k += 32) {
+            S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
+            if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          acc.x += v[u].x;
+          acc.y += v[u].y;
+          acc.z += v[u].z;
+          acc.w += v[u].w;
+        }
+      }
+    } else if (first && warp == 0 && (SETUP || centred)) {
+      zdx = 0.0;
+      for (int k = lane; k < G; k += 32) {
+        S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
+        if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
+      }
+    }
+    if (first && warp == 0) {
+      S = warp_sum(S);
+      zdx = warp_sum(zdx);
+    }
+    red[warp * 32 + lane] = acc;
+    named_barrier_or(1, T, false);
+    if (warp == 0 && gi < g1) {
+      double4 tot = red[lane];
+      for (int w = 1; w < ncw; ++w) {
+        const double4 r4 = red[w * 32 + lane];
+        tot.x += r4.x;
+        tot.y += r4.y;
+        tot.z += r4.z;
+        tot.w += r4.w;
+      }
+      const int row = 4 * gi;
+      const double tv[4] = {tot.x, tot.y, tot.z, tot.w};
+      if constexpr (SETUP) {
+        // z = A·α and v = z − ‖α‖² (generate_v, core_proposedAMM.cuh:4-15)
+        float zf[4], vf[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          zf[e] = (float)tv[e];
+          vf[e] = (float)((double)zf[e] - S);
+        }
+        *reinterpret_cast<float4*>(b.z + row) = make_float4(zf[0], zf[1], zf[2], zf[3]);
+        *reinterpret_cast<float4*>(b.v + row) = make_float4(vf[0], vf[1], vf[2], vf[3]);
+      } else {
+        const float4 yp = first ? pre_yp : *reinterpret_cast<const float4*>(yprev + row);
+        const float xa[4] = {__fmul_rn(scale, yp.x), __fmul_rn(scale, yp.y),
+                             __fmul_rn(scale, yp.z), __fmul_rn(scale, yp.w)};
+        float yo[4];
+        if (!amm) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) yo[e] = (float)tv[e];
+        } else {
+          const float4 ym = first ? pre_ym : *reinterpret_cast<const float4*>(b.y_memo + row);
+          const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
+          if (!centred) {  // previous: y_memo + A_S·tmp (core_previousAMM.cuh:225-232)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) yo[e] = (float)((double)ymv[e] + tv[e]);
+          } else {
+            // y_memo + Σdx·v + z·dx in FP64, rounded (core_proposedAMM.cuh:198-212)
+            const float4 vv = first ? pre_v : *reinterpret_cast<const float4*>(b.v + row);
+            const float va[4] = {vv.x, vv.y, vv.z, vv.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float base = (float)(fma(sum_dx, (double)va[e], zdx) + (double)ymv[e]);
+              yo[e] = (float)((double)base + (tv[e] - S));
+            }
+          }
+        }
+        *reinterpret_cast<float4*>(ynew + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
+        if (mode == kExactMemo) {
+          *reinterpret_cast<float4*>(b.x_memo + row) = make_float4(xa[0], xa[1], xa[2], xa[3]);
+          *reinterpret_cast<float4*>(b.y_memo + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double yd = (double)yo[e];
+          xy = fma(yd, (double)xa[e], xy);
+          yy = fma(yd, yd, yy);
+          if (b.has_vstar) yv = fma(yd, first ? pre_vs[e] : b.vstar[row + e], yv);
+        }
+      }
+    }
+    named_barrier_or(1, T, false);  // red is reused by the next row chunk
+  }
+  if constexpr (SETUP) {
+    if (q == 0 && warp == 0) {
+      if (g0 >= g1) {  // no rows here (m/4 < number of CTAs): ‖α‖² is summed separately
+        for (int k = lane; k < G; k += 32) S += __ldcg(b.spart64 + k);
+        S = warp_sum(S);
+      }
+      if (lane == 0) *b.alpha2 = S;
+    }
+    return;
+  } else {
+    if (warp != 0) return;
+    xy = warp_sum(xy);
+    yy = warp_sum(yy);
+    yv = warp_sum(yv);
+    uint32_t last = 0;
+    if (lane == 0) {
+      b.rpart[4 * q + 0] = xy;
+      b.rpart[4 * q + 1] = yy;
+      b.rpart[4 * q + 2] = yv;
+      __threadfence();
+      last = (atomicAdd(b.ticket, 1u) == (uint32_t)(G - 1)) ? 1u : 0u;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    // the last CTA: Rayleigh quotient and the next step.  Warp 0 sums the CTA partials
+    // lane-strided and then by an xor butterfly: a fixed association order.
+    xy = 0.0;
+    yy = 0.0;
+    yv = 0.0;
+    for (int k = lane; k < G; k += 32) {
+      xy += __ldcg(b.rpart + 4 * k + 0);
+      yy += __ldcg(b.rpart + 4 * k + 1);
+      yv += __ldcg(b.rpart + 4 * k + 2);
+    }
+    xy = warp_sum(xy);
+    yy = warp_sum(yy);
+    yv = warp_sum(yv);
+    if (lane != 0) return;
+    b.ticket[0] = 0u;
+    finish_step(b, a.cc, a.iter, st_s, xy, yy, yv);
   }
 }
 
@@ -767,7 +971,7 @@ static cudaError_t launch_panel(const PanelArgs& a, bool setup, cudaStream_t s) 
   int smem = 0;
   cudaError_t e = configure(a.g, setup, &fn, &smem);
   if (e != cudaSuccess) return e;
-  fn<<<a.g.nclusters, a.g.threads + 32, smem, s>>>(a);
+  fn<<<a.g.nclusters, a.g.threads, smem, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }
