@@ -381,8 +381,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     return;
   }
   if (amm) {
-    // coefficient data of the slice; published by the CTA barrier ahead of the first group
-    for (int k = t; k < nb; k += T) {
+    // coefficient data of the slice, loaded by the warps after warp 0 (whose thread 0 issues
+    // the copies); published by the CTA barrier ahead of the first group
+    const int t1 = T > 32 ? t - 32 : t, T1 = T > 32 ? T - 32 : T;
+    for (int k = t1; k >= 0 && k < nb; k += T1) {
       if (sampled) {
         wl_idx[k] = __ldg(b.wl_col[pb] + lo + k);
         wl_w[k] = __ldg(b.wl_wm[pb] + lo + k);
@@ -652,7 +654,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     // next draw into this buffer (several CTAs may zero one chunk total: the same value).
     const int cs = b.chunk_shift;
     for (int k = t; k < nb; k += T) {
-      const uint32_t col = wl_idx[k];
+      const uint32_t col = wl_idx[k];  // written before the barriers of the group loop
       b.count[pb][col] = 0u;
       b.chunk[pb][col >> cs] = 0u;
     }
