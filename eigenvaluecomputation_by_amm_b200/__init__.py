@@ -6,6 +6,13 @@ fails loudly (ImportError) when it has not been built
 (``python -m eigenvaluecomputation_by_amm_b200.build``); there is no CPU fallback.
 """
 from ._lib import AmmError  # noqa: F401
-from .api import AMMContext, column_major  # noqa: F401
+from .api import AMMContext, BatchSolver, column_major  # noqa: F401
 
-__all__ = ["AMMContext", "column_major", "AmmError"]
+
+def lambda_max(A, max_iter: int = 1000, tol: float = 1e-10, nvec: int = 8):
+    """λ_max(A·Aᵀ) per matrix with a libamm backward (see ``autograd.lambda_max``)."""
+    from .autograd import lambda_max as _lm
+    return _lm(A, max_iter=max_iter, tol=tol, nvec=nvec)
+
+
+__all__ = ["AMMContext", "BatchSolver", "column_major", "lambda_max", "AmmError"]

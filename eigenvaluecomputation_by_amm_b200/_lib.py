@@ -42,6 +42,22 @@ class amm_config(C.Structure):
     ]
 
 
+class amm_batch_matrix(C.Structure):
+    _fields_ = [("A", C.c_void_p), ("ld", C.c_int64), ("m", C.c_int64), ("n", C.c_int64)]
+
+
+class amm_batch_config(C.Structure):
+    _fields_ = [
+        ("nvec", C.c_int32),
+        ("rr_period", C.c_int32),
+        ("max_iter", C.c_int64),
+        ("tol", C.c_double),
+        ("seed", C.c_uint64),
+        ("use_graph", C.c_int32),
+        ("tile_gc", C.c_int32),
+    ]
+
+
 class AmmError(RuntimeError):
     def __init__(self, status: int, where: str):
         self.status = status
@@ -84,6 +100,15 @@ _SIGS = {
     "amm_get_sampling_tables": [_P, C.c_int, _P, _P, _P],
     "amm_sample_indices": [_P, C.c_int, _P, _P],
     "amm_pick_sorted_noalloc": [_P, _P, _I64, _P, C.c_int, _I64, _P, _P, _P],
+    "amm_batch_config_default": [C.POINTER(amm_batch_config)],
+    "amm_batch_create": [C.POINTER(_P), C.POINTER(amm_batch_matrix), _I64,
+                         C.POINTER(amm_batch_config), C.c_int],
+    "amm_batch_destroy": [_P],
+    "amm_batch_vector_offsets": [_P, _P],
+    "amm_batch_run": [_P, _P, _P, _P, _P],
+    "amm_batch_run_each": [_P, _P, _P, _P, _P],
+    "amm_batch_grad": [_P, _P, _P, _P, _P, _P],
+    "amm_batch_tile_choice": [_P, _P, _P],
     "amm_benchmark_product": [_P, C.c_int, C.c_int, _P, _P, _P],
     "amm_grad_lambda": [_P, _P, _P, _I64, _P],
     "amm_get_geometry": [_P, _P],
@@ -93,6 +118,7 @@ _SIGS = {
 }
 _RET = {
     "amm_config_default": None,
+    "amm_batch_config_default": None,
     "amm_status_string": C.c_char_p,
     "amm_last_cuda_error": C.c_char_p,
     "amm_kernel_launch_count": C.c_int64,

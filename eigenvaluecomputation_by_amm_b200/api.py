@@ -15,7 +15,7 @@ import torch
 from . import _lib
 from ._lib import AmmError, amm_config, check
 
-__all__ = ["AMMContext", "column_major", "AmmError"]
+__all__ = ["AMMContext", "BatchSolver", "column_major", "AmmError"]
 
 
 def column_major(A: torch.Tensor) -> torch.Tensor:
@@ -271,3 +271,81 @@ class AMMContext:
         check(self.lib.amm_grad_lambda(self._ctx, _ptr(v), _ptr(g), self.m, _stream(stream)),
               "amm_grad_lambda")
         return g
+
+
+class BatchSolver:
+    """λ_max of A_b·A_bᵀ for many FP32 matrices in one persistent launch (amm_batch_*).
+
+    ``mats`` is a list of column-major FP32 CUDA tensors (shape (m_b, n_b), stride(0) == 1,
+    stride(1) % 4 == 0, m_b <= 2048).  ``nvec`` vectors per matrix (1, 4 or 8) with
+    Rayleigh–Ritz every ``rr_period`` products; iteration stops when λ_max changes by at most
+    ``tol`` relatively or after ``max_iter`` products.  The tensors are borrowed: keep them alive.
+    """
+
+    def __init__(self, mats, nvec: int = 8, max_iter: int = 500, tol: float = 1e-7,
+                 rr_period: int = 1, seed: int = 1234, use_graph: bool = True, tile_gc: int = 0,
+                 device: Optional[int] = None):
+        self.lib = _lib.load()
+        self.mats = list(mats)
+        self.count = len(self.mats)
+        self.nvec = int(nvec)
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self._dev = torch.device("cuda", self.device)
+        descs = (_lib.amm_batch_matrix * self.count)()
+        for i, A in enumerate(self.mats):
+            if A.dtype != torch.float32 or A.dim() != 2 or A.stride(0) != 1:
+                raise ValueError("batch matrices must be column-major FP32 CUDA tensors")
+            descs[i].A = A.data_ptr()
+            descs[i].ld = A.stride(1) if A.shape[1] > 1 else max(A.shape[0], 4)
+            descs[i].m, descs[i].n = A.shape
+        cfg = _lib.amm_batch_config()
+        self.lib.amm_batch_config_default(C.byref(cfg))
+        cfg.nvec, cfg.max_iter, cfg.tol = int(nvec), int(max_iter), float(tol)
+        cfg.rr_period, cfg.seed = int(rr_period), int(seed)
+        cfg.use_graph, cfg.tile_gc = (1 if use_graph else 0), int(tile_gc)
+        self._b = C.c_void_p()
+        check(self.lib.amm_batch_create(C.byref(self._b), descs, self.count, C.byref(cfg),
+                                        self.device), "amm_batch_create")
+        offs = np.zeros(self.count + 1, np.int64)
+        check(self.lib.amm_batch_vector_offsets(self._b, offs.ctypes.data_as(C.c_void_p)),
+              "amm_batch_vector_offsets")
+        self.offsets = offs
+        self.lam = torch.empty(self.count, self.nvec, dtype=torch.float64, device=self._dev)
+        self.vectors = torch.empty(int(offs[-1]), dtype=torch.float32, device=self._dev)
+        self.iters = torch.empty(self.count, dtype=torch.int32, device=self._dev)
+
+    def run(self, each: bool = False, stream=None):
+        """One persistent launch (or one launch per matrix with ``each``); asynchronous."""
+        fn = self.lib.amm_batch_run_each if each else self.lib.amm_batch_run
+        check(fn(self._b, _ptr(self.lam), _ptr(self.vectors), _ptr(self.iters), _stream(stream)),
+              "amm_batch_run_each" if each else "amm_batch_run")
+        return self.lam[:, 0], self.vectors, self.iters
+
+    def vector(self, i: int) -> torch.Tensor:
+        return self.vectors[int(self.offsets[i]):int(self.offsets[i + 1])]
+
+    def grad(self, grads, scale: Optional[torch.Tensor] = None, stream=None):
+        """grads[b] <- scale_b · 2·v_b(v_bᵀA_b) (column-major tensors shaped like A_b)."""
+        ptrs = (C.c_void_p * self.count)(*[g.data_ptr() for g in grads])
+        lds = np.array([g.stride(1) if g.shape[1] > 1 else max(g.shape[0], 1) for g in grads],
+                       np.int64)
+        sc = None if scale is None else scale.to(device=self._dev, dtype=torch.float32).contiguous()
+        check(self.lib.amm_batch_grad(self._b, _ptr(self.vectors), ptrs,
+                                      lds.ctypes.data_as(C.c_void_p), _ptr(sc), _stream(stream)),
+              "amm_batch_grad")
+
+    def tile_choice(self):
+        k, gc = C.c_int32(0), C.c_int32(0)
+        check(self.lib.amm_batch_tile_choice(self._b, C.byref(k), C.byref(gc)), "amm_batch_tile_choice")
+        return int(k.value), int(gc.value)
+
+    def close(self):
+        if self._b:
+            self.lib.amm_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

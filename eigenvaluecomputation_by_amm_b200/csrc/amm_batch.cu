@@ -1,0 +1,885 @@
+// Batched power method: λ_max of C_b = A_b·A_bᵀ for many independent FP32 matrices of uneven
+// sizes in ONE persistent launch (block power iteration with K vectors and Rayleigh–Ritz), and
+// the batched backward ∂λ/∂A = 2·v(vᵀA).
+//
+// The reference handles one matrix per run (AMM.cu:74-95); this path batches the exact product
+// of powerMethod_by_exact.cuh:37-53 with the Rayleigh step of dotProduct_and_generate_x
+// (common.h:103-153) generalised to a block of K orthonormal vectors.
+//
+// Work split: one CTA (512 threads) per matrix at a time, matrices taken largest-first from an
+// atomic queue.  A matrix of m rows is held by "teams" of P threads (P = smallest power of two
+// >= m/4, at least 32), each thread owning 4 consecutive rows of the K vectors X and of the
+// product Y in registers; the 512/P teams split the columns.  Per group of GC columns a team
+// loads the columns once (coalesced 16-byte loads), forms the K·GC partial dots A_jᵀX over its
+// rows, reduces them across the team (warp butterfly, then shared memory for teams wider than a
+// warp) and accumulates Y += A_j·(A_jᵀX): the fused single-pass product of the main kernel.
+// After the pass the team partials of Y are summed in a fixed order, the Gram matrices
+// G = YᵀY and H = XᵀY are reduced in FP64, X <- Y·R⁻¹ (Cholesky QR), and every rr_period
+// iterations (and at the end) H is diagonalised by a warp-parallel cyclic Jacobi in FP64: its
+// largest eigenvalue is λ_max, its eigenvector q gives v = X·q.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "amm.h"
+#include "amm_device.cuh"
+#include "amm_internal.h"
+
+namespace amm {
+namespace batch {
+
+constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxRows = 4 * kThreads;  // 2048
+constexpr int kMaxK = 8;
+constexpr int kJacobiSweeps = 16;
+
+struct Mat {
+  const float* A;  // column-major, ld % 4 == 0, 16-byte aligned
+  int64_t ld;
+  int32_t m, n;
+  int64_t out_off;  // first row of this matrix's vector in the output
+};
+
+struct Args {
+  const Mat* mats;
+  const int32_t* order;  // processing order (largest first)
+  int32_t count;
+  int32_t max_iter;
+  double tol;
+  int32_t rr_period;
+  int32_t pad;
+  uint64_t seed;
+  uint32_t* queue;  // [0]: next work item; zero before the launch
+  double* lam;      // count x K Ritz values, descending ([0] = λ_max)
+  float* vec;       // Σ m: v of each matrix (top Ritz vector, unit)
+  int32_t* iters;   // iterations run (-1: rank-deficient block, no result)
+};
+
+// A shared-memory float4 load the compiler keeps in place (X is re-read per column group
+// instead of being held in registers across the pass).
+__device__ __forceinline__ float4 lds_f4(const float* p) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"((uint32_t)__cvta_generic_to_shared(p)));
+  return v;
+}
+
+// Start block: a counter-based hash of (seed, matrix, row, vector) -> uniform [-1, 1).
+__device__ __forceinline__ float start_value(uint64_t seed, int mi, int row, int v) {
+  uint64_t z = seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(mi + 1)) ^
+               ((uint64_t)row << 20) ^ ((uint64_t)v << 52);
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (float)(int32_t)(uint32_t)(z >> 32) * (1.0f / 2147483648.0f);
+}
+
+// Pair (p, q), p < q, of slot s in round r of a round-robin over K (even) indices.
+__device__ __forceinline__ void rr_pair(int K, int r, int s, int* p, int* q) {
+  int a, b;
+  if (s == 0) {
+    a = K - 1;
+    b = r;
+  } else {
+    a = (r + s) % (K - 1);
+    b = (r - s + (K - 1)) % (K - 1);
+  }
+  *p = a < b ? a : b;
+  *q = a < b ? b : a;
+}
+
+// Cyclic Jacobi on the symmetric K x K matrix H (FP64, shared memory) by one warp; V receives
+// the eigenvectors (columns), H the eigenvalues on its diagonal.  Rotations of one round act on
+// disjoint index pairs, so a round is applied in parallel: lane = pair slot * K + index.
+template <int K>
+__device__ void jacobi_warp(double* H, double* V, double* cs, int lane) {
+  for (int i = lane; i < K * K; i += 32) V[i] = (i / K == i % K) ? 1.0 : 0.0;
+  __syncwarp();
+  if constexpr (K == 1) return;
+  for (int sweep = 0; sweep < kJacobiSweeps; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int i = lane; i < K * K; i += 32) {
+      const double h = H[i];
+      if (i / K == i % K)
+        dia += h * h;
+      else
+        off += h * h;
+    }
+    off = warp_sum(off);
+    dia = warp_sum(dia);
+    if (!(off > 1e-30 * dia)) break;  // also stops on NaN
+    for (int r = 0; r < K - 1; ++r) {
+      if (lane < K / 2) {
+        int p, q;
+        rr_pair(K, r, lane, &p, &q);
+        const double hpq = H[p * K + q];
+        double c = 1.0, s = 0.0;
+        if (hpq != 0.0) {
+          const double tau = (H[q * K + q] - H[p * K + p]) / (2.0 * hpq);
+          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          c = 1.0 / sqrt(1.0 + tt * tt);
+          s = tt * c;
+        }
+        cs[2 * lane] = c;
+        cs[2 * lane + 1] = s;
+      }
+      __syncwarp();
+      const int slot = lane / K, i = lane % K;
+      int p = 0, q = 0;
+      double c = 1.0, s = 0.0;
+      const bool act = slot < K / 2;
+      if (act) {
+        rr_pair(K, r, slot, &p, &q);
+        c = cs[2 * slot];
+        s = cs[2 * slot + 1];
+      }
+      // columns p, q of H and V: H <- H·J, V <- V·J
+      double hip = 0, hiq = 0, vip = 0, viq = 0;
+      if (act) {
+        hip = H[i * K + p];
+        hiq = H[i * K + q];
+        vip = V[i * K + p];
+        viq = V[i * K + q];
+      }
+      __syncwarp();
+      if (act) {
+        H[i * K + p] = c * hip - s * hiq;
+        H[i * K + q] = s * hip + c * hiq;
+        V[i * K + p] = c * vip - s * viq;
+        V[i * K + q] = s * vip + c * viq;
+      }
+      __syncwarp();
+      // rows p, q: H <- Jᵀ·H
+      double hpi = 0, hqi = 0;
+      if (act) {
+        hpi = H[p * K + i];
+        hqi = H[q * K + i];
+      }
+      __syncwarp();
+      if (act) {
+        H[p * K + i] = c * hpi - s * hqi;
+        H[q * K + i] = s * hpi + c * hqi;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+constexpr int align16(int x) { return (x + 15) & ~15; }
+
+template <int K>
+struct Smem {
+  // byte offsets into dynamic shared memory, each 16-byte aligned
+  static constexpr int yred = 0;                                         // float [4*kThreads][K]
+  static constexpr int part = align16(yred + 4 * kThreads * K * 4);      // float [2][kWarps][32]
+  static constexpr int gpart = align16(part + 2 * kWarps * 32 * 4);      // double [kWarps][2*K*K]
+  static constexpr int gram = align16(gpart + kWarps * 2 * K * K * 8);   // double G[K*K], H[K*K]
+  static constexpr int vmat = align16(gram + 2 * K * K * 8);             // double V[K*K]
+  static constexpr int rinv = align16(vmat + K * K * 8);                 // float Rinv[K*K]
+  static constexpr int qv = align16(rinv + K * K * 4);                   // float q[K]
+  static constexpr int cs = align16(qv + K * 4);                         // double cs[kMaxK]
+  static constexpr int ctl = align16(cs + kMaxK * 8);                    // int [4]
+  static constexpr int xs = align16(ctl + 16);                           // float X[K][kMaxRows]
+  static constexpr int total = align16(xs + K * kMaxRows * 4);
+  static_assert(gpart % 8 == 0 && cs % 8 == 0 && xs % 16 == 0, "shared-memory alignment");
+};
+
+// Sum of the NV values d over the team (P threads).  Returns, in every lane, the total of value
+// lane / (32 / NV); the caller gathers value i from lane i·(32 / NV).  Fixed reduction order
+// (deterministic).
+template <int NV>
+__device__ __forceinline__ float team_allreduce(float (&d)[NV], float* part, int buf, int warp,
+                                                int lane, int P, int team, int team_warp0) {
+  float r = warp_reduce_multi<float, NV>(d, lane);
+  if (P > 32) {
+    float* pb = part + buf * kWarps * 32;
+    pb[warp * 32 + lane] = r;
+    named_barrier_or(1 + team, P, false);
+    float s = 0.f;
+    for (int w = 0; w < P / 32; ++w) s += pb[(team_warp0 + w) * 32 + lane];
+    r = s;
+  }
+  return r;
+}
+
+template <int K, int GC>
+__global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ Args a) {
+  constexpr int NV = K * GC;
+  static_assert(NV <= 32 && (32 % NV) == 0, "K*GC must divide 32");
+  using SL = Smem<K>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* yred = reinterpret_cast<float*>(smem + SL::yred);
+  float* part = reinterpret_cast<float*>(smem + SL::part);
+  double* gpart = reinterpret_cast<double*>(smem + SL::gpart);
+  double* Gm = reinterpret_cast<double*>(smem + SL::gram);
+  double* Hm = Gm + K * K;
+  double* Vm = reinterpret_cast<double*>(smem + SL::vmat);
+  float* Rinv = reinterpret_cast<float*>(smem + SL::rinv);
+  float* qv = reinterpret_cast<float*>(smem + SL::qv);
+  double* cs = reinterpret_cast<double*>(smem + SL::cs);
+  int* ctl = reinterpret_cast<int*>(smem + SL::ctl);
+  float* Xs = reinterpret_cast<float*>(smem + SL::xs);  // X, one copy for all teams: [v][row]
+
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  for (;;) {
+    if (t == 0) ctl[0] = (int)atomicAdd(a.queue, 1u);
+    __syncthreads();
+    const int item = ctl[0];
+    __syncthreads();
+    if (item >= a.count) return;
+    const int mi = a.order[item];
+    const Mat M = a.mats[mi];
+    const int m = M.m, n = M.n;
+    int P = 32;
+    while (P < kThreads && 4 * P < m) P <<= 1;
+    const int NT = kThreads / P;
+    const int team = t / P, tl = t % P;
+    const int team_warp0 = team * (P / 32);
+    const int r0 = 4 * tl;
+
+    // ---- start block X0 (hash), orthonormalised below like every later Y ----
+    float Y[4][K];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+#pragma unroll
+      for (int v = 0; v < K; ++v)
+        Y[e][v] = (r0 + e < m) ? start_value(a.seed, mi, r0 + e, v) : 0.f;
+    if (team == 0)
+#pragma unroll
+      for (int v = 0; v < K; ++v)
+        *reinterpret_cast<float4*>(Xs + v * kMaxRows + r0) = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+
+    double lam_prev = 0.0;
+    int it = 0, state = 0;  // state: 0 running, 1 converged / last, 2 degenerate
+    for (;; ++it) {
+      // ---- Gram matrices of the block: G = YᵀY, H = sym(XᵀY) (FP64, team 0 contributes) ----
+      {
+        constexpr int NP = K * (K + 1) / 2;
+        const bool contrib = (team == 0);
+        int pidx = 0;
+        for (int a0 = 0; a0 < K; ++a0)
+          for (int b0 = a0; b0 < K; ++b0, ++pidx) {
+            double g = 0.0, h = 0.0;
+            if (contrib) {
+              const float4 xa = *reinterpret_cast<const float4*>(Xs + a0 * kMaxRows + r0);
+              const float4 xb = *reinterpret_cast<const float4*>(Xs + b0 * kMaxRows + r0);
+              const float xav[4] = {xa.x, xa.y, xa.z, xa.w}, xbv[4] = {xb.x, xb.y, xb.z, xb.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                g = fma((double)Y[e][a0], (double)Y[e][b0], g);
+                h = fma(0.5 * (double)xav[e], (double)Y[e][b0], h);
+                h = fma(0.5 * (double)xbv[e], (double)Y[e][a0], h);
+              }
+            }
+            g = warp_sum(g);
+            h = warp_sum(h);
+            if (lane == 0) {
+              gpart[warp * 2 * NP + pidx] = g;
+              gpart[warp * 2 * NP + NP + pidx] = h;
+            }
+          }
+        __syncthreads();
+        if (t < 2 * NP) {
+          double s = 0.0;
+          for (int w = 0; w < kWarps; ++w) s += gpart[w * 2 * NP + t];
+          const int which = t / NP, pi = t % NP;
+          int a1 = 0, rem = pi;
+          while (rem >= K - a1) {
+            rem -= K - a1;
+            ++a1;
+          }
+          const int b1 = a1 + rem;
+          double* D = which ? Hm : Gm;
+          D[a1 * K + b1] = s;
+          D[b1 * K + a1] = s;
+        }
+        __syncthreads();
+      }
+      // ---- warp 0: Rayleigh–Ritz (every rr_period steps and at the end), Cholesky of G ----
+      if (warp == 0) {
+        const bool first = (it == 0);
+        if (!first) {
+          const bool check = (K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter);
+          if (check) {
+            jacobi_warp<K>(Hm, Vm, cs, lane);
+            if (lane == 0) {
+              int best = 0;
+              for (int i = 1; i < K; ++i)
+                if (Hm[i * K + i] > Hm[best * K + best]) best = i;
+              const double lam = Hm[best * K + best];
+              for (int i = 0; i < K; ++i) qv[i] = (float)Vm[i * K + best];
+              int st = 0;
+              if (!(fabs(lam - lam_prev) > a.tol * fabs(lam)) || it >= a.max_iter) st = 1;
+              if (!isfinite(lam)) st = 2;
+              lam_prev = lam;
+              ctl[1] = st;
+              if (st) {
+                // Ritz values, descending
+                double th[kMaxK];
+                for (int i = 0; i < K; ++i) th[i] = Hm[i * K + i];
+                for (int i = 0; i < K; ++i)
+                  for (int j = i + 1; j < K; ++j)
+                    if (th[j] > th[i]) {
+                      const double tmp = th[i];
+                      th[i] = th[j];
+                      th[j] = tmp;
+                    }
+                for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = th[i];
+                a.iters[mi] = (st == 2) ? -1 : it;
+              }
+            }
+          } else if (lane == 0) {
+            ctl[1] = 0;
+          }
+        } else if (lane == 0) {
+          ctl[1] = 0;
+        }
+        __syncwarp();
+        if (lane == 0 && ctl[1] == 0) {
+          // G = L·Lᵀ; Rinv = L⁻ᵀ (upper triangular), so that X = Y·Rinv has orthonormal columns
+          double L[kMaxK][kMaxK];
+          double tr = 0.0;
+          for (int i = 0; i < K; ++i) tr += Gm[i * K + i];
+          bool ok = tr > 0.0 && isfinite(tr);
+          for (int j = 0; j < K && ok; ++j) {
+            double d = Gm[j * K + j];
+            for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+            if (!(d > 1e-24 * tr)) {
+              ok = false;
+              break;
+            }
+            L[j][j] = sqrt(d);
+            for (int i = j + 1; i < K; ++i) {
+              double s = Gm[i * K + j];
+              for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+              L[i][j] = s / L[j][j];
+            }
+          }
+          if (!ok) {
+            ctl[1] = 2;
+            if (!first) {
+              for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = nan("");
+            }
+            a.iters[mi] = -1;
+          } else {
+            double Li[kMaxK][kMaxK];  // L⁻¹ (lower)
+            for (int j = 0; j < K; ++j) {
+              Li[j][j] = 1.0 / L[j][j];
+              for (int i = j + 1; i < K; ++i) {
+                double s = 0.0;
+                for (int k = j; k < i; ++k) s += L[i][k] * Li[k][j];
+                Li[i][j] = -s / L[i][i];
+              }
+            }
+            for (int i = 0; i < K; ++i)
+              for (int j = 0; j < K; ++j) Rinv[i * K + j] = (j >= i) ? (float)Li[j][i] : 0.f;
+          }
+        }
+      }
+      __syncthreads();
+      state = ctl[1];
+      if (state != 0) {
+        if (state == 1 && team == 0) {  // v = X·q over this thread's rows
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            if (r0 + e < m) {
+              float s = 0.f;
+#pragma unroll
+              for (int v = 0; v < K; ++v) s = fmaf(Xs[v * kMaxRows + r0 + e], qv[v], s);
+              a.vec[M.out_off + r0 + e] = s;
+            }
+          }
+        }
+        break;
+      }
+      // ---- X <- Y·Rinv (team 0 writes the shared copy) ----
+      if (team == 0) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+          float xj[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            float s = 0.f;
+#pragma unroll
+            for (int i = 0; i <= j; ++i) s = fmaf(Y[e][i], Rinv[i * K + j], s);
+            xj[e] = s;
+          }
+          *reinterpret_cast<float4*>(Xs + j * kMaxRows + r0) = make_float4(xj[0], xj[1], xj[2], xj[3]);
+        }
+      }
+      __syncthreads();
+      // ---- Y = C·X: the fused pass over the columns (team-local) ----
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+#pragma unroll
+        for (int v = 0; v < K; ++v) Y[e][v] = 0.f;
+      const bool rows = r0 < m;
+      const float* __restrict__ Ab = M.A + r0;
+      int buf = 0;
+      for (int g0 = team * GC; g0 < n; g0 += NT * GC, buf ^= 1) {
+        float4 av[GC];
+#pragma unroll
+        for (int c = 0; c < GC; ++c) {
+          av[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (rows && g0 + c < n)
+            av[c] = __ldcs(reinterpret_cast<const float4*>(Ab + (int64_t)(g0 + c) * M.ld));
+          if (r0 + 1 >= m) av[c].y = 0.f;  // rows past m (the padding up to ld) count as zero
+          if (r0 + 2 >= m) av[c].z = 0.f;
+          if (r0 + 3 >= m) av[c].w = 0.f;
+        }
+        float d[NV];
+#pragma unroll
+        for (int v = 0; v < K; ++v) {
+          const float4 xv = lds_f4(Xs + v * kMaxRows + r0);
+#pragma unroll
+          for (int c = 0; c < GC; ++c) {
+            float s = av[c].x * xv.x;
+            s = fmaf(av[c].y, xv.y, s);
+            s = fmaf(av[c].z, xv.z, s);
+            s = fmaf(av[c].w, xv.w, s);
+            d[c * K + v] = s;
+          }
+        }
+        const float red = team_allreduce<NV>(d, part, buf, warp, lane, P, team, team_warp0);
+#pragma unroll
+        for (int c = 0; c < GC; ++c)
+#pragma unroll
+          for (int v = 0; v < K; ++v) {
+            const float tc = __shfl_sync(0xffffffffu, red, (c * K + v) * (32 / NV));
+            Y[0][v] = fmaf(av[c].x, tc, Y[0][v]);
+            Y[1][v] = fmaf(av[c].y, tc, Y[1][v]);
+            Y[2][v] = fmaf(av[c].z, tc, Y[2][v]);
+            Y[3][v] = fmaf(av[c].w, tc, Y[3][v]);
+          }
+      }
+      // ---- sum the team partials of Y (fixed order), every team receives the total ----
+      if (NT > 1) {
+        __syncthreads();
+        if (rows) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int v = 0; v < K; ++v) yred[((team * 4 * P) + r0 + e) * K + v] = Y[e][v];
+        }
+        __syncthreads();
+        if (rows) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int v = 0; v < K; ++v) {
+              float s = 0.f;
+              for (int tm = 0; tm < NT; ++tm) s += yred[((tm * 4 * P) + r0 + e) * K + v];
+              Y[e][v] = s;
+            }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- backward: grad_b = 2·v_b·(v_bᵀ·A_b), column-major like A_b, one warp per column ----
+struct GradArgs {
+  const Mat* mats;
+  const int64_t* col_start;  // count + 1 prefix of column counts
+  int32_t count;
+  const float* vec;          // Σ m
+  float* const* grads;       // count pointers
+  const int64_t* grad_ld;    // count
+  const float* scale;        // count (upstream gradient per matrix), or null (1)
+};
+
+__global__ void __launch_bounds__(256) grad_kernel(const __grid_constant__ GradArgs a) {
+  const int64_t total = a.col_start[a.count];
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int64_t gc = gw; gc < total; gc += nw) {
+    int lo = 0, hi = a.count - 1;  // matrix of global column gc
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.col_start[mid] <= gc)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const Mat M = a.mats[lo];
+    const int64_t j = gc - a.col_start[lo];
+    const float* col = M.A + j * M.ld;
+    const float* v = a.vec + M.out_off;
+    float s = 0.f;
+    for (int r = lane; r < M.m; r += 32) s = fmaf(col[r], v[r], s);
+    s = warp_sum(s);
+    const float k = 2.f * s * (a.scale ? a.scale[lo] : 1.f);
+    float* g = a.grads[lo] + j * a.grad_ld[lo];
+    for (int r = lane; r < M.m; r += 32) g[r] = k * v[r];
+  }
+}
+
+using KernelFn = void (*)(Args);
+
+struct Variant {
+  int K, GC;
+  KernelFn fn;
+};
+
+static const Variant kVariants[] = {
+    {1, 8, batch_kernel<1, 8>},   {1, 16, batch_kernel<1, 16>},
+    {4, 2, batch_kernel<4, 2>},   {4, 4, batch_kernel<4, 4>},   {4, 8, batch_kernel<4, 8>},
+    {8, 1, batch_kernel<8, 1>},   {8, 2, batch_kernel<8, 2>},   {8, 4, batch_kernel<8, 4>},
+};
+
+static int smem_bytes(int K) {
+  switch (K) {
+    case 1: return Smem<1>::total;
+    case 4: return Smem<4>::total;
+    default: return Smem<8>::total;
+  }
+}
+
+}  // namespace batch
+}  // namespace amm
+
+// ------------------------------------------------------------------------------------------
+// Host side: the batch context
+// ------------------------------------------------------------------------------------------
+using amm::batch::Mat;
+
+struct amm_batch {
+  int device = 0;
+  int nsm = 0;
+  amm_batch_config cfg{};
+  int64_t count = 0;
+  std::vector<Mat> mats;
+  std::vector<int32_t> order;
+  int64_t vec_len = 0;
+  int64_t total_cols = 0;
+  // device memory (one allocation)
+  void* mem = nullptr;
+  Mat* d_mats = nullptr;
+  int32_t* d_order = nullptr;
+  uint32_t* d_queue = nullptr;
+  int64_t* d_col_start = nullptr;
+  float** d_grads = nullptr;
+  int64_t* d_grad_ld = nullptr;
+  int variant = -1;  // chosen tile shape (index into kVariants)
+  std::map<int, float> tune_ms;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t cap = nullptr;
+  double* g_lam = nullptr;
+  float* g_vec = nullptr;
+  int32_t* g_iters = nullptr;
+};
+
+namespace {
+
+int fail(cudaError_t e, const char* what) { return amm::record_cuda_failure(e, what); }
+
+#define BATCH_CUDA(call)                            \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return fail(e_, #call);  \
+  } while (0)
+
+struct Guard {
+  int old = -1;
+  explicit Guard(int dev) {
+    cudaGetDevice(&old);
+    if (old != dev) cudaSetDevice(dev);
+  }
+  ~Guard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (old >= 0 && cur != old) cudaSetDevice(old);
+  }
+};
+
+int launch(amm_batch* b, int variant, int grid, double* d_lam, float* d_vec, int32_t* d_iters,
+           int max_iter, const int32_t* order, int count, cudaStream_t s) {
+  const auto& V = amm::batch::kVariants[variant];
+  const int sm = amm::batch::smem_bytes(V.K);
+  BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  amm::batch::Args a{};
+  a.mats = b->d_mats;
+  a.order = order;
+  a.count = count;
+  a.max_iter = max_iter;
+  a.tol = b->cfg.tol;
+  a.rr_period = b->cfg.rr_period > 0 ? b->cfg.rr_period : 1;
+  a.seed = b->cfg.seed;
+  a.queue = b->d_queue;
+  a.lam = d_lam;
+  a.vec = d_vec;
+  a.iters = d_iters;
+  BATCH_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(uint32_t), s));
+  V.fn<<<grid, amm::batch::kThreads, sm, s>>>(a);
+  amm::count_launch(1);
+  BATCH_CUDA(cudaGetLastError());
+  return AMM_OK;
+}
+
+// Tile-shape autotuner: every variant with the requested K runs the whole batch for a few
+// iterations; the fastest (CUDA events) is kept for the context.
+int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaStream_t s) {
+  if (b->variant >= 0) return AMM_OK;
+  int best = -1;
+  float best_ms = 0.f;
+  cudaEvent_t e0, e1;
+  BATCH_CUDA(cudaEventCreate(&e0));
+  BATCH_CUDA(cudaEventCreate(&e1));
+  const int grid = (int)std::min<int64_t>(b->count, (int64_t)b->nsm);
+  const int n_var = (int)(sizeof(amm::batch::kVariants) / sizeof(amm::batch::kVariants[0]));
+  for (int v = 0; v < n_var; ++v) {
+    if (amm::batch::kVariants[v].K != b->cfg.nvec) continue;
+    if (b->cfg.tile_gc > 0 && amm::batch::kVariants[v].GC != b->cfg.tile_gc) continue;
+    int rc = launch(b, v, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);  // warm
+    if (rc) return rc;
+    BATCH_CUDA(cudaEventRecord(e0, s));
+    rc = launch(b, v, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);
+    if (rc) return rc;
+    BATCH_CUDA(cudaEventRecord(e1, s));
+    BATCH_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    b->tune_ms[v] = ms;
+    if (best < 0 || ms < best_ms) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best < 0) return AMM_ERR_UNSUPPORTED;
+  b->variant = best;
+  return AMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void amm_batch_config_default(amm_batch_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->nvec = 8;
+  c->max_iter = 500;
+  c->tol = 1e-7;
+  c->rr_period = 1;
+  c->use_graph = 1;
+  c->seed = 1234;
+  c->tile_gc = 0;
+}
+
+int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t count,
+                     const amm_batch_config* cfg, int device) {
+  if (!out || !mats || !cfg || count < 1 || count > (1 << 20)) return AMM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (cfg->nvec != 1 && cfg->nvec != 4 && cfg->nvec != 8) return AMM_ERR_UNSUPPORTED;
+  if (cfg->max_iter < 1 || !(cfg->tol >= 0.0) || cfg->rr_period < 0) return AMM_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AMM_ERR_NO_DEVICE;
+  if (device < 0 || device >= ndev) return AMM_ERR_INVALID_ARGUMENT;
+  std::vector<Mat> ms((size_t)count);
+  int64_t off = 0, cols = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    const amm_batch_matrix& x = mats[i];
+    if (!x.A || x.m < 1 || x.n < 1 || x.ld < x.m) return AMM_ERR_INVALID_ARGUMENT;
+    if (x.m > amm::batch::kMaxRows || x.n > INT32_MAX) return AMM_ERR_UNSUPPORTED;
+    if (x.m < cfg->nvec) return AMM_ERR_UNSUPPORTED;
+    if ((reinterpret_cast<uintptr_t>(x.A) & 15) != 0 || (x.ld % 4) != 0) return AMM_ERR_ALIGNMENT;
+    ms[i].A = static_cast<const float*>(x.A);
+    ms[i].ld = x.ld;
+    ms[i].m = (int32_t)x.m;
+    ms[i].n = (int32_t)x.n;
+    ms[i].out_off = off;
+    off += x.m;
+    cols += x.n;
+  }
+  amm_batch* b = new amm_batch();
+  b->device = device;
+  b->cfg = *cfg;
+  b->count = count;
+  b->mats = ms;
+  b->vec_len = off;
+  b->total_cols = cols;
+  b->order.resize((size_t)count);
+  for (int64_t i = 0; i < count; ++i) b->order[i] = (int32_t)i;
+  // largest first (work m·n), ties by index: the queue then balances like LPT scheduling
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t x, int32_t y) {
+    return (int64_t)ms[x].m * ms[x].n > (int64_t)ms[y].m * ms[y].n;
+  });
+  Guard g(device);
+  cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device);
+  size_t bytes = 0;
+  auto carve = [&](size_t n, size_t align) {
+    bytes = (bytes + align - 1) / align * align;
+    const size_t o = bytes;
+    bytes += n;
+    return o;
+  };
+  const size_t o_mats = carve(sizeof(Mat) * count, 256);
+  const size_t o_order = carve(sizeof(int32_t) * count, 256);
+  const size_t o_queue = carve(sizeof(uint32_t) * 4, 256);
+  const size_t o_cols = carve(sizeof(int64_t) * (count + 1), 256);
+  const size_t o_grads = carve(sizeof(float*) * count, 256);
+  const size_t o_gld = carve(sizeof(int64_t) * count, 256);
+  cudaError_t e = cudaMalloc(&b->mem, bytes);
+  if (e != cudaSuccess) {
+    delete b;
+    return e == cudaErrorMemoryAllocation ? AMM_ERR_OUT_OF_MEMORY : fail(e, "cudaMalloc");
+  }
+  char* base = static_cast<char*>(b->mem);
+  b->d_mats = reinterpret_cast<Mat*>(base + o_mats);
+  b->d_order = reinterpret_cast<int32_t*>(base + o_order);
+  b->d_queue = reinterpret_cast<uint32_t*>(base + o_queue);
+  b->d_col_start = reinterpret_cast<int64_t*>(base + o_cols);
+  b->d_grads = reinterpret_cast<float**>(base + o_grads);
+  b->d_grad_ld = reinterpret_cast<int64_t*>(base + o_gld);
+  std::vector<int64_t> cs((size_t)count + 1, 0);
+  for (int64_t i = 0; i < count; ++i) cs[i + 1] = cs[i] + ms[i].n;
+  e = cudaMemcpy(b->d_mats, ms.data(), sizeof(Mat) * count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_order, b->order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_col_start, cs.data(), sizeof(int64_t) * (count + 1),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(b->mem);
+    delete b;
+    return fail(e, "cudaMemcpy(batch descriptors)");
+  }
+  *out = b;
+  return AMM_OK;
+}
+
+int amm_batch_destroy(amm_batch* b) {
+  if (!b) return AMM_ERR_INVALID_ARGUMENT;
+  Guard g(b->device);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->mem) cudaFree(b->mem);
+  delete b;
+  return AMM_OK;
+}
+
+int amm_batch_vector_offsets(amm_batch* b, int64_t* offsets) {
+  if (!b || !offsets) return AMM_ERR_INVALID_ARGUMENT;
+  for (int64_t i = 0; i < b->count; ++i) offsets[i] = b->mats[i].out_off;
+  offsets[b->count] = b->vec_len;
+  return AMM_OK;
+}
+
+int amm_batch_run(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_iters,
+                  void* stream) {
+  if (!b || !d_lambda || !d_vectors || !d_iters) return AMM_ERR_INVALID_ARGUMENT;
+  Guard g(b->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int rc = autotune(b, d_lambda, d_vectors, d_iters, s);
+  if (rc) return rc;
+  const int grid = (int)std::min<int64_t>(b->count, (int64_t)b->nsm);
+  if (!b->cfg.use_graph)
+    return launch(b, b->variant, grid, d_lambda, d_vectors, d_iters, (int)b->cfg.max_iter,
+                  b->d_order, (int)b->count, s);
+  if (b->gexec && (b->g_lam != d_lambda || b->g_vec != d_vectors || b->g_iters != d_iters)) {
+    cudaGraphExecDestroy(b->gexec);
+    cudaGraphDestroy(b->graph);
+    b->gexec = nullptr;
+    b->graph = nullptr;
+  }
+  if (!b->gexec) {
+    if (!b->cap) BATCH_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    BATCH_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed));
+    const int64_t before = amm::launch_count();
+    rc = launch(b, b->variant, grid, d_lambda, d_vectors, d_iters, (int)b->cfg.max_iter,
+                b->d_order, (int)b->count, b->cap);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(b->cap, &gr);
+    amm::count_launch(-(int)(amm::launch_count() - before));
+    if (rc) {
+      if (gr) cudaGraphDestroy(gr);
+      return rc;
+    }
+    if (ce != cudaSuccess) return fail(ce, "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&b->gexec, gr, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(gr);
+      return fail(ie, "cudaGraphInstantiate");
+    }
+    b->graph = gr;
+    b->g_lam = d_lambda;
+    b->g_vec = d_vectors;
+    b->g_iters = d_iters;
+  }
+  BATCH_CUDA(cudaGraphLaunch(b->gexec, s));
+  amm::count_launch(1);
+  return AMM_OK;
+}
+
+int amm_batch_run_each(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_iters,
+                       void* stream) {
+  if (!b || !d_lambda || !d_vectors || !d_iters) return AMM_ERR_INVALID_ARGUMENT;
+  Guard g(b->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int rc = autotune(b, d_lambda, d_vectors, d_iters, s);
+  if (rc) return rc;
+  // one single-CTA launch per matrix; each reads its matrix index from a one-entry slice of
+  // the order array
+  for (int64_t i = 0; i < b->count; ++i) {
+    rc = launch(b, b->variant, 1, d_lambda, d_vectors, d_iters, (int)b->cfg.max_iter,
+                b->d_order + i, 1, s);
+    if (rc) return rc;
+  }
+  return AMM_OK;
+}
+
+int amm_batch_grad(amm_batch* b, const float* d_vectors, void* const* grad_ptrs,
+                   const int64_t* grad_ld, const float* d_scale, void* stream) {
+  if (!b || !d_vectors || !grad_ptrs || !grad_ld) return AMM_ERR_INVALID_ARGUMENT;
+  for (int64_t i = 0; i < b->count; ++i) {
+    if (!grad_ptrs[i] || grad_ld[i] < b->mats[i].m) return AMM_ERR_INVALID_ARGUMENT;
+  }
+  Guard g(b->device);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  BATCH_CUDA(cudaMemcpyAsync(b->d_grads, grad_ptrs, sizeof(void*) * b->count,
+                             cudaMemcpyHostToDevice, s));
+  BATCH_CUDA(cudaMemcpyAsync(b->d_grad_ld, grad_ld, sizeof(int64_t) * b->count,
+                             cudaMemcpyHostToDevice, s));
+  amm::batch::GradArgs a{};
+  a.mats = b->d_mats;
+  a.col_start = b->d_col_start;
+  a.count = (int32_t)b->count;
+  a.vec = d_vectors;
+  a.grads = b->d_grads;
+  a.grad_ld = b->d_grad_ld;
+  a.scale = d_scale;
+  int64_t warps = b->total_cols;
+  int64_t blocks = (warps * 32 + 255) / 256;
+  if (blocks > (int64_t)b->nsm * 16) blocks = (int64_t)b->nsm * 16;
+  amm::batch::grad_kernel<<<(int)blocks, 256, 0, s>>>(a);
+  amm::count_launch(1);
+  BATCH_CUDA(cudaGetLastError());
+  // the pointer arrays are read by the kernel: keep the host copies alive until it has run
+  BATCH_CUDA(cudaStreamSynchronize(s));
+  return AMM_OK;
+}
+
+int amm_batch_tile_choice(amm_batch* b, int32_t* k_out, int32_t* gc_out) {
+  if (!b || !k_out || !gc_out) return AMM_ERR_INVALID_ARGUMENT;
+  if (b->variant < 0) return AMM_ERR_NOT_READY;
+  *k_out = amm::batch::kVariants[b->variant].K;
+  *gc_out = amm::batch::kVariants[b->variant].GC;
+  return AMM_OK;
+}
+
+}  // extern "C"

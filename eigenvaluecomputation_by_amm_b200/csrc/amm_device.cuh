@@ -322,4 +322,24 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t nblocks) {
   return true;
 }
 
+// Warp reduction of N values at once (multi-value butterfly): lane l ends with the full sum of
+// value l / (32/N); returns it (a fixed tree, deterministic).
+template <typename V, int N>
+__device__ __forceinline__ V warp_reduce_multi(V (&v)[N], int lane) {
+  int off = 16;
+#pragma unroll
+  for (int n = N / 2; n >= 1; n >>= 1, off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+      const V send = upper ? v[i] : v[i + n];
+      const V keep = upper ? v[i + n] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  V r = v[0];
+  for (; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+  return r;
+}
+
 }  // namespace amm

@@ -169,25 +169,6 @@ __device__ __forceinline__ void warp_partials_sum(const V* base, int stride, int
   }
 }
 
-// Warp reduction of N values at once (multi-value butterfly): lane l ends with the full sum of
-// value l / (32/N); returns it (a fixed tree, deterministic).
-template <typename V, int N>
-__device__ __forceinline__ V warp_reduce_multi(V (&v)[N], int lane) {
-  int off = 16;
-#pragma unroll
-  for (int n = N / 2; n >= 1; n >>= 1, off >>= 1) {
-    const bool upper = (lane & off) != 0;
-#pragma unroll
-    for (int i = 0; i < n; ++i) {
-      const V send = upper ? v[i] : v[i + n];
-      const V keep = upper ? v[i + n] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
-    }
-  }
-  V r = v[0];
-  for (; off > 0; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
-  return r;
-}
 
 // Set-up variant of fused_block: the axpy uses coef = α_j; the next group's statistics are
 // per-vector FP32 partial sums of <= 8 values (BF16 squares are exact in FP32) folded into

@@ -196,6 +196,56 @@ int amm_pick_sorted_noalloc(const uint32_t *d_states_in, uint32_t *d_states_out,
                             const void *d_cdf, int cdf_precision, int64_t n,
                             uint32_t *d_idx_sorted, int32_t *d_distinct, void *stream);
 
+/* ---- Batched λ_max for many independent FP32 matrices (no counterpart in the reference,
+ * which solves one matrix per run, AMM.cu:74-95) ----
+ * Block power iteration with nvec orthonormal vectors (1, 4 or 8) and Rayleigh–Ritz, all
+ * matrices in one persistent launch (captured in a CUDA graph when use_graph is set).  Each A_b
+ * is column-major FP32 with m <= 2048, ld % 4 == 0 and 16-byte alignment; rows m..ld-1 are
+ * ignored.  The exact product per step is the one of powerMethod_by_exact.cuh:37-53; the
+ * Rayleigh quotient generalises dotProduct_and_generate_x (common.h:103-153) to a block. */
+typedef struct amm_batch amm_batch;
+
+typedef struct amm_batch_matrix {
+  const void *A;   /* device pointer, borrowed */
+  int64_t ld;
+  int64_t m;
+  int64_t n;
+} amm_batch_matrix;
+
+typedef struct amm_batch_config {
+  int32_t nvec;       /* block size: 1, 4 or 8                                          */
+  int32_t rr_period;  /* Rayleigh–Ritz (and convergence test) every rr_period steps      */
+  int64_t max_iter;   /* products per matrix at most                                     */
+  double tol;         /* stop when |Δλ_max| <= tol·λ_max between two Rayleigh–Ritz steps */
+  uint64_t seed;      /* start block (counter-based hash of seed, matrix, row, vector)    */
+  int32_t use_graph;  /* replay the launch from a CUDA graph                             */
+  int32_t tile_gc;    /* columns per group; 0 lets the autotuner choose                  */
+} amm_batch_config;
+
+void amm_batch_config_default(amm_batch_config *cfg);
+/* Descriptors are copied; the matrices stay owned by the caller and must outlive the context. */
+int amm_batch_create(amm_batch **out, const amm_batch_matrix *mats, int64_t count,
+                     const amm_batch_config *cfg, int device);
+int amm_batch_destroy(amm_batch *b);
+/* offsets[count + 1]: first row of each matrix's vector in the packed vector output. */
+int amm_batch_vector_offsets(amm_batch *b, int64_t *offsets);
+/* One persistent launch over all matrices (largest first from a device queue).  d_lambda:
+ * count x nvec Ritz values, descending (λ_max first); d_vectors: Σ m, the unit top Ritz vector
+ * of each matrix; d_iters: products run per matrix (-1: rank-deficient block).  The first call
+ * autotunes the tile shape (columns per group) on this batch. */
+int amm_batch_run(amm_batch *b, double *d_lambda, float *d_vectors, int32_t *d_iters,
+                  void *stream);
+/* The same computation with one launch per matrix (the comparison arm). */
+int amm_batch_run_each(amm_batch *b, double *d_lambda, float *d_vectors, int32_t *d_iters,
+                       void *stream);
+/* Backward of λ_max: grad_b = scale_b · 2·v_b·(v_bᵀA_b), column-major with leading dimension
+ * grad_ld[b]; grad_ptrs and grad_ld are host arrays of count entries, d_scale a device array of
+ * count factors or NULL.  Synchronises the stream. */
+int amm_batch_grad(amm_batch *b, const float *d_vectors, void *const *grad_ptrs,
+                   const int64_t *grad_ld, const float *d_scale, void *stream);
+/* The tile shape the autotuner picked (AMM_ERR_NOT_READY before the first run). */
+int amm_batch_tile_choice(amm_batch *b, int32_t *nvec, int32_t *cols_per_group);
+
 /* Measurement hook: time `reps` back-to-back launches of the fused product kernel for one
  * step kind (AMM_STEP_EXACT, AMM_STEP_PREVIOUS or AMM_STEP_PROPOSED) on the bound matrix,
  * with CUDA events on `stream`, from the start vector of the last call (ones before any
