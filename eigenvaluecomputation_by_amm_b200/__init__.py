@@ -9,7 +9,7 @@ from ._lib import AmmError  # noqa: F401
 from .api import AMMContext, BatchSolver, column_major  # noqa: F401
 
 
-def lambda_max(A, max_iter: int = 1000, tol: float = 1e-10, nvec: int = 8):
+def lambda_max(A, max_iter: int = 1000, tol: float = 1e-6, nvec: int = 8):
     """λ_max(A·Aᵀ) per matrix with a libamm backward (see ``autograd.lambda_max``)."""
     from .autograd import lambda_max as _lm
     return _lm(A, max_iter=max_iter, tol=tol, nvec=nvec)

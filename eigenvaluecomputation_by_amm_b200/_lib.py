@@ -55,6 +55,8 @@ class amm_batch_config(C.Structure):
         ("seed", C.c_uint64),
         ("use_graph", C.c_int32),
         ("tile_gc", C.c_int32),
+        ("c_divisor", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 

@@ -278,13 +278,15 @@ class BatchSolver:
 
     ``mats`` is a list of column-major FP32 CUDA tensors (shape (m_b, n_b), stride(0) == 1,
     stride(1) % 4 == 0, m_b <= 2048).  ``nvec`` vectors per matrix (1, 4 or 8) with
-    Rayleigh–Ritz every ``rr_period`` products; iteration stops when λ_max changes by at most
-    ``tol`` relatively or after ``max_iter`` products.  The tensors are borrowed: keep them alive.
+    Rayleigh–Ritz every ``rr_period`` products; iteration stops when the residual of the top
+    Ritz pair ‖C·v − λ·v‖ is at most ``tol``·λ, or after ``max_iter`` products.  ``c_divisor`` k > 0 replaces the exact
+    product by the previous-AMM estimate with c = n/k sampled columns per step.  The tensors are
+    borrowed: keep them alive.
     """
 
-    def __init__(self, mats, nvec: int = 8, max_iter: int = 500, tol: float = 1e-7,
+    def __init__(self, mats, nvec: int = 8, max_iter: int = 500, tol: float = 1e-6,
                  rr_period: int = 1, seed: int = 1234, use_graph: bool = True, tile_gc: int = 0,
-                 device: Optional[int] = None):
+                 c_divisor: int = 0, device: Optional[int] = None):
         self.lib = _lib.load()
         self.mats = list(mats)
         self.count = len(self.mats)
@@ -303,6 +305,7 @@ class BatchSolver:
         cfg.nvec, cfg.max_iter, cfg.tol = int(nvec), int(max_iter), float(tol)
         cfg.rr_period, cfg.seed = int(rr_period), int(seed)
         cfg.use_graph, cfg.tile_gc = (1 if use_graph else 0), int(tile_gc)
+        cfg.c_divisor = int(c_divisor)
         self._b = C.c_void_p()
         check(self.lib.amm_batch_create(C.byref(self._b), descs, self.count, C.byref(cfg),
                                         self.device), "amm_batch_create")

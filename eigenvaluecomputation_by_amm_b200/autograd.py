@@ -32,7 +32,7 @@ def _column_major_batch(A: torch.Tensor) -> torch.Tensor:
 
 class LambdaMax(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-10,
+    def forward(ctx, A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-6,
                 nvec: int = 8):
         if not A.is_cuda or A.dtype != torch.float32 or A.dim() != 3:
             raise ValueError("lambda_max expects an FP32 CUDA tensor of shape (B, m, n)")
@@ -63,8 +63,11 @@ class LambdaMax(torch.autograd.Function):
         return gbuf[:, :, :m].transpose(1, 2), None, None, None
 
 
-def lambda_max(A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-10, nvec: int = 8):
-    """λ_max(A_b·A_bᵀ) (FP64, shape (B,) or scalar) with a libamm backward for A."""
+def lambda_max(A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-6, nvec: int = 8):
+    """λ_max(A_b·A_bᵀ) (FP64, shape (B,) or scalar) with a libamm backward for A.
+
+    Iteration stops at ‖C·v − λ·v‖ <= tol·λ (or max_iter products); the eigenvector, and so the
+    gradient, is then accurate to about tol·λ_1/(λ_1 − λ_2)."""
     single = A.dim() == 2
     lam, _ = LambdaMax.apply(A.unsqueeze(0) if single else A, max_iter, tol, nvec)
     return lam[0] if single else lam

@@ -39,11 +39,17 @@ constexpr int kMaxRows = 4 * kThreads;  // 2048
 constexpr int kMaxK = 8;
 constexpr int kJacobiSweeps = 16;
 
+constexpr int kMaxCols = 8192;   // AMM mode: the CDF lives in shared memory
+constexpr int kMaxPicks = 1024;  // AMM mode: c <= n / 8
+
 struct Mat {
   const float* A;  // column-major, ld % 4 == 0, 16-byte aligned
   int64_t ld;
   int32_t m, n;
   int64_t out_off;  // first row of this matrix's vector in the output
+  int64_t st_off;   // AMM mode: first of this matrix's c xorshift states
+  int32_t c;        // AMM mode: samples per product (0: exact)
+  int32_t pad;
 };
 
 struct Args {
@@ -55,6 +61,7 @@ struct Args {
   int32_t rr_period;
   int32_t pad;
   uint64_t seed;
+  uint32_t* states;  // AMM mode: xorshift32 states of every matrix (advanced in place)
   uint32_t* queue;  // [0]: next work item; zero before the launch
   double* lam;      // count x K Ritz values, descending ([0] = λ_max)
   float* vec;       // Σ m: v of each matrix (top Ritz vector, unit)
@@ -186,9 +193,16 @@ struct Smem {
   static constexpr int rinv = align16(vmat + K * K * 8);                 // float Rinv[K*K]
   static constexpr int qv = align16(rinv + K * K * 4);                   // float q[K]
   static constexpr int cs = align16(qv + K * 4);                         // double cs[kMaxK]
-  static constexpr int ctl = align16(cs + kMaxK * 8);                    // int [4]
+  static constexpr int ritz = align16(cs + kMaxK * 8);                   // double θ[K], λ
+  static constexpr int ctl = align16(ritz + (kMaxK + 1) * 8);            // int [4]
   static constexpr int xs = align16(ctl + 16);                           // float X[K][kMaxRows]
-  static constexpr int total = align16(xs + K * kMaxRows * 4);
+  static constexpr int total = align16(xs + K * kMaxRows * 4);      // exact mode ends here
+  static constexpr int cdf = total;                                    // float [kMaxCols]
+  static constexpr int hist = align16(cdf + kMaxCols * 4);             // uint32 [kMaxCols]
+  static constexpr int lcol = align16(hist + kMaxCols * 4);            // int32 [kMaxPicks]
+  static constexpr int lw = align16(lcol + kMaxPicks * 4);             // float [kMaxPicks]
+  static constexpr int scan = align16(lw + kMaxPicks * 4);             // uint32 [40], double[32]
+  static constexpr int total_amm = align16(scan + 40 * 4 + 32 * 8);
   static_assert(gpart % 8 == 0 && cs % 8 == 0 && xs % 16 == 0, "shared-memory alignment");
 };
 
@@ -210,6 +224,113 @@ __device__ __forceinline__ float team_allreduce(float (&d)[NV], float* part, int
   return r;
 }
 
+// Rayleigh–Ritz (every rr_period steps and at the end) and the next basis, by warp 0; kept out
+// of line so that its FP64 scratch does not compete for registers with the product loop.
+// H = XᵀCX is diagonalised (θ, V); λ = max θ, its Ritz vector v = X·q (q and the sorted θ go
+// to shared memory for the residual test the whole CTA runs next).  The next basis is
+// X <- Y·M, M = V·L⁻ᵀ with L·Lᵀ = VᵀGV: Cholesky QR of the block rotated into the Ritz basis,
+// so the next H is nearly diagonal and the Jacobi sweeps are few.  ctl[1]: 0 go on, 2 failed
+// (rank-deficient block or a non-finite λ); ctl[2]: a Ritz pair was formed.
+template <int K>
+__device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm, double* Hm,
+                                       double* Vm, double* cs, double* ritz, float* Rinv,
+                                       float* qv, int* ctl, int lane) {
+  const bool first = (it == 0);
+  const bool rr = !first && ((K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter));
+  if (rr) jacobi_warp<K>(Hm, Vm, cs, lane);
+  if (lane == 0) {
+    int st = 0;
+    ctl[2] = rr ? 1 : 0;
+    if (rr) {
+      int best = 0;
+      for (int i = 1; i < K; ++i)
+        if (Hm[i * K + i] > Hm[best * K + best]) best = i;
+      const double lam = Hm[best * K + best];
+      for (int i = 0; i < K; ++i) qv[i] = (float)Vm[i * K + best];
+      double th[kMaxK];  // Ritz values, descending
+      for (int i = 0; i < K; ++i) th[i] = Hm[i * K + i];
+      for (int i = 0; i < K; ++i)
+        for (int j = i + 1; j < K; ++j)
+          if (th[j] > th[i]) {
+            const double tmp = th[i];
+            th[i] = th[j];
+            th[j] = tmp;
+          }
+      for (int i = 0; i < K; ++i) ritz[i] = th[i];
+      ritz[kMaxK] = lam;
+      if (!isfinite(lam)) st = 2;
+    }
+    if (st == 0) {
+      double Gp[kMaxK][kMaxK];
+      if (rr) {  // VᵀGV
+        double T[kMaxK][kMaxK];
+        for (int i = 0; i < K; ++i)
+          for (int j = 0; j < K; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < K; ++k) s += Gm[i * K + k] * Vm[k * K + j];
+            T[i][j] = s;
+          }
+        for (int i = 0; i < K; ++i)
+          for (int j = 0; j < K; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < K; ++k) s += Vm[k * K + i] * T[k][j];
+            Gp[i][j] = s;
+          }
+      } else {
+        for (int i = 0; i < K; ++i)
+          for (int j = 0; j < K; ++j) Gp[i][j] = Gm[i * K + j];
+      }
+      double L[kMaxK][kMaxK];
+      double tr = 0.0;
+      for (int i = 0; i < K; ++i) tr += Gp[i][i];
+      bool ok = tr > 0.0 && isfinite(tr);
+      for (int j = 0; j < K && ok; ++j) {
+        double d = Gp[j][j];
+        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+        if (!(d > 1e-24 * tr)) {
+          ok = false;
+          break;
+        }
+        L[j][j] = sqrt(d);
+        for (int i = j + 1; i < K; ++i) {
+          double s = Gp[i][j];
+          for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+          L[i][j] = s / L[j][j];
+        }
+      }
+      if (!ok) {  // rank-deficient block: no result for this matrix
+        st = 2;
+      } else {
+        double Li[kMaxK][kMaxK];  // L⁻¹ (lower)
+        for (int j = 0; j < K; ++j) {
+          Li[j][j] = 1.0 / L[j][j];
+          for (int i = j + 1; i < K; ++i) {
+            double s = 0.0;
+            for (int k = j; k < i; ++k) s += L[i][k] * Li[k][j];
+            Li[i][j] = -s / L[i][i];
+          }
+        }
+        // M = V·L⁻ᵀ (or L⁻ᵀ without a rotation); (L⁻ᵀ)[k][j] = Li[j][k] for k <= j
+        for (int i = 0; i < K; ++i)
+          for (int j = 0; j < K; ++j) {
+            double s = 0.0;
+            if (rr) {
+              for (int k = 0; k <= j; ++k) s += Vm[i * K + k] * Li[j][k];
+            } else {
+              s = (i <= j) ? Li[j][i] : 0.0;
+            }
+            Rinv[i * K + j] = (float)s;
+          }
+      }
+    }
+    if (st == 2) {
+      for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = nan("");
+      a.iters[mi] = -1;
+    }
+    ctl[1] = st;
+  }
+}
+
 template <int K, int GC>
 __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ Args a) {
   constexpr int NV = K * GC;
@@ -225,8 +346,15 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   float* Rinv = reinterpret_cast<float*>(smem + SL::rinv);
   float* qv = reinterpret_cast<float*>(smem + SL::qv);
   double* cs = reinterpret_cast<double*>(smem + SL::cs);
+  double* ritz = reinterpret_cast<double*>(smem + SL::ritz);
   int* ctl = reinterpret_cast<int*>(smem + SL::ctl);
   float* Xs = reinterpret_cast<float*>(smem + SL::xs);  // X, one copy for all teams: [v][row]
+  float* cdf = reinterpret_cast<float*>(smem + SL::cdf);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(smem + SL::hist);
+  int32_t* lcol = reinterpret_cast<int32_t*>(smem + SL::lcol);
+  float* lw = reinterpret_cast<float*>(smem + SL::lw);
+  uint32_t* scan = reinterpret_cast<uint32_t*>(smem + SL::scan);
+  double* dscan = reinterpret_cast<double*>(smem + SL::scan + 40 * 4);
 
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   for (;;) {
@@ -244,6 +372,68 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     const int team = t / P, tl = t % P;
     const int team_warp0 = team * (P / 32);
     const int r0 = 4 * tl;
+    const bool amm = M.c > 0;
+    double total = 0.0;
+    if (amm) {
+      // ---- column norms² (get_norms, device_memory.h:34-59) into cdf[], then the CDF ----
+      int buf = 0;
+      for (int g0 = team * GC; g0 < n; g0 += NT * GC, buf ^= 1) {
+        float d[GC];
+#pragma unroll
+        for (int c = 0; c < GC; ++c) {
+          float4 av = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (r0 < m && g0 + c < n)
+            av = __ldg(reinterpret_cast<const float4*>(M.A + r0 + (int64_t)(g0 + c) * M.ld));
+          if (r0 + 1 >= m) av.y = 0.f;
+          if (r0 + 2 >= m) av.z = 0.f;
+          if (r0 + 3 >= m) av.w = 0.f;
+          d[c] = fmaf(av.x, av.x, fmaf(av.y, av.y, fmaf(av.z, av.z, av.w * av.w)));
+        }
+        const float red = team_allreduce<GC>(d, part, buf, warp, lane, P, team, team_warp0);
+        if (tl < GC * (32 / GC) && (lane % (32 / GC)) == 0) {
+          const int c = lane / (32 / GC);
+          if (g0 + c < n) cdf[g0 + c] = red;
+        }
+      }
+      __syncthreads();
+      // inclusive prefix in FP64, stored as FP32 (set_weights / CUB scan, common.h:34-40 and
+      // powerMethod_by_previous.cuh:26-32); each thread owns a run of consecutive columns
+      const int per = (n + kThreads - 1) / kThreads;
+      const int j0 = t * per, j1 = min(n, j0 + per);
+      double run = 0.0;
+      for (int j = j0; j < j1; ++j) run += (double)cdf[j];
+      // block exclusive scan of the run totals (FP64, fixed order)
+      double incl = run;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) dscan[warp] = incl;
+      __syncthreads();
+      if (warp == 0) {
+        double w = lane < kWarps ? dscan[lane] : 0.0;
+        double wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const double y = __shfl_up_sync(0xffffffffu, wi, o);
+          if (lane >= o) wi += y;
+        }
+        if (lane < kWarps) dscan[lane] = wi - w;
+        if (lane == 31) dscan[kWarps] = wi;
+      }
+      __syncthreads();
+      double pre = dscan[warp] + incl - run;
+      total = dscan[kWarps];
+      __syncthreads();
+      for (int j = j0; j < j1; ++j) {
+        const float nj = cdf[j];
+        pre += (double)nj;
+        cdf[j] = (float)pre;  // in place: this thread alone reads and writes cdf[j0, j1)
+        hist[j] = 0u;
+      }
+      __syncthreads();
+    }
 
     // ---- start block X0 (hash), orthonormalised below like every later Y ----
     float Y[4][K];
@@ -258,7 +448,6 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         *reinterpret_cast<float4*>(Xs + v * kMaxRows + r0) = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
 
-    double lam_prev = 0.0;
     int it = 0, state = 0;  // state: 0 running, 1 converged / last, 2 degenerate
     for (;; ++it) {
       // ---- Gram matrices of the block: G = YᵀY, H = sym(XᵀY) (FP64, team 0 contributes) ----
@@ -304,88 +493,40 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         }
         __syncthreads();
       }
-      // ---- warp 0: Rayleigh–Ritz (every rr_period steps and at the end), Cholesky of G ----
-      if (warp == 0) {
-        const bool first = (it == 0);
-        if (!first) {
-          const bool check = (K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter);
-          if (check) {
-            jacobi_warp<K>(Hm, Vm, cs, lane);
-            if (lane == 0) {
-              int best = 0;
-              for (int i = 1; i < K; ++i)
-                if (Hm[i * K + i] > Hm[best * K + best]) best = i;
-              const double lam = Hm[best * K + best];
-              for (int i = 0; i < K; ++i) qv[i] = (float)Vm[i * K + best];
-              int st = 0;
-              if (!(fabs(lam - lam_prev) > a.tol * fabs(lam)) || it >= a.max_iter) st = 1;
-              if (!isfinite(lam)) st = 2;
-              lam_prev = lam;
-              ctl[1] = st;
-              if (st) {
-                // Ritz values, descending
-                double th[kMaxK];
-                for (int i = 0; i < K; ++i) th[i] = Hm[i * K + i];
-                for (int i = 0; i < K; ++i)
-                  for (int j = i + 1; j < K; ++j)
-                    if (th[j] > th[i]) {
-                      const double tmp = th[i];
-                      th[i] = th[j];
-                      th[j] = tmp;
-                    }
-                for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = th[i];
-                a.iters[mi] = (st == 2) ? -1 : it;
-              }
-            }
-          } else if (lane == 0) {
-            ctl[1] = 0;
-          }
-        } else if (lane == 0) {
-          ctl[1] = 0;
-        }
-        __syncwarp();
-        if (lane == 0 && ctl[1] == 0) {
-          // G = L·Lᵀ; Rinv = L⁻ᵀ (upper triangular), so that X = Y·Rinv has orthonormal columns
-          double L[kMaxK][kMaxK];
-          double tr = 0.0;
-          for (int i = 0; i < K; ++i) tr += Gm[i * K + i];
-          bool ok = tr > 0.0 && isfinite(tr);
-          for (int j = 0; j < K && ok; ++j) {
-            double d = Gm[j * K + j];
-            for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
-            if (!(d > 1e-24 * tr)) {
-              ok = false;
-              break;
-            }
-            L[j][j] = sqrt(d);
-            for (int i = j + 1; i < K; ++i) {
-              double s = Gm[i * K + j];
-              for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
-              L[i][j] = s / L[j][j];
-            }
-          }
-          if (!ok) {
-            ctl[1] = 2;
-            if (!first) {
-              for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = nan("");
-            }
-            a.iters[mi] = -1;
-          } else {
-            double Li[kMaxK][kMaxK];  // L⁻¹ (lower)
-            for (int j = 0; j < K; ++j) {
-              Li[j][j] = 1.0 / L[j][j];
-              for (int i = j + 1; i < K; ++i) {
-                double s = 0.0;
-                for (int k = j; k < i; ++k) s += L[i][k] * Li[k][j];
-                Li[i][j] = -s / L[i][i];
-              }
-            }
-            for (int i = 0; i < K; ++i)
-              for (int j = 0; j < K; ++j) Rinv[i * K + j] = (j >= i) ? (float)Li[j][i] : 0.f;
-          }
-        }
-      }
+      if (warp == 0) ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, lane);
       __syncthreads();
+      if (ctl[2] && ctl[1] == 0) {
+        // residual of the top Ritz pair, r = C·v − λ·v = (Y − λ·X)·q, over team 0's rows (FP64)
+        const double lam = ritz[kMaxK];
+        double r2 = 0.0;
+        if (team == 0 && r0 < m) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            float yq = 0.f, xq = 0.f;
+#pragma unroll
+            for (int v = 0; v < K; ++v) {
+              yq = fmaf(Y[e][v], qv[v], yq);
+              xq = fmaf(Xs[v * kMaxRows + r0 + e], qv[v], xq);
+            }
+            const double r = (double)yq - lam * (double)xq;
+            r2 = fma(r, r, r2);
+          }
+        }
+        r2 = warp_sum(r2);
+        if (lane == 0) gpart[warp] = r2;
+        __syncthreads();
+        if (t == 0) {
+          double s = 0.0;
+          for (int w = 0; w < kWarps; ++w) s += gpart[w];
+          const bool done = sqrt(s) <= a.tol * fabs(lam) || it >= a.max_iter;
+          if (done) {
+            for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = ritz[i];
+            a.iters[mi] = it;
+            ctl[1] = 1;
+          }
+        }
+        __syncthreads();
+      }
       state = ctl[1];
       if (state != 0) {
         if (state == 1 && team == 0) {  // v = X·q over this thread's rows
@@ -401,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         }
         break;
       }
-      // ---- X <- Y·Rinv (team 0 writes the shared copy) ----
+      // ---- X <- Y·M (team 0 writes the shared copy) ----
       if (team == 0) {
 #pragma unroll
         for (int j = 0; j < K; ++j) {
@@ -410,14 +551,55 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           for (int e = 0; e < 4; ++e) {
             float s = 0.f;
 #pragma unroll
-            for (int i = 0; i <= j; ++i) s = fmaf(Y[e][i], Rinv[i * K + j], s);
+            for (int i = 0; i < K; ++i) s = fmaf(Y[e][i], Rinv[i * K + j], s);
             xj[e] = s;
           }
           *reinterpret_cast<float4*>(Xs + j * kMaxRows + r0) = make_float4(xj[0], xj[1], xj[2], xj[3]);
         }
       }
       __syncthreads();
-      // ---- Y = C·X: the fused pass over the columns (team-local) ----
+      // ---- AMM: draw c columns (get_rand + pick_index, device_memory.h:506-545) and list the
+      // distinct ones in ascending order with weight multiplicity / (c·p_j) ----
+      int ncols = n;
+      if (amm) {
+        const float total_f = cdf[n - 1];
+        uint32_t* st = a.states + M.st_off;
+        for (int k = t; k < M.c; k += kThreads) {
+          const uint32_t y = xorshift32(st[k]);
+          st[k] = y;
+          const float target = __fmul_rn(total_f, uniform_from(y));
+          int lo = 0, hi = n;  // first i with cdf[i] > target, else n - 1
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf[mid] <= target)
+              lo = mid + 1;
+            else
+              hi = mid;
+          }
+          atomicAdd(&hist[lo < n ? lo : n - 1], 1u);
+        }
+        __syncthreads();
+        const int per = (n + kThreads - 1) / kThreads;
+        const int j0 = t * per, j1 = min(n, j0 + per);
+        uint32_t nz = 0;
+        for (int j = j0; j < j1; ++j) nz += hist[j] ? 1u : 0u;
+        uint32_t cd = 0;
+        uint32_t r = block_exclusive_scan(nz, scan, &cd);
+        for (int j = j0; j < j1; ++j) {
+          const uint32_t mult = hist[j];
+          if (mult) {
+            // the realised probability of column j is its FP32 CDF step over the total
+            const double step = (double)cdf[j] - (j > 0 ? (double)cdf[j - 1] : 0.0);
+            lcol[r] = j;
+            lw[r] = (float)((double)mult * (double)total_f / ((double)M.c * step));
+            ++r;
+            hist[j] = 0u;
+          }
+        }
+        ncols = (int)cd;
+        __syncthreads();
+      }
+      // ---- Y = C·X (or its AMM estimate): the fused pass over the columns (team-local) ----
 #pragma unroll
       for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -425,17 +607,31 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       const bool rows = r0 < m;
       const float* __restrict__ Ab = M.A + r0;
       int buf = 0;
-      for (int g0 = team * GC; g0 < n; g0 += NT * GC, buf ^= 1) {
-        float4 av[GC];
+      // this team's columns of group g0 (weights in AMM mode); rows past m (the padding up to
+      // ld) count as zero
+      auto load_group = [&](int g0, float4 (&av)[GC], float (&wt)[GC]) {
 #pragma unroll
         for (int c = 0; c < GC; ++c) {
           av[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (rows && g0 + c < n)
-            av[c] = __ldcs(reinterpret_cast<const float4*>(Ab + (int64_t)(g0 + c) * M.ld));
-          if (r0 + 1 >= m) av[c].y = 0.f;  // rows past m (the padding up to ld) count as zero
+          wt[c] = 1.f;
+          const int col = (g0 + c < ncols) ? (amm ? lcol[g0 + c] : g0 + c) : -1;
+          if (amm && col >= 0) wt[c] = lw[g0 + c];
+          if (rows && col >= 0)
+            av[c] = __ldcs(reinterpret_cast<const float4*>(Ab + (int64_t)col * M.ld));
+          if (r0 + 1 >= m) av[c].y = 0.f;
           if (r0 + 2 >= m) av[c].z = 0.f;
           if (r0 + 3 >= m) av[c].w = 0.f;
         }
+      };
+      float4 av[GC];
+      float wt[GC];
+      if (team * GC < ncols) load_group(team * GC, av, wt);
+      for (int g0 = team * GC; g0 < ncols; g0 += NT * GC, buf ^= 1) {
+        // the next group's loads are issued before this group's reduction (one group ahead)
+        float4 nav[GC];
+        float nwt[GC];
+        const bool more = g0 + NT * GC < ncols;
+        if (more) load_group(g0 + NT * GC, nav, nwt);
         float d[NV];
 #pragma unroll
         for (int v = 0; v < K; ++v) {
@@ -454,12 +650,19 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         for (int c = 0; c < GC; ++c)
 #pragma unroll
           for (int v = 0; v < K; ++v) {
-            const float tc = __shfl_sync(0xffffffffu, red, (c * K + v) * (32 / NV));
+            const float tc = __shfl_sync(0xffffffffu, red, (c * K + v) * (32 / NV)) * wt[c];
             Y[0][v] = fmaf(av[c].x, tc, Y[0][v]);
             Y[1][v] = fmaf(av[c].y, tc, Y[1][v]);
             Y[2][v] = fmaf(av[c].z, tc, Y[2][v]);
             Y[3][v] = fmaf(av[c].w, tc, Y[3][v]);
           }
+        if (more) {
+#pragma unroll
+          for (int c = 0; c < GC; ++c) {
+            av[c] = nav[c];
+            wt[c] = nwt[c];
+          }
+        }
       }
       // ---- sum the team partials of Y (fixed order), every team receives the total ----
       if (NT > 1) {
@@ -533,16 +736,16 @@ struct Variant {
 };
 
 static const Variant kVariants[] = {
-    {1, 8, batch_kernel<1, 8>},   {1, 16, batch_kernel<1, 16>},
-    {4, 2, batch_kernel<4, 2>},   {4, 4, batch_kernel<4, 4>},   {4, 8, batch_kernel<4, 8>},
-    {8, 1, batch_kernel<8, 1>},   {8, 2, batch_kernel<8, 2>},   {8, 4, batch_kernel<8, 4>},
+    {1, 4, batch_kernel<1, 4>}, {1, 8, batch_kernel<1, 8>}, {4, 2, batch_kernel<4, 2>},
+    {4, 4, batch_kernel<4, 4>}, {8, 1, batch_kernel<8, 1>}, {8, 2, batch_kernel<8, 2>},
+    {8, 4, batch_kernel<8, 4>},
 };
 
-static int smem_bytes(int K) {
+static int smem_bytes(int K, bool amm) {
   switch (K) {
-    case 1: return Smem<1>::total;
-    case 4: return Smem<4>::total;
-    default: return Smem<8>::total;
+    case 1: return amm ? Smem<1>::total_amm : Smem<1>::total;
+    case 4: return amm ? Smem<4>::total_amm : Smem<4>::total;
+    default: return amm ? Smem<8>::total_amm : Smem<8>::total;
   }
 }
 
@@ -563,6 +766,8 @@ struct amm_batch {
   std::vector<int32_t> order;
   int64_t vec_len = 0;
   int64_t total_cols = 0;
+  int64_t n_states = 0;
+  bool amm = false;
   // device memory (one allocation)
   void* mem = nullptr;
   Mat* d_mats = nullptr;
@@ -571,6 +776,8 @@ struct amm_batch {
   int64_t* d_col_start = nullptr;
   float** d_grads = nullptr;
   int64_t* d_grad_ld = nullptr;
+  uint32_t* d_states0 = nullptr;  // seeded xorshift states (AMM mode), copied per run
+  uint32_t* d_states = nullptr;
   int variant = -1;  // chosen tile shape (index into kVariants)
   std::map<int, float> tune_ms;
   cudaGraph_t graph = nullptr;
@@ -607,7 +814,7 @@ struct Guard {
 int launch(amm_batch* b, int variant, int grid, double* d_lam, float* d_vec, int32_t* d_iters,
            int max_iter, const int32_t* order, int count, cudaStream_t s) {
   const auto& V = amm::batch::kVariants[variant];
-  const int sm = amm::batch::smem_bytes(V.K);
+  const int sm = amm::batch::smem_bytes(V.K, b->amm);
   BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   amm::batch::Args a{};
   a.mats = b->d_mats;
@@ -618,10 +825,14 @@ int launch(amm_batch* b, int variant, int grid, double* d_lam, float* d_vec, int
   a.rr_period = b->cfg.rr_period > 0 ? b->cfg.rr_period : 1;
   a.seed = b->cfg.seed;
   a.queue = b->d_queue;
+  a.states = b->d_states;
   a.lam = d_lam;
   a.vec = d_vec;
   a.iters = d_iters;
   BATCH_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(uint32_t), s));
+  if (b->amm)  // every run draws from the seeded states
+    BATCH_CUDA(cudaMemcpyAsync(b->d_states, b->d_states0, sizeof(uint32_t) * b->n_states,
+                               cudaMemcpyDeviceToDevice, s));
   V.fn<<<grid, amm::batch::kThreads, sm, s>>>(a);
   amm::count_launch(1);
   BATCH_CUDA(cudaGetLastError());
@@ -673,11 +884,12 @@ void amm_batch_config_default(amm_batch_config* c) {
   std::memset(c, 0, sizeof(*c));
   c->nvec = 8;
   c->max_iter = 500;
-  c->tol = 1e-7;
+  c->tol = 1e-6;
   c->rr_period = 1;
   c->use_graph = 1;
   c->seed = 1234;
   c->tile_gc = 0;
+  c->c_divisor = 0;
 }
 
 int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t count,
@@ -685,12 +897,14 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   if (!out || !mats || !cfg || count < 1 || count > (1 << 20)) return AMM_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   if (cfg->nvec != 1 && cfg->nvec != 4 && cfg->nvec != 8) return AMM_ERR_UNSUPPORTED;
-  if (cfg->max_iter < 1 || !(cfg->tol >= 0.0) || cfg->rr_period < 0) return AMM_ERR_INVALID_ARGUMENT;
+  if (cfg->max_iter < 1 || !(cfg->tol >= 0.0) || cfg->rr_period < 0 || cfg->c_divisor < 0)
+    return AMM_ERR_INVALID_ARGUMENT;
+  const bool amm_mode = cfg->c_divisor > 0;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AMM_ERR_NO_DEVICE;
   if (device < 0 || device >= ndev) return AMM_ERR_INVALID_ARGUMENT;
   std::vector<Mat> ms((size_t)count);
-  int64_t off = 0, cols = 0;
+  int64_t off = 0, cols = 0, nst = 0;
   for (int64_t i = 0; i < count; ++i) {
     const amm_batch_matrix& x = mats[i];
     if (!x.A || x.m < 1 || x.n < 1 || x.ld < x.m) return AMM_ERR_INVALID_ARGUMENT;
@@ -702,6 +916,16 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
     ms[i].m = (int32_t)x.m;
     ms[i].n = (int32_t)x.n;
     ms[i].out_off = off;
+    ms[i].st_off = nst;
+    ms[i].c = 0;
+    if (amm_mode) {
+      if (x.n > amm::batch::kMaxCols) return AMM_ERR_UNSUPPORTED;
+      int64_t c = x.n / cfg->c_divisor;
+      if (c < 1) c = 1;
+      if (c > amm::batch::kMaxPicks) return AMM_ERR_UNSUPPORTED;
+      ms[i].c = (int32_t)c;
+      nst += c;
+    }
     off += x.m;
     cols += x.n;
   }
@@ -712,6 +936,8 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   b->mats = ms;
   b->vec_len = off;
   b->total_cols = cols;
+  b->n_states = nst;
+  b->amm = amm_mode;
   b->order.resize((size_t)count);
   for (int64_t i = 0; i < count; ++i) b->order[i] = (int32_t)i;
   // largest first (work m·n), ties by index: the queue then balances like LPT scheduling
@@ -733,6 +959,8 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   const size_t o_cols = carve(sizeof(int64_t) * (count + 1), 256);
   const size_t o_grads = carve(sizeof(float*) * count, 256);
   const size_t o_gld = carve(sizeof(int64_t) * count, 256);
+  const size_t o_st0 = carve(sizeof(uint32_t) * (nst > 0 ? nst : 1), 256);
+  const size_t o_st = carve(sizeof(uint32_t) * (nst > 0 ? nst : 1), 256);
   cudaError_t e = cudaMalloc(&b->mem, bytes);
   if (e != cudaSuccess) {
     delete b;
@@ -745,6 +973,8 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   b->d_col_start = reinterpret_cast<int64_t*>(base + o_cols);
   b->d_grads = reinterpret_cast<float**>(base + o_grads);
   b->d_grad_ld = reinterpret_cast<int64_t*>(base + o_gld);
+  b->d_states0 = reinterpret_cast<uint32_t*>(base + o_st0);
+  b->d_states = reinterpret_cast<uint32_t*>(base + o_st);
   std::vector<int64_t> cs((size_t)count + 1, 0);
   for (int64_t i = 0; i < count; ++i) cs[i + 1] = cs[i] + ms[i].n;
   e = cudaMemcpy(b->d_mats, ms.data(), sizeof(Mat) * count, cudaMemcpyHostToDevice);
@@ -753,6 +983,21 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_col_start, cs.data(), sizeof(int64_t) * (count + 1),
                    cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nst > 0) {
+    // xorshift32 states: a splitmix64 stream from the seed (never zero, a fixed point)
+    std::vector<uint32_t> st((size_t)nst);
+    uint64_t z = cfg->seed;
+    for (int64_t k = 0; k < nst; ++k) {
+      z += 0x9E3779B97F4A7C15ull;
+      uint64_t x = z;
+      x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+      x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+      x ^= x >> 31;
+      const uint32_t v = (uint32_t)(x >> 32);
+      st[(size_t)k] = v ? v : 0x6A09E667u;
+    }
+    e = cudaMemcpy(b->d_states0, st.data(), sizeof(uint32_t) * nst, cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     cudaFree(b->mem);
     delete b;

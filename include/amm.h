@@ -216,10 +216,14 @@ typedef struct amm_batch_config {
   int32_t nvec;       /* block size: 1, 4 or 8                                          */
   int32_t rr_period;  /* Rayleigh–Ritz (and convergence test) every rr_period steps      */
   int64_t max_iter;   /* products per matrix at most                                     */
-  double tol;         /* stop when |Δλ_max| <= tol·λ_max between two Rayleigh–Ritz steps */
+  double tol;         /* stop when ‖C·v − λ_max·v‖ <= tol·λ_max (v: the top Ritz vector)  */
   uint64_t seed;      /* start block (counter-based hash of seed, matrix, row, vector)    */
   int32_t use_graph;  /* replay the launch from a CUDA graph                             */
   int32_t tile_gc;    /* columns per group; 0 lets the autotuner choose                  */
+  int32_t c_divisor;  /* 0: exact products; k > 0: previous-AMM products with c = n/k      */
+                      /* samples per step (n <= 8192, c <= 1024), drawn as pick_index does */
+                      /* from a seeded xorshift32 state per sample, every run from the seed */
+  int32_t pad;
 } amm_batch_config;
 
 void amm_batch_config_default(amm_batch_config *cfg);

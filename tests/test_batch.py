@@ -1,7 +1,8 @@
 """Batched λ_max (amm_batch_*) and its backward, called through the C ABI.
 
-λ and v are compared with FP64 LAPACK (numpy eigh on C = A·Aᵀ): λ_max within rtol 1e-5 for
-the 8-vector block and 1e-4 for the single vector; the gradient 2·v(vᵀA) within 1e-4 (relative,
+The solver stops at a residual ‖C·v − λ·v‖ <= 1e-6·λ.  λ and v are compared with FP64 LAPACK
+(numpy eigh on C = A·Aᵀ): λ_max within rtol 1e-5 for the 4- and 8-vector blocks and 1e-4 for
+the single vector; the gradient 2·v(vᵀA) within 1e-4 (relative,
 Frobenius) of FP64 torch.linalg.eigvalsh autograd and within 1e-3·max|g| of central finite
 differences (h = 1e-3, FP64) on 32 entries.
 """
@@ -58,12 +59,14 @@ def test_batch_config_validation(amm_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nvec,rtol", [(8, 1e-5), (4, 1e-5), (1, 1e-4)])
-def test_batch_lambda_and_vector_vs_fp64(amm_lib, nvec, rtol):
+@pytest.mark.parametrize("nvec,rtol,vtol", [(8, 1e-5, 2e-5), (4, 1e-5, 2e-5), (1, 1e-4, 1e-3)])
+def test_batch_lambda_and_vector_vs_fp64(amm_lib, nvec, rtol, vtol):
+    """At a residual of 1e-6·λ the eigenvector error is about 1e-6·λ_1/(λ_1 − λ_2): the single
+    vector (no Rayleigh–Ritz over a block) gets the looser bound on 1 − |v·v*|."""
     from eigenvaluecomputation_by_amm_b200 import BatchSolver
     host = _mats(SIZES, seed=5)
     keep = [_device_col_major(A) for A in host]
-    bs = BatchSolver([v for _, v in keep], nvec=nvec, max_iter=3000, tol=1e-10)
+    bs = BatchSolver([v for _, v in keep], nvec=nvec, max_iter=3000, tol=1e-6)
     lam, vec, iters = bs.run()
     torch.cuda.synchronize()
     lam = lam.cpu().numpy()
@@ -74,7 +77,7 @@ def test_batch_lambda_and_vector_vs_fp64(amm_lib, nvec, rtol):
         assert abs(lam[i] - w[0]) <= rtol * w[0], (i, lam[i], w[0], it[i])
         v = bs.vector(i).cpu().numpy().astype(np.float64)
         assert abs(np.linalg.norm(v) - 1.0) < 1e-5
-        assert abs(float(v @ V[:, 0])) > 1 - 2e-5, i
+        assert abs(float(v @ V[:, 0])) > 1 - vtol, i
     bs.close()
 
 
@@ -85,7 +88,7 @@ def test_batch_ritz_values_and_one_launch_per_matrix(amm_lib):
     from eigenvaluecomputation_by_amm_b200 import BatchSolver
     host = _mats(SIZES[:5], seed=9)
     keep = [_device_col_major(A) for A in host]
-    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=3000, tol=1e-11)
+    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=3000, tol=1e-6)
     bs.run()
     lam1 = bs.lam.clone()
     vec1 = bs.vectors.clone()
@@ -96,10 +99,14 @@ def test_batch_ritz_values_and_one_launch_per_matrix(amm_lib):
     bs.run()  # graph replay: deterministic
     assert torch.equal(lam1, bs.lam)
     for i, A in enumerate(host):
+        # the stop is on the top pair; the next Ritz values are converged less far
         w, _ = _eigh_top(A, 3)
-        np.testing.assert_allclose(lam1[i, :3].cpu().numpy(), w, rtol=1e-4)
+        got = lam1[i, :3].cpu().numpy()
+        assert abs(got[0] - w[0]) <= 1e-5 * w[0]
+        np.testing.assert_allclose(got[1:], w[1:], rtol=2e-3)
     k, gc = bs.tile_choice()
     assert k == 8 and gc in (1, 2, 4)
+    assert int(bs.iters.max()) < 3000  # stopped on the residual, not on max_iter
     bs.close()
 
 
@@ -111,7 +118,7 @@ def test_lambda_max_gradient_vs_eigvalsh_and_finite_differences():
     A = (rng.standard_normal((B, m, n)) * np.exp(0.5 * rng.standard_normal((B, 1, n))))
     A = A.astype(np.float32)
     tA = torch.from_numpy(A).cuda().requires_grad_(True)
-    lam = lambda_max(tA, max_iter=3000)
+    lam = lambda_max(tA, max_iter=3000, tol=1e-9)
     lam.sum().backward()
     g = tA.grad.double().cpu()
     # FP64 eigvalsh autograd
@@ -140,7 +147,7 @@ def test_batch_gradient_scale_and_layout(amm_lib):
     from eigenvaluecomputation_by_amm_b200 import BatchSolver
     host = _mats([(96, 300), (200, 150)], seed=11)
     keep = [_device_col_major(A) for A in host]
-    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=2000, tol=1e-10)
+    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=2000, tol=1e-6)
     bs.run()
     grads, stores = [], []
     for A in host:
@@ -156,4 +163,33 @@ def test_batch_gradient_scale_and_layout(amm_lib):
         got = grads[i].double().cpu().numpy()
         np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-5 * np.abs(want).max())
         assert torch.all(stores[i][:, A.shape[0]:] == 7.0)
+    bs.close()
+
+
+@pytest.mark.gpu
+def test_batch_amm_mode_spiked_matrices(amm_lib):
+    """Previous-AMM products (c = n/8) in the batch: reproducible from the seed, identical with
+    one launch per matrix, and within 2% of λ_max where a spike shared by every column dominates
+    (then every sampled column carries the top direction)."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver
+    rng = np.random.default_rng(21)
+    host = []
+    for m, n in [(64, 256), (200, 1600), (517, 4096), (1024, 8192)]:
+        u = rng.standard_normal(m)
+        u /= np.linalg.norm(u)
+        A = 0.05 * rng.standard_normal((m, n)) + u[:, None] * rng.uniform(0.5, 1.5, n)[None, :]
+        host.append(A.astype(np.float32))
+    keep = [_device_col_major(A) for A in host]
+    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=12, tol=0.0, c_divisor=8)
+    bs.run()
+    lam1 = bs.lam.clone()
+    bs.run()
+    assert torch.equal(lam1, bs.lam)
+    bs.run(each=True)
+    torch.cuda.synchronize()
+    assert torch.equal(lam1, bs.lam)
+    for i, A in enumerate(host):
+        w, _ = _eigh_top(A)
+        assert abs(lam1[i, 0].item() - w[0]) <= 0.02 * w[0], (i, lam1[i, 0].item(), w[0])
+    assert int(bs.iters.min()) == 12
     bs.close()
