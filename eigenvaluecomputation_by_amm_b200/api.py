@@ -286,7 +286,7 @@ class BatchSolver:
 
     def __init__(self, mats, nvec: int = 8, max_iter: int = 500, tol: float = 1e-6,
                  rr_period: int = 1, seed: int = 1234, use_graph: bool = True, tile_gc: int = 0,
-                 c_divisor: int = 0, device: Optional[int] = None):
+                 c_divisor: int = 0, cluster: int = 0, device: Optional[int] = None):
         self.lib = _lib.load()
         self.mats = list(mats)
         self.count = len(self.mats)
@@ -306,6 +306,7 @@ class BatchSolver:
         cfg.rr_period, cfg.seed = int(rr_period), int(seed)
         cfg.use_graph, cfg.tile_gc = (1 if use_graph else 0), int(tile_gc)
         cfg.c_divisor = int(c_divisor)
+        cfg.cluster = int(cluster)
         self._b = C.c_void_p()
         check(self.lib.amm_batch_create(C.byref(self._b), descs, self.count, C.byref(cfg),
                                         self.device), "amm_batch_create")
@@ -338,9 +339,11 @@ class BatchSolver:
               "amm_batch_grad")
 
     def tile_choice(self):
-        k, gc = C.c_int32(0), C.c_int32(0)
-        check(self.lib.amm_batch_tile_choice(self._b, C.byref(k), C.byref(gc)), "amm_batch_tile_choice")
-        return int(k.value), int(gc.value)
+        """(vectors, columns per group, CTAs per matrix) picked by the autotuner."""
+        k, gc, cl = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        check(self.lib.amm_batch_tile_choice(self._b, C.byref(k), C.byref(gc), C.byref(cl)),
+              "amm_batch_tile_choice")
+        return int(k.value), int(gc.value), int(cl.value)
 
     def close(self):
         if self._b:

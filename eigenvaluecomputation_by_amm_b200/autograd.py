@@ -17,7 +17,7 @@ from .api import BatchSolver
 
 __all__ = ["lambda_max", "LambdaMax"]
 
-# tile shape picked by the autotuner, per batch shape signature
+# tile shape (columns per group, CTAs per matrix) picked by the autotuner, per batch shape
 _TILES: Dict[Tuple, int] = {}
 
 
@@ -40,11 +40,12 @@ class LambdaMax(torch.autograd.Function):
         buf = _column_major_batch(A)
         mats = [buf[b].t()[:m] for b in range(B)]            # (m, n) views, stride (1, ld)
         key = (B, m, n, nvec)
-        solver = BatchSolver(mats, nvec=nvec, max_iter=max_iter, tol=tol,
-                             tile_gc=_TILES.get(key, 0), use_graph=False)
+        gc, cl = _TILES.get(key, (0, 0))
+        solver = BatchSolver(mats, nvec=nvec, max_iter=max_iter, tol=tol, tile_gc=gc,
+                             cluster=cl, use_graph=False)
         lam, _, iters = solver.run()
         if key not in _TILES:
-            _TILES[key] = solver.tile_choice()[1]
+            _TILES[key] = solver.tile_choice()[1:]
         lam = lam.clone()
         ctx.solver = solver
         ctx.buf = buf

@@ -84,7 +84,7 @@ def bench_batch(args):
         bs = BatchSolver(mats, nvec=8, max_iter=args.iters, tol=0.0, c_divisor=cdiv)
         t_one = time_runs(bs, each=False)
         t_each = time_runs(bs, each=True)
-        k, gc = bs.tile_choice()
+        k, gc, cl = bs.tile_choice()
         lam = bs.lam[:, 0].double().cpu().numpy()
         errs = []
         for i in range(0, args.count, max(1, args.count // args.check)):
@@ -94,7 +94,7 @@ def bench_batch(args):
         res = {"matrices_per_s": args.count * 1000.0 / t_one, "ms_per_launch": t_one,
                "one_launch_per_matrix_matrices_per_s": args.count * 1000.0 / t_each,
                "ms_one_launch_per_matrix": t_each, "speedup_vs_launch_per_matrix": t_each / t_one,
-               "tile_cols_per_group": gc, "lambda_rel_err_max": max(errs),
+               "tile_cols_per_group": gc, "ctas_per_matrix": cl, "lambda_rel_err_max": max(errs),
                "lambda_rel_err_median": float(np.median(errs)), "checked": len(errs)}
         if cdiv == 0:
             ach = bytes_per_product * args.iters / (t_one * 1e-3) / 1e9

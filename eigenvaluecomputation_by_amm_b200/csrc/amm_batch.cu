@@ -18,6 +18,7 @@
 // iterations (and at the end) H is diagonalised by a warp-parallel cyclic Jacobi in FP64: its
 // largest eigenvalue is λ_max, its eigenvector q gives v = X·q.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -76,6 +77,17 @@ __device__ __forceinline__ float4 lds_f4(const float* p) {
                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                : "r"((uint32_t)__cvta_generic_to_shared(p)));
   return v;
+}
+
+// Shared-memory position of X[row][v].  For an even block the vectors are interleaved in pairs
+// ([v/2][row][2]) so that a thread's 4 rows of a vector pair are two 16-byte loads holding the
+// float2 operands of the packed FMAs.
+template <int K>
+__device__ __forceinline__ int xs_idx(int v, int row) {
+  if constexpr (K % 2 == 0)
+    return (v >> 1) * (2 * kMaxRows) + row * 2 + (v & 1);
+  else
+    return v * kMaxRows + row;
 }
 
 // Start block: a counter-based hash of (seed, matrix, row, vector) -> uniform [-1, 1).
@@ -234,7 +246,7 @@ __device__ __forceinline__ float team_allreduce(float (&d)[NV], float* part, int
 template <int K>
 __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm, double* Hm,
                                        double* Vm, double* cs, double* ritz, float* Rinv,
-                                       float* qv, int* ctl, int lane) {
+                                       float* qv, int* ctl, int lane, bool writer) {
   const bool first = (it == 0);
   const bool rr = !first && ((K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter));
   if (rr) jacobi_warp<K>(Hm, Vm, cs, lane);
@@ -323,7 +335,7 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
           }
       }
     }
-    if (st == 2) {
+    if (st == 2 && writer) {
       for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = nan("");
       a.iters[mi] = -1;
     }
@@ -357,11 +369,17 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   double* dscan = reinterpret_cast<double*>(smem + SL::scan + 40 * 4);
 
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int CL = (int)cluster.num_blocks();   // CTAs sharing one matrix
+  const int crank = (int)cluster.block_rank();
+  const bool writer = (crank == 0);           // rank 0 writes the results
   for (;;) {
-    if (t == 0) ctl[0] = (int)atomicAdd(a.queue, 1u);
-    __syncthreads();
-    const int item = ctl[0];
-    __syncthreads();
+    // rank 0 takes the next matrix from the queue; the cluster reads it from rank 0
+    if (writer && t == 0) ctl[0] = (int)atomicAdd(a.queue, 1u);
+    cluster.sync();
+    const int item = *cluster.map_shared_rank(&ctl[0], 0);
+    cluster.sync();
     if (item >= a.count) return;
     const int mi = a.order[item];
     const Mat M = a.mats[mi];
@@ -370,6 +388,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     while (P < kThreads && 4 * P < m) P <<= 1;
     const int NT = kThreads / P;
     const int team = t / P, tl = t % P;
+    const int NTG = CL * NT;             // teams of the whole cluster split the columns
+    const int gteam = crank * NT + team;
     const int team_warp0 = team * (P / 32);
     const int r0 = 4 * tl;
     const bool amm = M.c > 0;
@@ -377,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     if (amm) {
       // ---- column norms² (get_norms, device_memory.h:34-59) into cdf[], then the CDF ----
       int buf = 0;
-      for (int g0 = team * GC; g0 < n; g0 += NT * GC, buf ^= 1) {
+      for (int g0 = gteam * GC; g0 < n; g0 += NTG * GC, buf ^= 1) {
         float d[GC];
 #pragma unroll
         for (int c = 0; c < GC; ++c) {
@@ -394,6 +414,14 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           const int c = lane / (32 / GC);
           if (g0 + c < n) cdf[g0 + c] = red;
         }
+      }
+      if (CL > 1) {  // norms of the columns the other CTAs of the cluster own
+        cluster.sync();
+        for (int j = t; j < n; j += kThreads) {
+          const int owner = ((j / GC) % NTG) / NT;
+          if (owner != crank) cdf[j] = *cluster.map_shared_rank(&cdf[j], owner);
+        }
+        cluster.sync();  // nobody overwrites its norms before every CTA has gathered
       }
       __syncthreads();
       // inclusive prefix in FP64, stored as FP32 (set_weights / CUB scan, common.h:34-40 and
@@ -445,7 +473,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     if (team == 0)
 #pragma unroll
       for (int v = 0; v < K; ++v)
-        *reinterpret_cast<float4*>(Xs + v * kMaxRows + r0) = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) Xs[xs_idx<K>(v, r0 + e)] = 0.f;
     __syncthreads();
 
     int it = 0, state = 0;  // state: 0 running, 1 converged / last, 2 degenerate
@@ -459,9 +488,12 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           for (int b0 = a0; b0 < K; ++b0, ++pidx) {
             double g = 0.0, h = 0.0;
             if (contrib) {
-              const float4 xa = *reinterpret_cast<const float4*>(Xs + a0 * kMaxRows + r0);
-              const float4 xb = *reinterpret_cast<const float4*>(Xs + b0 * kMaxRows + r0);
-              const float xav[4] = {xa.x, xa.y, xa.z, xa.w}, xbv[4] = {xb.x, xb.y, xb.z, xb.w};
+              float xav[4], xbv[4];
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                xav[e] = Xs[xs_idx<K>(a0, r0 + e)];
+                xbv[e] = Xs[xs_idx<K>(b0, r0 + e)];
+              }
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
                 g = fma((double)Y[e][a0], (double)Y[e][b0], g);
@@ -493,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         }
         __syncthreads();
       }
-      if (warp == 0) ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, lane);
+      if (warp == 0) ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, lane, writer);
       __syncthreads();
       if (ctl[2] && ctl[1] == 0) {
         // residual of the top Ritz pair, r = C·v − λ·v = (Y − λ·X)·q, over team 0's rows (FP64)
@@ -506,7 +538,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
 #pragma unroll
             for (int v = 0; v < K; ++v) {
               yq = fmaf(Y[e][v], qv[v], yq);
-              xq = fmaf(Xs[v * kMaxRows + r0 + e], qv[v], xq);
+              xq = fmaf(Xs[xs_idx<K>(v, r0 + e)], qv[v], xq);
             }
             const double r = (double)yq - lam * (double)xq;
             r2 = fma(r, r, r2);
@@ -520,8 +552,10 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           for (int w = 0; w < kWarps; ++w) s += gpart[w];
           const bool done = sqrt(s) <= a.tol * fabs(lam) || it >= a.max_iter;
           if (done) {
-            for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = ritz[i];
-            a.iters[mi] = it;
+            if (writer) {
+              for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = ritz[i];
+              a.iters[mi] = it;
+            }
             ctl[1] = 1;
           }
         }
@@ -529,13 +563,13 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       }
       state = ctl[1];
       if (state != 0) {
-        if (state == 1 && team == 0) {  // v = X·q over this thread's rows
+        if (state == 1 && team == 0 && writer) {  // v = X·q over this thread's rows
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             if (r0 + e < m) {
               float s = 0.f;
 #pragma unroll
-              for (int v = 0; v < K; ++v) s = fmaf(Xs[v * kMaxRows + r0 + e], qv[v], s);
+              for (int v = 0; v < K; ++v) s = fmaf(Xs[xs_idx<K>(v, r0 + e)], qv[v], s);
               a.vec[M.out_off + r0 + e] = s;
             }
           }
@@ -554,7 +588,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             for (int i = 0; i < K; ++i) s = fmaf(Y[e][i], Rinv[i * K + j], s);
             xj[e] = s;
           }
-          *reinterpret_cast<float4*>(Xs + j * kMaxRows + r0) = make_float4(xj[0], xj[1], xj[2], xj[3]);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) Xs[xs_idx<K>(j, r0 + e)] = xj[e];
         }
       }
       __syncthreads();
@@ -564,9 +599,21 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       if (amm) {
         const float total_f = cdf[n - 1];
         uint32_t* st = a.states + M.st_off;
-        for (int k = t; k < M.c; k += kThreads) {
-          const uint32_t y = xorshift32(st[k]);
-          st[k] = y;
+        // every CTA of the cluster draws the same picks from the same states; rank 0 stores the
+        // advanced states once all have read them
+        uint32_t ys[kMaxPicks / kThreads];
+#pragma unroll
+        for (int u = 0; u < kMaxPicks / kThreads; ++u) {
+          const int k = t + u * kThreads;
+          ys[u] = k < M.c ? xorshift32(st[k]) : 0u;
+        }
+        if (CL > 1) cluster.sync();
+#pragma unroll
+        for (int u = 0; u < kMaxPicks / kThreads; ++u) {
+          const int k = t + u * kThreads;
+          if (k >= M.c) continue;
+          const uint32_t y = ys[u];
+          if (writer) st[k] = y;
           const float target = __fmul_rn(total_f, uniform_from(y));
           int lo = 0, hi = n;  // first i with cdf[i] > target, else n - 1
           while (lo < hi) {
@@ -625,37 +672,77 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       };
       float4 av[GC];
       float wt[GC];
-      if (team * GC < ncols) load_group(team * GC, av, wt);
-      for (int g0 = team * GC; g0 < ncols; g0 += NT * GC, buf ^= 1) {
+      if (gteam * GC < ncols) load_group(gteam * GC, av, wt);
+      for (int g0 = gteam * GC; g0 < ncols; g0 += NTG * GC, buf ^= 1) {
         // the next group's loads are issued before this group's reduction (one group ahead)
         float4 nav[GC];
         float nwt[GC];
-        const bool more = g0 + NT * GC < ncols;
-        if (more) load_group(g0 + NT * GC, nav, nwt);
+        const bool more = g0 + NTG * GC < ncols;
+        if (more) load_group(g0 + NTG * GC, nav, nwt);
         float d[NV];
+        if constexpr (K % 2 == 0) {
+          // packed FP32x2: a vector pair per instruction (X pairs interleaved in shared memory)
 #pragma unroll
-        for (int v = 0; v < K; ++v) {
-          const float4 xv = lds_f4(Xs + v * kMaxRows + r0);
+          for (int vp = 0; vp < K / 2; ++vp) {
+            const float4 x01 = lds_f4(Xs + vp * 2 * kMaxRows + 2 * r0);      // rows 0, 1
+            const float4 x23 = lds_f4(Xs + vp * 2 * kMaxRows + 2 * r0 + 4);  // rows 2, 3
+            const float2 xr[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
+                                  make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
 #pragma unroll
-          for (int c = 0; c < GC; ++c) {
-            float s = av[c].x * xv.x;
-            s = fmaf(av[c].y, xv.y, s);
-            s = fmaf(av[c].z, xv.z, s);
-            s = fmaf(av[c].w, xv.w, s);
-            d[c * K + v] = s;
+            for (int c = 0; c < GC; ++c) {
+              float2 s = __fmul2_rn(make_float2(av[c].x, av[c].x), xr[0]);
+              s = __ffma2_rn(make_float2(av[c].y, av[c].y), xr[1], s);
+              s = __ffma2_rn(make_float2(av[c].z, av[c].z), xr[2], s);
+              s = __ffma2_rn(make_float2(av[c].w, av[c].w), xr[3], s);
+              d[c * K + 2 * vp] = s.x;
+              d[c * K + 2 * vp + 1] = s.y;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < K; ++v) {
+            const float4 xv = lds_f4(Xs + v * kMaxRows + r0);
+#pragma unroll
+            for (int c = 0; c < GC; ++c) {
+              float s = av[c].x * xv.x;
+              s = fmaf(av[c].y, xv.y, s);
+              s = fmaf(av[c].z, xv.z, s);
+              s = fmaf(av[c].w, xv.w, s);
+              d[c * K + v] = s;
+            }
           }
         }
         const float red = team_allreduce<NV>(d, part, buf, warp, lane, P, team, team_warp0);
+        if constexpr (K % 2 == 0) {
 #pragma unroll
-        for (int c = 0; c < GC; ++c)
+          for (int c = 0; c < GC; ++c)
 #pragma unroll
-          for (int v = 0; v < K; ++v) {
-            const float tc = __shfl_sync(0xffffffffu, red, (c * K + v) * (32 / NV)) * wt[c];
-            Y[0][v] = fmaf(av[c].x, tc, Y[0][v]);
-            Y[1][v] = fmaf(av[c].y, tc, Y[1][v]);
-            Y[2][v] = fmaf(av[c].z, tc, Y[2][v]);
-            Y[3][v] = fmaf(av[c].w, tc, Y[3][v]);
-          }
+            for (int vp = 0; vp < K / 2; ++vp) {
+              float2 tc = make_float2(
+                  __shfl_sync(0xffffffffu, red, (c * K + 2 * vp) * (32 / NV)),
+                  __shfl_sync(0xffffffffu, red, (c * K + 2 * vp + 1) * (32 / NV)));
+              if (amm) tc = __fmul2_rn(tc, make_float2(wt[c], wt[c]));
+              const float ae[4] = {av[c].x, av[c].y, av[c].z, av[c].w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const float2 y2 = __ffma2_rn(make_float2(ae[e], ae[e]), tc,
+                                             make_float2(Y[e][2 * vp], Y[e][2 * vp + 1]));
+                Y[e][2 * vp] = y2.x;
+                Y[e][2 * vp + 1] = y2.y;
+              }
+            }
+        } else {
+#pragma unroll
+          for (int c = 0; c < GC; ++c)
+#pragma unroll
+            for (int v = 0; v < K; ++v) {
+              const float tc = __shfl_sync(0xffffffffu, red, (c * K + v) * (32 / NV)) * wt[c];
+              Y[0][v] = fmaf(av[c].x, tc, Y[0][v]);
+              Y[1][v] = fmaf(av[c].y, tc, Y[1][v]);
+              Y[2][v] = fmaf(av[c].z, tc, Y[2][v]);
+              Y[3][v] = fmaf(av[c].w, tc, Y[3][v]);
+            }
+        }
         if (more) {
 #pragma unroll
           for (int c = 0; c < GC; ++c) {
@@ -684,6 +771,30 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
               Y[e][v] = s;
             }
         }
+      }
+      // ---- sum the CTA partials of the cluster through distributed shared memory (fixed
+      // rank order): every CTA receives the same Y ----
+      if (CL > 1) {
+        __syncthreads();
+        if (team == 0 && rows) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int v = 0; v < K; ++v) yred[(r0 + e) * K + v] = Y[e][v];
+        }
+        cluster.sync();
+        if (rows) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int v = 0; v < K; ++v) {
+              float s = 0.f;
+              for (int rk = 0; rk < CL; ++rk)
+                s += *cluster.map_shared_rank(&yred[(r0 + e) * K + v], rk);
+              Y[e][v] = s;
+            }
+        }
+        cluster.sync();  // the buffers are rewritten by the next step
       }
     }
     __syncthreads();
@@ -734,6 +845,7 @@ struct Variant {
   int K, GC;
   KernelFn fn;
 };
+constexpr int kClusterSizes[] = {1, 2, 4, 8};
 
 static const Variant kVariants[] = {
     {1, 4, batch_kernel<1, 4>}, {1, 8, batch_kernel<1, 8>}, {4, 2, batch_kernel<4, 2>},
@@ -779,7 +891,9 @@ struct amm_batch {
   uint32_t* d_states0 = nullptr;  // seeded xorshift states (AMM mode), copied per run
   uint32_t* d_states = nullptr;
   int variant = -1;  // chosen tile shape (index into kVariants)
-  std::map<int, float> tune_ms;
+  int cluster = 1;   // CTAs per matrix (cluster size)
+  int grid = 0;      // CTAs of the persistent launch for that cluster size
+  std::map<std::pair<int, int>, float> tune_ms;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t cap = nullptr;
@@ -811,11 +925,44 @@ struct Guard {
   }
 };
 
-int launch(amm_batch* b, int variant, int grid, double* d_lam, float* d_vec, int32_t* d_iters,
-           int max_iter, const int32_t* order, int count, cudaStream_t s) {
+// CTAs of a persistent launch with clusters of cl CTAs: as many clusters as fit at once (one
+// CTA per SM), and no more than there are matrices.  0 if that cluster size cannot run.
+int persistent_grid(amm_batch* b, int variant, int cl) {
+  const auto& V = amm::batch::kVariants[variant];
+  const int sm = amm::batch::smem_bytes(V.K, b->amm);
+  if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
+    return 0;
+  if (cl > 1 &&
+      cudaFuncSetAttribute(V.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl * b->nsm, 1, 1);
+  cfg.blockDim = dim3(amm::batch::kThreads, 1, 1);
+  cfg.dynamicSmemBytes = sm;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&nclusters, (void*)V.fn, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (nclusters < 1) return 0;
+  const int64_t use = std::min<int64_t>(nclusters, b->count);
+  return (int)use * cl;
+}
+
+int launch(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_vec,
+           int32_t* d_iters, int max_iter, const int32_t* order, int count, cudaStream_t s) {
   const auto& V = amm::batch::kVariants[variant];
   const int sm = amm::batch::smem_bytes(V.K, b->amm);
   BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  if (cl > 1)
+    BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   amm::batch::Args a{};
   a.mats = b->d_mats;
   a.order = order;
@@ -833,45 +980,65 @@ int launch(amm_batch* b, int variant, int grid, double* d_lam, float* d_vec, int
   if (b->amm)  // every run draws from the seeded states
     BATCH_CUDA(cudaMemcpyAsync(b->d_states, b->d_states0, sizeof(uint32_t) * b->n_states,
                                cudaMemcpyDeviceToDevice, s));
-  V.fn<<<grid, amm::batch::kThreads, sm, s>>>(a);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(amm::batch::kThreads, 1, 1);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  BATCH_CUDA(cudaLaunchKernelEx(&cfg, V.fn, a));
   amm::count_launch(1);
   BATCH_CUDA(cudaGetLastError());
   return AMM_OK;
 }
 
-// Tile-shape autotuner: every variant with the requested K runs the whole batch for a few
-// iterations; the fastest (CUDA events) is kept for the context.
+// Tile-shape autotuner: every (columns per group, cluster size) pair with the requested K runs
+// the whole batch for a few iterations; the fastest (CUDA events) is kept for the context.
 int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaStream_t s) {
   if (b->variant >= 0) return AMM_OK;
-  int best = -1;
+  int best = -1, best_cl = 1, best_grid = 0;
   float best_ms = 0.f;
   cudaEvent_t e0, e1;
   BATCH_CUDA(cudaEventCreate(&e0));
   BATCH_CUDA(cudaEventCreate(&e1));
-  const int grid = (int)std::min<int64_t>(b->count, (int64_t)b->nsm);
   const int n_var = (int)(sizeof(amm::batch::kVariants) / sizeof(amm::batch::kVariants[0]));
   for (int v = 0; v < n_var; ++v) {
     if (amm::batch::kVariants[v].K != b->cfg.nvec) continue;
     if (b->cfg.tile_gc > 0 && amm::batch::kVariants[v].GC != b->cfg.tile_gc) continue;
-    int rc = launch(b, v, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);  // warm
-    if (rc) return rc;
-    BATCH_CUDA(cudaEventRecord(e0, s));
-    rc = launch(b, v, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);
-    if (rc) return rc;
-    BATCH_CUDA(cudaEventRecord(e1, s));
-    BATCH_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    b->tune_ms[v] = ms;
-    if (best < 0 || ms < best_ms) {
-      best = v;
-      best_ms = ms;
+    for (int cl : amm::batch::kClusterSizes) {
+      if (b->cfg.cluster > 0 && cl != b->cfg.cluster) continue;
+      const int grid = persistent_grid(b, v, cl);
+      if (grid <= 0) continue;
+      int rc = launch(b, v, cl, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);
+      if (rc) return rc;
+      BATCH_CUDA(cudaEventRecord(e0, s));
+      rc = launch(b, v, cl, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);
+      if (rc) return rc;
+      BATCH_CUDA(cudaEventRecord(e1, s));
+      BATCH_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      b->tune_ms[{v, cl}] = ms;
+      if (best < 0 || ms < best_ms) {
+        best = v;
+        best_cl = cl;
+        best_grid = grid;
+        best_ms = ms;
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (best < 0) return AMM_ERR_UNSUPPORTED;
   b->variant = best;
+  b->cluster = best_cl;
+  b->grid = best_grid;
   return AMM_OK;
 }
 
@@ -890,6 +1057,7 @@ void amm_batch_config_default(amm_batch_config* c) {
   c->seed = 1234;
   c->tile_gc = 0;
   c->c_divisor = 0;
+  c->cluster = 0;
 }
 
 int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t count,
@@ -1032,10 +1200,9 @@ int amm_batch_run(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_i
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   int rc = autotune(b, d_lambda, d_vectors, d_iters, s);
   if (rc) return rc;
-  const int grid = (int)std::min<int64_t>(b->count, (int64_t)b->nsm);
   if (!b->cfg.use_graph)
-    return launch(b, b->variant, grid, d_lambda, d_vectors, d_iters, (int)b->cfg.max_iter,
-                  b->d_order, (int)b->count, s);
+    return launch(b, b->variant, b->cluster, b->grid, d_lambda, d_vectors, d_iters,
+                  (int)b->cfg.max_iter, b->d_order, (int)b->count, s);
   if (b->gexec && (b->g_lam != d_lambda || b->g_vec != d_vectors || b->g_iters != d_iters)) {
     cudaGraphExecDestroy(b->gexec);
     cudaGraphDestroy(b->graph);
@@ -1046,8 +1213,8 @@ int amm_batch_run(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_i
     if (!b->cap) BATCH_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
     BATCH_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed));
     const int64_t before = amm::launch_count();
-    rc = launch(b, b->variant, grid, d_lambda, d_vectors, d_iters, (int)b->cfg.max_iter,
-                b->d_order, (int)b->count, b->cap);
+    rc = launch(b, b->variant, b->cluster, b->grid, d_lambda, d_vectors, d_iters,
+                (int)b->cfg.max_iter, b->d_order, (int)b->count, b->cap);
     cudaGraph_t gr = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(b->cap, &gr);
     amm::count_launch(-(int)(amm::launch_count() - before));
@@ -1081,8 +1248,8 @@ int amm_batch_run_each(amm_batch* b, double* d_lambda, float* d_vectors, int32_t
   // one single-CTA launch per matrix; each reads its matrix index from a one-entry slice of
   // the order array
   for (int64_t i = 0; i < b->count; ++i) {
-    rc = launch(b, b->variant, 1, d_lambda, d_vectors, d_iters, (int)b->cfg.max_iter,
-                b->d_order + i, 1, s);
+    rc = launch(b, b->variant, b->cluster, b->cluster, d_lambda, d_vectors, d_iters,
+                (int)b->cfg.max_iter, b->d_order + i, 1, s);
     if (rc) return rc;
   }
   return AMM_OK;
@@ -1119,11 +1286,12 @@ int amm_batch_grad(amm_batch* b, const float* d_vectors, void* const* grad_ptrs,
   return AMM_OK;
 }
 
-int amm_batch_tile_choice(amm_batch* b, int32_t* k_out, int32_t* gc_out) {
+int amm_batch_tile_choice(amm_batch* b, int32_t* k_out, int32_t* gc_out, int32_t* cl_out) {
   if (!b || !k_out || !gc_out) return AMM_ERR_INVALID_ARGUMENT;
   if (b->variant < 0) return AMM_ERR_NOT_READY;
   *k_out = amm::batch::kVariants[b->variant].K;
   *gc_out = amm::batch::kVariants[b->variant].GC;
+  if (cl_out) *cl_out = b->cluster;
   return AMM_OK;
 }
 

@@ -223,7 +223,7 @@ typedef struct amm_batch_config {
   int32_t c_divisor;  /* 0: exact products; k > 0: previous-AMM products with c = n/k      */
                       /* samples per step (n <= 8192, c <= 1024), drawn as pick_index does */
                       /* from a seeded xorshift32 state per sample, every run from the seed */
-  int32_t pad;
+  int32_t cluster;    /* CTAs (a thread-block cluster) per matrix: 1, 2, 4, 8; 0 = autotune */
 } amm_batch_config;
 
 void amm_batch_config_default(amm_batch_config *cfg);
@@ -247,8 +247,10 @@ int amm_batch_run_each(amm_batch *b, double *d_lambda, float *d_vectors, int32_t
  * count factors or NULL.  Synchronises the stream. */
 int amm_batch_grad(amm_batch *b, const float *d_vectors, void *const *grad_ptrs,
                    const int64_t *grad_ld, const float *d_scale, void *stream);
-/* The tile shape the autotuner picked (AMM_ERR_NOT_READY before the first run). */
-int amm_batch_tile_choice(amm_batch *b, int32_t *nvec, int32_t *cols_per_group);
+/* The tile shape the autotuner picked: block size, columns per group and CTAs per matrix
+ * (cluster size; cluster_size may be NULL).  AMM_ERR_NOT_READY before the first run. */
+int amm_batch_tile_choice(amm_batch *b, int32_t *nvec, int32_t *cols_per_group,
+                          int32_t *cluster_size);
 
 /* Measurement hook: time `reps` back-to-back launches of the fused product kernel for one
  * step kind (AMM_STEP_EXACT, AMM_STEP_PREVIOUS or AMM_STEP_PROPOSED) on the bound matrix,
