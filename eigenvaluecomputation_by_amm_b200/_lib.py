@@ -83,6 +83,8 @@ _SIGS = {
     "amm_get_rng_state": [_P, _P, _I64, _P],
     "amm_seed_rng": [_P, C.c_uint64, _I64, _P],
     "amm_seed_start_vectors": [_P, C.c_uint64],
+    "amm_seed_rng_at": [_P, C.c_uint64, C.c_uint64, _I64, _P],
+    "amm_seed_start_vectors_at": [_P, C.c_uint64, C.c_uint64],
     "amm_draw_start_vector": [_P, _P, _P],
     "amm_set_cdf": [_P, C.c_int, _P, _P],
     "amm_set_eigenvector": [_P, _P, _P],
@@ -102,6 +104,8 @@ _SIGS = {
     "amm_get_sampling_tables": [_P, C.c_int, _P, _P, _P],
     "amm_sample_indices": [_P, C.c_int, _P, _P],
     "amm_pick_sorted_noalloc": [_P, _P, _I64, _P, C.c_int, _I64, _P, _P, _P],
+    "amm_generate_matrix": [C.c_char_p, _I64, C.c_uint64, _P, _P, _P],
+    "amm_read_matrix_file": [C.c_char_p, _P, _I64, _P],
     "amm_batch_config_default": [C.POINTER(amm_batch_config)],
     "amm_batch_create": [C.POINTER(_P), C.POINTER(amm_batch_matrix), _I64,
                          C.POINTER(amm_batch_config), C.c_int],

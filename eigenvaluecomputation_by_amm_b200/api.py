@@ -15,7 +15,8 @@ import torch
 from . import _lib
 from ._lib import AmmError, amm_config, check
 
-__all__ = ["AMMContext", "BatchSolver", "column_major", "AmmError"]
+__all__ = ["AMMContext", "BatchSolver", "column_major", "AmmError", "generate_matrix",
+           "read_matrix_file"]
 
 
 def column_major(A: torch.Tensor) -> torch.Tensor:
@@ -355,3 +356,32 @@ class BatchSolver:
             self.close()
         except Exception:
             pass
+
+
+def generate_matrix(matrix_type: str, size: int, seed: int, stream=None, device=None):
+    """The reference's -matrixType generator (amm_generate_matrix): a symmetric size x size FP32
+    matrix (column-major; symmetric, so also row-major) with the diagonal offset added, and the
+    offset."""
+    lib = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else int(device))
+    A = torch.empty(int(size), int(size), dtype=torch.float32, device=dev)
+    off = C.c_float(0.0)
+    check(lib.amm_generate_matrix(matrix_type.encode(), int(size), int(seed), _ptr(A),
+                                  C.byref(off), _stream(stream)), "amm_generate_matrix")
+    return A, float(off.value)
+
+
+def read_matrix_file(path: str, size: Optional[int] = None):
+    """The reference's -filepath loader (amm_read_matrix_file): (host FP32 array of shape
+    (size, size), original size).  size defaults to the file's size rounded up to 128, as the
+    reference pads it."""
+    lib = _lib.load()
+    orig = C.c_int64(0)
+    check(lib.amm_read_matrix_file(str(path).encode(), None, 0, C.byref(orig)),
+          "amm_read_matrix_file")
+    n0 = int(orig.value)
+    size = int(size) if size else (n0 + 127) // 128 * 128
+    out = np.empty((size, size), np.float32)
+    check(lib.amm_read_matrix_file(str(path).encode(), out.ctypes.data_as(C.c_void_p), size,
+                                   C.byref(orig)), "amm_read_matrix_file")
+    return out, n0

@@ -514,6 +514,10 @@ int amm_get_rng_state(amm_ctx* ctx, uint32_t* d_out, int64_t count, void* stream
 }
 
 int amm_seed_rng(amm_ctx* ctx, uint64_t seed, int64_t count, void* stream) {
+  return amm_seed_rng_at(ctx, seed, 0, count, stream);
+}
+
+int amm_seed_rng_at(amm_ctx* ctx, uint64_t seed, uint64_t offset, int64_t count, void* stream) {
   if (!ctx || count < ctx->cfg.c || count > ctx->state_len) return AMM_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(ctx->device);
   cudaStream_t s = as_stream(stream);
@@ -522,6 +526,7 @@ int amm_seed_rng(amm_ctx* ctx, uint64_t seed, int64_t count, void* stream) {
     return AMM_ERR_CUDA;
   curandStatus_t cs = curandSetStream(gen, s);
   if (cs == CURAND_STATUS_SUCCESS) cs = curandSetPseudoRandomGeneratorSeed(gen, seed + 1234ULL);
+  if (cs == CURAND_STATUS_SUCCESS) cs = curandSetGeneratorOffset(gen, offset);
   if (cs == CURAND_STATUS_SUCCESS) cs = curandGenerate(gen, ctx->b.states[0], (size_t)count);
   curandDestroyGenerator(gen);
   if (cs != CURAND_STATUS_SUCCESS) {
@@ -534,6 +539,10 @@ int amm_seed_rng(amm_ctx* ctx, uint64_t seed, int64_t count, void* stream) {
 }
 
 int amm_seed_start_vectors(amm_ctx* ctx, uint64_t seed) {
+  return amm_seed_start_vectors_at(ctx, seed, 0);
+}
+
+int amm_seed_start_vectors_at(amm_ctx* ctx, uint64_t seed, uint64_t offset) {
   if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(ctx->device);
   if (!ctx->x0_gen &&
@@ -542,7 +551,8 @@ int amm_seed_start_vectors(amm_ctx* ctx, uint64_t seed) {
     g_last_cuda_error = "curandCreateGenerator failed";
     return AMM_ERR_CUDA;
   }
-  if (curandSetPseudoRandomGeneratorSeed(ctx->x0_gen, seed) != CURAND_STATUS_SUCCESS) {
+  if (curandSetPseudoRandomGeneratorSeed(ctx->x0_gen, seed) != CURAND_STATUS_SUCCESS ||
+      curandSetGeneratorOffset(ctx->x0_gen, offset) != CURAND_STATUS_SUCCESS) {
     g_last_cuda_error = "curandSetPseudoRandomGeneratorSeed failed";
     return AMM_ERR_CUDA;
   }

@@ -109,12 +109,19 @@ int amm_get_rng_state(amm_ctx *ctx, uint32_t *d_states_out, int64_t count, void 
  * (XORWOW) generator seeded with seed + 1234 (set_internal_randomness,
  * device_memory.h:339-343); count values are generated (the reference uses m). */
 int amm_seed_rng(amm_ctx *ctx, uint64_t seed, int64_t count, void *stream);
+/* The same from position `offset` of that generator's sequence.  The reference drives ONE
+ * generator through the whole run and re-seeding it does not rewind it: the states start
+ * after the values write_data consumed (size² for a -matrixType matrix, none for -filepath). */
+int amm_seed_rng_at(amm_ctx *ctx, uint64_t seed, uint64_t offset, int64_t count, void *stream);
 
 /* Start vectors as the reference draws them: a context-owned default (XORWOW) cuRAND
  * generator re-seeded with `seed` (the reference seeds with 1234 + -seed, AMM.cu:85), and
  * one curandGenerateNormal(m, mean 0, sd 1) per call, continuing the sequence
  * (powerMethod_by_exact.cuh:32 and the same line in every driver). */
 int amm_seed_start_vectors(amm_ctx *ctx, uint64_t seed);
+/* The same from position `offset` (in the reference's main, after everything write_data and
+ * set_internal_randomness drew from its one generator: size² + m or m values). */
+int amm_seed_start_vectors_at(amm_ctx *ctx, uint64_t seed, uint64_t offset);
 int amm_draw_start_vector(amm_ctx *ctx, float *d_x0, void *stream);
 
 /* Replace the sampling CDF of one weighting (0 = ‖A_j‖², previous AMM; 1 = ‖A_j − α_j‖²,
@@ -195,6 +202,22 @@ int amm_sample_indices(amm_ctx *ctx, int which, uint32_t *d_idx, void *stream);
 int amm_pick_sorted_noalloc(const uint32_t *d_states_in, uint32_t *d_states_out, int64_t c,
                             const void *d_cdf, int cdf_precision, int64_t n,
                             uint32_t *d_idx_sorted, int32_t *d_distinct, void *stream);
+
+/* ---- Matrix sources of the reference's driver ----
+ * amm_generate_matrix: the -matrixType generators of generate_matrix (device_memory.h:360-433):
+ * "gaussian_<mean>_<std>", "lognormal_<mean>_<std>" or "uniform_<lo>_<hi>" values from a cuRAND
+ * XORWOW generator seeded with `seed` fill the size x size FP32 matrix d_A (column-major,
+ * ld = size, size·size even), the lower triangle is mirrored into the upper one and the
+ * reference's diagonal offset is added (returned in *offset; the reported eigenvalue of the
+ * driver is sqrt(λ) − offset, powerMethod_by_exact.cuh:83-84).  Same seed, same matrix as the
+ * reference.  Synchronises the stream. */
+int amm_generate_matrix(const char *type, int64_t size, uint64_t seed, float *d_A, float *offset,
+                        void *stream);
+/* amm_read_matrix_file: the -filepath loader (host_memory.h:143-159, device_memory.h:369-401):
+ * a uint32 size header followed by size x size FP32 values; file row y lands at
+ * h_A[y*size + x] of a zero-filled size x size host buffer (the reference's layout, so a
+ * symmetric covariance file reads as itself).  With h_A NULL only *original_size is set. */
+int amm_read_matrix_file(const char *path, float *h_A, int64_t size, int64_t *original_size);
 
 /* ---- Batched λ_max for many independent FP32 matrices (no counterpart in the reference,
  * which solves one matrix per run, AMM.cu:74-95) ----

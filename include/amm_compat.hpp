@@ -159,6 +159,9 @@ struct device_memory {
   cudaStream_t stream_1 = nullptr;
   std::ofstream ofs_output;
   uint32_t seed = 0;
+  // Values drawn so far from the reference's single cuRAND generator, which re-seeding does
+  // not rewind: the matrix (size²) when generated, then the m states; the start vectors follow.
+  uint64_t gen_pos = 0;
 
   explicit device_memory(host_memory& p) {
     m = p.m;
@@ -224,9 +227,39 @@ struct device_memory {
   device_memory(const device_memory&) = delete;
   device_memory& operator=(const device_memory&) = delete;
 
-  // Bind dm.dA (after the caller or a loader filled it), as write_data does (:316-337).
+  // Set by a caller that filled dA itself; otherwise write_data loads or generates A.
+  bool matrix_ready = false;
+
+  // The matrix part of write_data (:316-337 with generate_matrix, :360-433): the -filepath
+  // covariance file (padded with zeros to m), or the -matrixType generator seeded with -seed
+  // (p.diagonal_offset receives its offset).  FP32 storage only; with -bf16 the caller fills
+  // dA and sets matrix_ready.
+  void load_or_generate(host_memory& p) {
+    if (p.bf16) throw amm_compat::error(AMM_ERR_UNSUPPORTED, "write_data: fill dA for -bf16");
+    if (!p.filepath.empty()) {
+      std::vector<float> h((size_t)m * (size_t)m);
+      int64_t orig = 0;
+      amm_compat::check(amm_read_matrix_file(p.filepath.c_str(), h.data(), (int64_t)m, &orig),
+                        "amm_read_matrix_file");
+      if (cudaMemcpy(dA, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice) !=
+          cudaSuccess)
+        throw amm_compat::error(AMM_ERR_CUDA, "write_data upload");
+      p.diagonal_offset = 0.0f;
+    } else {
+      float off = 0.0f;
+      amm_compat::check(amm_generate_matrix(p.matrixType.c_str(), (int64_t)m, seed, (float*)dA,
+                                            &off, stream_1),
+                        "amm_generate_matrix");
+      p.diagonal_offset = off;
+      gen_pos += m * m;
+    }
+    matrix_ready = true;
+  }
+
+  // As the reference's write_data (:316-337): A (loaded, generated, or the caller's when
+  // matrix_ready is set) is bound and its column statistics and ||alpha||^2 are computed.
   void write_data(host_memory& p) {
-    (void)p;
+    if (!matrix_ready) load_or_generate(p);
     amm_compat::check(amm_set_matrix(ctx, dA, (int64_t)m, stream_1), "amm_set_matrix");
     double a2 = 0.0;
     amm_compat::check(
@@ -235,14 +268,17 @@ struct device_memory {
     p.alpha2 = (float)a2;
   }
 
-  // xorshift states from -seed (:339-343).
+  // xorshift states from -seed (:339-343), at the generator's current position.
   void set_internal_randomness() {
-    amm_compat::check(amm_seed_rng(ctx, seed, (int64_t)(m > c ? m : c), stream_1), "amm_seed_rng");
+    const int64_t count = (int64_t)(m > c ? m : c);
+    amm_compat::check(amm_seed_rng_at(ctx, seed, gen_pos, count, stream_1), "amm_seed_rng_at");
+    gen_pos += (uint64_t)count;
   }
 
-  // The start-vector generator, re-seeded like AMM.cu:85 (1234 + seed).
+  // The start-vector generator, re-seeded like AMM.cu:85 (1234 + seed), continuing from the
+  // position the states left it at.
   void seed_start_vectors(uint64_t s) {
-    amm_compat::check(amm_seed_start_vectors(ctx, s), "amm_seed_start_vectors");
+    amm_compat::check(amm_seed_start_vectors_at(ctx, s, gen_pos), "amm_seed_start_vectors_at");
   }
 
   void zero_clear() { is_init = true; }

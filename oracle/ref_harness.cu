@@ -292,4 +292,32 @@ int ref_pick_index(int64_t n, int64_t c, const float *cdf, const uint32_t *state
   return rc;
 }
 
+// The reference's matrix generator (device_memory.h:360-433) for -matrixType `type` and seed
+// `seed` on an m x m matrix: A_out receives dA (column-major) with its diagonal offset added,
+// *offset_out the offset.
+int ref_generate(const char *type, int64_t m, uint32_t seed, float *A_out, float *offset_out) {
+  if (!sizes_ok(m, 8)) return -1;
+  std::vector<float> zero((size_t)m * (size_t)m, 0.0f);
+  Cwd cwd(nullptr, m, zero.data());
+  auto args = make_args("exact", m, 8, 1, 0, 0.0, 0, seed);
+  std::vector<char *> argv;
+  for (auto &s : args) argv.push_back(const_cast<char *>(s.c_str()));
+  host_memory p;
+  if (!p.parser((int)argv.size(), argv.data())) return -1;
+  int rc = 0;
+  {
+    // constructed with -filepath (its result-file naming needs one), then write_data() runs
+    // with the path cleared, which takes the reference's -matrixType generator branch
+    device_memory dm(p);
+    p.filepath = "";
+    p.matrixType = std::string(type);
+    dm.write_data(p);
+    cudaDeviceSynchronize();
+    if (offset_out) *offset_out = p.diagonal_offset;
+    if (A_out) cudaMemcpy(A_out, dm.dA, sizeof(float) * m * m, cudaMemcpyDeviceToHost);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = -3;
+  }
+  return rc;
+}
+
 }  // extern "C"

@@ -34,8 +34,9 @@ def load():
         _lib.ref_amm_steps.argtypes = [C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_int,
                                        P, P, P] + [P] * 7
         _lib.ref_pick_index.argtypes = [C.c_int64, C.c_int64, P, P, P, P]
+        _lib.ref_generate.argtypes = [C.c_char_p, C.c_int64, C.c_uint32, P, P]
         for f in (_lib.ref_draw_x0, _lib.ref_seed_states, _lib.ref_power_method,
-                  _lib.ref_amm_steps, _lib.ref_pick_index):
+                  _lib.ref_amm_steps, _lib.ref_pick_index, _lib.ref_generate):
             f.restype = C.c_int
     return _lib
 
@@ -47,6 +48,15 @@ def _p(a):
 def _check(rc, what):
     if rc != 0:
         raise RuntimeError(f"{what} failed with {rc}")
+
+
+def generate(matrix_type: str, m: int, seed: int):
+    """The reference's generate_matrix (device_memory.h:360-433): (A column-major m x m with the
+    diagonal offset added, offset)."""
+    out = np.zeros(m * m, np.float32)
+    off = np.zeros(1, np.float32)
+    _check(load().ref_generate(matrix_type.encode(), m, seed, _p(out), _p(off)), "ref_generate")
+    return out.reshape(m, m).T, float(off[0])   # element (r, c) at out[r + c*m]
 
 
 def draw_x0(m: int, x0_seed: int) -> np.ndarray:
