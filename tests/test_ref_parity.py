@@ -150,3 +150,38 @@ def test_reference_rectangular_embedding_previous():
     ctx.power_method("previous", ctx_x)
     tr = ctx.trace()
     assert np.all(rel(tr["eigs"][1:], ref["eigs"][1:]) < 1e-4)
+
+
+@pytest.mark.parametrize("kernel", ["previousAMM"])
+def test_eigenfaces_shape_indices_bit_exact_vs_reference(kernel):
+    """The eigenfaces-like configuration (4096 x 16384 FP32, c = 1024; see helpers.
+    eigenfaces_like) through the reference padded with zero rows to 16384 x 16384: after 8
+    steps the sorted index set of the last product and the xorshift states are bit-exact and
+    λ agrees within 1e-4 from the second step on (the padded rows only enter the first
+    normalisation)."""
+    from helpers import eigenfaces_like
+    m, n, c, step = 4096, 16384, 1024, 8
+    A = eigenfaces_like(n, seed=2)
+    Ap = np.zeros((n, n), np.float32)
+    Ap[:m] = A
+    rng = np.random.default_rng(12)
+    st = rng.integers(1, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+    ref = R.power_method(kernel, Ap, 77, st, c=c, step=step)
+    del Ap
+    full = R.draw_x0(n, 77).astype(np.float64)
+    x0s = (full[:m] / np.sqrt((full ** 2).sum())).astype(np.float32)
+    ctx = ctx_for(A, c=c, step=step, cdf_precision="f32")
+    ctx.set_cdf(0, torch.from_numpy(ref["cdf"]))
+    ctx.set_rng_state(tu32(st[:c]))
+    ctx.power_method("previous", torch.from_numpy(x0s).cuda())
+    tr = ctx.trace()
+    assert np.all(rel(tr["eigs"][1:], ref["eigs"][1:]) < 1e-4)
+    got_states = ctx.get_rng_state(c).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got_states, ref["states"][:c])
+    # the last product's picks: drawn (without advancing) from the states after step - 1 steps
+    short = ctx_for(A, c=c, step=step - 1, cdf_precision="f32")
+    short.set_cdf(0, torch.from_numpy(ref["cdf"]))
+    short.set_rng_state(tu32(st[:c]))
+    short.power_method("previous", torch.from_numpy(x0s).cuda())
+    picks = np.sort(short.sample_indices(0).cpu().numpy().view(np.uint32))
+    assert np.array_equal(picks, ref["sorted"])
