@@ -146,6 +146,7 @@ void layout(amm_ctx* ctx, Carver& cv) {
   b.spart = cv.take<float>(b.nsm);
   b.spart64 = cv.take<double>(b.nsm);
   b.rpart = cv.take<double>(4 * b.nsm);
+  b.colsum = cv.take<double2>(n);
   b.ticket = cv.take<uint32_t>(4);
   b.alpha2 = cv.take<double>(1);
   b.colvec = cv.take<float>(n);

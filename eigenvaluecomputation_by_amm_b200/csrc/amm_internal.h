@@ -95,6 +95,7 @@ struct Buffers {
   float* partials;     // nsm x m
   float* spart;        // nsm  (Σ α_k t_k of each CTA, proposed)
   double* spart64;     // nsm  (Σ α_j² of each CTA, set-up)
+  double2* colsum;     // n (Σa, Σa²) of each column from the set-up pass
   double* rpart;       // nsm x 4 (x·y, y·y, y·v*, z·dx) of each CTA
   uint32_t* ticket;    // [0]: last-CTA ticket of a step, [2]: grid-barrier arrivals,
                        // [1], [3]: spare

@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   const int G = gridDim.x;
   const int q = blockIdx.x;
   const int m = b.m;
+  const double inv_m = 1.0 / (double)m;
   const int nvec = m / E;
   const int NS = g.nstages;
   const uint32_t col_bytes = (uint32_t)(m * sizeof(Elem));
@@ -528,21 +529,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       if (qq < cnt) {
         const int k = grp * GC + qq;
         if constexpr (SETUP) {
-          // α_j needs only Σa; the column sums go to global memory for the statistics kernel
+          // α_j = Σa·(1/m) (exactly Σa/m for a power-of-two m); the sums go to colsum and the
+          // column statistics are formed in the epilogue, off this per-group path
           const double sx = sxy[2 * qq];
-          const float af = (float)(sx / (double)m);
+          const float af = (float)(sx * inv_m);
           coef[qq] = af;
           a2acc = fma((double)af, (double)af, a2acc);
-          if (t == qq) {
-            // the column statistics (get_norms, device_memory.h:34-59): α = Σa/m, ‖A_j‖ =
-            // sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² − mean²·m) clamped at 0 (the reference
-            // stores NaN when cancellation makes it negative)
-            const double sy = sxy[2 * qq + 1];
-            const double mean = sx / (double)m;
-            b.alpha[lo + k] = (float)mean;
-            b.norm[lo + k] = (float)sqrt(sy);
-            b.normp[lo + k] = (float)sqrt(fmax(sy - mean * mean * (double)m, 0.0));
-          }
+          if (t == qq) b.colsum[lo + k] = make_double2(sx, sxy[2 * qq + 1]);
         } else {
           const float tot = tots[qq];
           if (!amm) {
@@ -814,6 +807,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     named_barrier_or(1, T, false);  // red is reused by the next row chunk
   }
   if constexpr (SETUP) {
+    // the column statistics (get_norms, device_memory.h:34-59) from the column sums: α = Σa/m
+    // (as the coefficient above), ‖A_j‖ = sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² − mean²·m) clamped
+    // at 0 (the reference stores NaN when cancellation makes it negative)
+    for (int j = q * T + t; j < b.n; j += G * T) {
+      const double2 s = __ldcg(b.colsum + j);
+      const double mean = s.x / (double)m;
+      b.alpha[j] = (float)(s.x * inv_m);
+      b.norm[j] = (float)sqrt(s.y);
+      b.normp[j] = (float)sqrt(fmax(s.y - mean * mean * (double)m, 0.0));
+    }
     if (q == 0 && warp == 0) {
       if (g0 >= g1) {  // no rows here (m/4 < number of CTAs): ‖α‖² is summed separately
         for (int k = lane; k < G; k += 32) S += __ldcg(b.spart64 + k);
