@@ -95,6 +95,8 @@ _SIGS = {
     "amm_power_proposed_v2": [_P, _P, _P],
     "amm_get_trace": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "amm_get_vectors": [_P, _P, _P, _P],
+    "amm_device_clock": [_P, _P],
+    "amm_get_step_clocks": [_P, _P, C.c_int64, _P, _P],
     "amm_core_previousAMM": [_P, _P, _P, _P, _P, _P, _P],
     "amm_core_proposedAMM": [_P, _P, _P, _P, _P, _P, _P],
     "amm_exact_product": [_P, _P, _P, _P],

@@ -24,8 +24,17 @@ def column_major(A: torch.Tensor) -> torch.Tensor:
     return A.t().contiguous().t()
 
 
+# torch's raw accessors of the current device and stream: a fraction of the host time of
+# torch.cuda.current_stream(), which builds a Stream object on every call (this runs once per
+# library call, while the GPU may be idle waiting for the launch)
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_cur_device = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def _stream(stream=None) -> int:
     if stream is None:
+        if _raw_stream is not None and _cur_device is not None:
+            return int(_raw_stream(_cur_device()))
         stream = torch.cuda.current_stream()
     return int(stream.cuda_stream)
 
@@ -156,7 +165,9 @@ class AMMContext:
     # -- power method ---------------------------------------------------------------------
     def power_method(self, method: str, x0: torch.Tensor, stream=None) -> "AMMContext":
         """Enqueue one power-method call (asynchronous); read it with trace()/vectors()."""
-        x0 = x0.to(device=self._dev, dtype=torch.float32).contiguous()
+        if not (x0.dtype == torch.float32 and x0.is_cuda and x0.get_device() == self.device
+                and x0.is_contiguous()):
+            x0 = x0.to(device=self._dev, dtype=torch.float32).contiguous()
         check(self.lib.amm_power_method(self._ctx, _lib.METHODS[method], _ptr(x0), _stream(stream)),
               f"amm_power_method({method})")
         self._x0_keep = x0
@@ -178,6 +189,21 @@ class AMMContext:
         return {"eigs": eigs[:k], "errs": errs[:k], "coss": coss[:k],
                 "kinds": [_lib.STEP_KINDS[int(v)] for v in kinds[:k]], "distinct": distinct[:k],
                 "t_ns": t_ns[:k], "steps_run": k}
+
+    def device_clock(self, out: torch.Tensor, stream=None):
+        """Enqueue a write of the device clock (%globaltimer, ns) into out[0] (int64, CUDA)."""
+        if out.dtype != torch.int64 or out.device.type != "cuda":
+            raise AmmError(_lib.AMM_ERR_INVALID_ARGUMENT, "device_clock: need a CUDA int64 tensor")
+        check(self.lib.amm_device_clock(_ptr(out), _stream(stream)), "amm_device_clock")
+
+    def step_clocks(self, stream=None) -> np.ndarray:
+        """Raw device clock stamps of the last call: [0] end of its first kernel, [i+1] end of
+        step i (ns)."""
+        out = np.zeros(self.step + 1, np.uint64)
+        k = C.c_int64(0)
+        check(self.lib.amm_get_step_clocks(self._ctx, out.ctypes.data_as(C.c_void_p), out.size,
+                                           C.byref(k), _stream(stream)), "amm_get_step_clocks")
+        return out[:k.value]
 
     def vectors(self, stream=None):
         x = torch.empty(self.m, dtype=torch.float32, device=self._dev)

@@ -3,6 +3,7 @@
 #include <curand.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -73,8 +74,6 @@ struct amm_ctx {
   float* y_final = nullptr;
   double* out3 = nullptr;
   cudaStream_t cap_stream = nullptr;
-  cudaStream_t side_stream = nullptr;  // the sampler runs here, concurrently with the product
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   curandGenerator_t x0_gen = nullptr;
   std::map<GraphKey, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
   int last_step = 0;
@@ -128,20 +127,20 @@ void layout(amm_ctx* ctx, Carver& cv) {
   b.x_memo = cv.take<float>(m);
   b.y_memo = cv.take<float>(m);
   b.vstar = cv.take<double>(m);
-  for (int w = 0; w < 2; ++w) {
-    b.states[w] = cv.take<uint32_t>(ctx->state_len);
+  for (int w = 0; w < 2; ++w) b.states[w] = cv.take<uint32_t>(ctx->state_len);
+  for (int w = 0; w < amm::kListWindow; ++w) {
     b.count[w] = cv.take<uint32_t>(n);
     b.chunk[w] = cv.take<uint32_t>(b.nchunks);
     b.samples[w] = cv.take<uint32_t>(c);
   }
   b.distinct_idx = cv.take<uint32_t>(c);
   b.distinct_mult = cv.take<uint32_t>(c);
-  for (int w = 0; w < 2; ++w) {
+  for (int w = 0; w < amm::kListWindow; ++w) {
     b.wl_col[w] = cv.take<uint32_t>(c);
     b.wl_wm[w] = cv.take<float>(c);
     b.wl_al[w] = cv.take<float>(c);
-    b.wl_count[w] = cv.take<uint32_t>(1);
   }
+  b.wl_count = cv.take<uint32_t>(amm::kListWindow);
   b.partials = cv.take<float>((size_t)b.nsm * m);
   b.spart = cv.take<float>(b.nsm);
   b.spart64 = cv.take<double>(b.nsm);
@@ -187,28 +186,15 @@ int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normal
                  cudaStream_t s) {
   const Buffers& b = ctx->b;
   const bool draws = cc.uses_amm && !cc.sanity;
-  if (draws && !ctx->side_stream) {
-    AMM_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
-    AMM_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-    AMM_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
-  }
   AMM_CUDA(amm::launch_init(b, cc, x0, no_normalize, s));
-  if (draws) {
-    AMM_CUDA(amm::launch_sample(b, cc, -1, s));
-    AMM_CUDA(amm::launch_compact(b, cc, -1, s));
-  }
   for (int i = 0; i < cc.step; ++i) {
-    const bool fork = draws && i + 1 < cc.step;
-    if (fork) {
-      AMM_CUDA(cudaEventRecord(ctx->ev_fork, s));
-      AMM_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0));
-      AMM_CUDA(amm::launch_sample(b, cc, i, ctx->side_stream));
-      AMM_CUDA(amm::launch_compact(b, cc, i, ctx->side_stream));
-      AMM_CUDA(cudaEventRecord(ctx->ev_join, ctx->side_stream));
+    // the work lists of the next kListWindow AMM steps, drawn before the first of them: the
+    // step kernels then run back to back with nothing else on the SMs
+    if (draws && i % amm::kListWindow == 0) {
+      AMM_CUDA(amm::launch_sample(b, cc, i, s));
+      AMM_CUDA(amm::launch_compact(b, cc, i, s));
     }
     AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, s));
-    // the next step reads the work list built on the side stream
-    if (fork) AMM_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
   }
   AMM_CUDA(amm::launch_finalize(b, cc, ctx->x_final, ctx->y_final, s));
   return AMM_OK;
@@ -254,7 +240,8 @@ int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
     it = ctx->graphs.emplace(key, std::make_pair(g, ex)).first;
   }
   AMM_CUDA(cudaGraphLaunch(it->second.second, s));
-  amm::count_launch(2 + cc.step + ((cc.uses_amm && !cc.sanity) ? 2 * cc.step : 0));
+  const int refills = (cc.step + amm::kListWindow - 1) / amm::kListWindow;
+  amm::count_launch(2 + cc.step + ((cc.uses_amm && !cc.sanity) ? 2 * refills : 0));
   return AMM_OK;
 }
 
@@ -283,7 +270,7 @@ int read_status(amm_ctx* ctx, cudaStream_t s) {
     AMM_CUDA(cudaMemsetAsync(ctx->b.status, 0, sizeof(uint32_t), s));
     if (st & amm::kDevTimeout) {
       // the sampling buffers may be inconsistent after an aborted kernel
-      for (int w = 0; w < 2; ++w) {
+      for (int w = 0; w < amm::kListWindow; ++w) {
         AMM_CUDA(cudaMemsetAsync(ctx->b.count[w], 0, sizeof(uint32_t) * ctx->cfg.n, s));
         AMM_CUDA(cudaMemsetAsync(ctx->b.chunk[w], 0, sizeof(uint32_t) * ctx->b.nchunks, s));
       }
@@ -469,9 +456,6 @@ int amm_destroy(amm_ctx* ctx) {
   DeviceGuard dg(ctx->device);
   drop_graphs(ctx);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
-  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
-  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->x0_gen) curandDestroyGenerator(ctx->x0_gen);
   if (ctx->pool) cudaFree(ctx->pool);
   delete ctx;
@@ -665,6 +649,27 @@ int amm_get_trace(amm_ctx* ctx, double* eigs, double* errs, double* coss, int32_
   return read_status(ctx, s);
 }
 
+int amm_device_clock(uint64_t* d_out, void* stream) {
+  if (!d_out) return AMM_ERR_INVALID_ARGUMENT;
+  AMM_CUDA(amm::launch_clock(reinterpret_cast<unsigned long long*>(d_out), as_stream(stream)));
+  return AMM_OK;
+}
+
+int amm_get_step_clocks(amm_ctx* ctx, uint64_t* out, int64_t cap, int64_t* count, void* stream) {
+  if (!ctx || !out || cap < 1) return AMM_ERR_INVALID_ARGUMENT;
+  if (!ctx->has_run) return AMM_ERR_NOT_READY;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  amm::IterState st{};
+  AMM_CUDA(cudaMemcpyAsync(&st, ctx->b.st + (ctx->last_step & 1), sizeof(st),
+                           cudaMemcpyDeviceToHost, s));
+  AMM_CUDA(cudaStreamSynchronize(s));
+  const int64_t k = std::min<int64_t>(cap, (int64_t)st.steps_run + 1);
+  AMM_CUDA(cudaMemcpy(out, ctx->b.tstamp, sizeof(uint64_t) * k, cudaMemcpyDeviceToHost));
+  if (count) *count = k;
+  return AMM_OK;
+}
+
 int amm_get_vectors(amm_ctx* ctx, float* d_x, float* d_y, void* stream) {
   if (!ctx) return AMM_ERR_INVALID_ARGUMENT;
   if (!ctx->has_run) return AMM_ERR_NOT_READY;
@@ -819,8 +824,8 @@ int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch
   cc.step = 1;
   AMM_CUDA(amm::launch_init(ctx->b, cc, ctx->x0_buf, 0, s));
   if (cc.uses_amm && !ctx->sanity_active) {
-    AMM_CUDA(amm::launch_sample(ctx->b, cc, -1, s));
-    AMM_CUDA(amm::launch_compact(ctx->b, cc, -1, s));
+    AMM_CUDA(amm::launch_sample(ctx->b, cc, 0, s));
+    AMM_CUDA(amm::launch_compact(ctx->b, cc, 0, s));
   }
   cudaEvent_t e0, e1;
   AMM_CUDA(cudaEventCreate(&e0));
@@ -828,7 +833,8 @@ int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch
   AMM_CUDA(cudaEventRecord(e0, s));
   for (int r = 0; r < reps; ++r) AMM_CUDA(amm::launch_iter_panel(ctx->b, ctx->geom, cc, 0, s));
   AMM_CUDA(cudaEventRecord(e1, s));
-  // drop the picks (finalize with step 0 reads st[0]: pending picks in count[0], states[0] kept)
+  // finalize with step 0 reads the call-start state st[0] (nothing used, nothing pending: the
+  // one list drawn was consumed), so states[0] is kept
   CallCfg fc = cc;
   fc.step = 0;
   AMM_CUDA(amm::launch_finalize(ctx->b, fc, nullptr, nullptr, s));

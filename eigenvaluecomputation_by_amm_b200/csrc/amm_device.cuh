@@ -257,6 +257,26 @@ __device__ __forceinline__ int decide_mode(const CallCfg& cc, int i, double cos_
   }
 }
 
+// Weighting (0 = ‖A_j‖², 1 = ‖A_j − α_j‖²) of a call's AMM step number `list` (0-based count of
+// the steps that consume picks): the proposed_v2 driver samples with ‖A_j‖² during its
+// previous-AMM warm-up (steps 0 .. vr_period-2) and with ‖A_j − α_j‖² after its exact step.
+__device__ __forceinline__ int list_weighting(const CallCfg& cc, int list) {
+  if (cc.method == kMethodPrevious) return 0;
+  if (cc.method == kMethodProposed) return 1;
+  if (cc.method == kMethodProposedV2) return list < cc.vr_period - 1 ? 0 : 1;
+  return 0;
+}
+
+// End of the work lists drawn once the window is refilled ahead of step i (i % kListWindow ==
+// 0), from the state that step i starts with: the next kListWindow AMM steps, but no more than
+// the steps left in the call; lists already drawn stay (pending lists are never redrawn).
+__host__ __device__ __forceinline__ int32_t window_end(const CallCfg& cc, int i,
+                                                       const IterState& st) {
+  const int32_t left = cc.step - i;
+  const int32_t e = st.used + (left < kListWindow ? left : kListWindow);
+  return e > st.drawn ? e : st.drawn;
+}
+
 // The step's scalars from the summed x·y, y·y and y·v* (dotProduct_and_generate_x,
 // common.h:103-153): λ = x·y, err = y·v*/‖y‖, cos = λ/‖y‖, the trace entries and the state of
 // the next step (its kind, the tolerance stop).  Run by one thread once the sums are final.
@@ -279,10 +299,8 @@ __device__ __forceinline__ void finish_step(const Buffers& b, const CallCfg& cc,
   nx.cos_prev = cosv;
   nx.lam_prev = lam;
   nx.steps_run = i + 1;
-  if (consumed && !cc.sanity) {
-    nx.sb = st.sb ^ 1;
-    nx.pb = st.pb ^ 1;
-  }
+  if (consumed && !cc.sanity) nx.used = st.used + 1;
+  if (cc.uses_amm && !cc.sanity && i % kListWindow == 0) nx.drawn = window_end(cc, i, st);
   bool done = false;
   if (!isfinite(lam) || !isfinite(scale)) {
     atomicOr(b.status, (uint32_t)kDevNonFinite);
@@ -294,6 +312,16 @@ __device__ __forceinline__ void finish_step(const Buffers& b, const CallCfg& cc,
   nx.mode = decide_mode(cc, i + 1, cosv, st.last_exact, &le);
   nx.last_exact = le;
   b.st[(i + 1) & 1] = nx;
+}
+
+// ---- programmatic dependent launch (a grid launched with programmatic stream serialization
+// may start while the grid before it in the stream finishes) ----
+// Wait until the preceding grid has completed and its memory is visible (returns at once for
+// a grid launched without the attribute).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Allow the next grid in the stream to be scheduled (its CTAs take SMs as this grid's retire).
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // ---- grid-wide barrier over co-resident CTAs ----

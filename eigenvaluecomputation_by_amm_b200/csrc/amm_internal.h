@@ -17,6 +17,11 @@ constexpr int kMaxThreads = 512;   // panel kernel block size limit
 constexpr int kGcMax = 8;          // columns per pipeline stage, upper bound
 constexpr int kSeg = 32;           // fine-search window of the sampler (elements)
 constexpr int kCoarseMax = 2048;   // coarse CDF table entries held in shared memory
+// AMM work lists drawn ahead.  The picks of an AMM step depend only on the sampling states and
+// the CDF, never on x, so the lists of up to kListWindow consecutive AMM steps are drawn and
+// compacted together before the first of them (one refill every kListWindow steps); list a of a
+// call (its a-th AMM step) lives in slot a % kListWindow.
+constexpr int kListWindow = 8;
 
 // Iteration state, double-buffered by iteration parity: kernels of iteration i read
 // st[i & 1]; the last CTA of the step kernel of iteration i writes st[(i + 1) & 1].
@@ -24,8 +29,8 @@ struct IterState {
   int32_t mode;        // StepKind of this iteration
   int32_t last_exact;  // proposed AMM: index of the last VR step
   int32_t done;        // early stop reached: later kernels of the call do nothing
-  int32_t sb;          // pending picks were drawn from states[sb]; advanced copy in states[sb^1]
-  int32_t pb;          // pending picks live in count[pb] / chunk[pb] / samples[pb]
+  int32_t used;        // work lists consumed by the call's AMM steps so far
+  int32_t drawn;       // work lists drawn so far: lists [used, drawn) are pending
   int32_t steps_run;   // completed steps
   int32_t distinct;    // distinct columns of the last AMM product (written by the panel kernel)
   int32_t pad;
@@ -79,18 +84,18 @@ struct Buffers {
   double* vstar;       // may be null
   int32_t has_vstar;
   // sampling
-  uint32_t* states[2];   // xorshift states (c used)
-  uint32_t* count[2];    // per-column multiplicity of the pending picks (n)
-  uint32_t* chunk[2];    // distinct columns per chunk (nchunks)
-  uint32_t* samples[2];  // raw picks in draw order (c)
+  uint32_t* states[2];   // xorshift states (c used); states[0]: committed at the call start
+  uint32_t* count[kListWindow];    // per slot: per-column multiplicity of the picks (n)
+  uint32_t* chunk[kListWindow];    // per slot: distinct columns per chunk (nchunks)
+  uint32_t* samples[kListWindow];  // per slot: raw picks in draw order (c)
   uint32_t* distinct_idx;   // sorted distinct indices of the last AMM product (c)
   uint32_t* distinct_mult;  // their multiplicities (c)
-  // work list of the pending picks (per pick buffer): sorted distinct columns with their
-  // coefficient data, built by compact_kernel
-  uint32_t* wl_col[2];      // c
-  float* wl_wm[2];          // c: w_j · multiplicity
-  float* wl_al[2];          // c: α_j
-  uint32_t* wl_count[2];    // 1: number of distinct columns
+  // work list of each slot: sorted distinct columns with their coefficient data, built by
+  // compact_kernel
+  uint32_t* wl_col[kListWindow];  // c
+  float* wl_wm[kListWindow];      // c: w_j · multiplicity
+  float* wl_al[kListWindow];      // c: α_j
+  uint32_t* wl_count;             // kListWindow: number of distinct columns of each slot
   // partial sums
   float* partials;     // nsm x m
   float* spart;        // nsm  (Σ α_k t_k of each CTA, proposed)
@@ -144,12 +149,12 @@ cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sani
 // no_normalize: use x0 as x_0 unscaled (single-product entry points).
 cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, int no_normalize,
                         cudaStream_t s);
-// Draw the picks of the first AMM step after step iter (iter = -1: start of a call); for
-// iter >= 0 it may run concurrently with the product of step iter.
+// Refill of the work-list window ahead of step iter (iter % kListWindow == 0): draw the picks of
+// the lists not yet drawn among the next kListWindow AMM steps.
 cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
 // Record a CUDA failure for amm_last_cuda_error and return AMM_ERR_CUDA.
 int record_cuda_failure(cudaError_t e, const char* what);
-// Build the sorted distinct work list of the picks just drawn (same decision as sample_kernel).
+// Build the sorted distinct work lists of the picks just drawn (same decision as sample_kernel).
 cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
 // One step (amm_panel.cu): the product, the grid-wide reduction of the partials into y, the
 // Rayleigh quotient and the next step's state.
@@ -161,6 +166,7 @@ cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, fl
                             cudaStream_t s);
 // Standalone helpers.
 cudaError_t launch_normalize(float* x, int m, cudaStream_t s);
+cudaError_t launch_clock(unsigned long long* out, cudaStream_t s);
 cudaError_t launch_rayleigh(const float* x_in, float* x_out, const float* y, const double* vstar,
                             int m, double* out3, cudaStream_t s);
 cudaError_t launch_sample_only(const Buffers& b, int which, uint32_t* idx, cudaStream_t s);

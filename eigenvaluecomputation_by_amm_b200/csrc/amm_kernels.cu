@@ -1,15 +1,13 @@
 // CUDA kernels of libamm (sm_100a).
 //
-// Hot path per power-method iteration i (all stream-ordered, no host round trip):
-//   panel_kernel   one pass over the columns of this step (all n for an exact step, the
-//                  distinct sampled columns for an AMM step): each column is brought into
-//                  shared memory by a 1-D TMA bulk copy, dotted with dx, and the scaled
-//                  column is accumulated into a per-CTA y in registers.  Each column is read
-//                  from HBM once (the reference reads it twice: previousAMM_kernel1 and _2).
-//   reduce_kernel  deterministic sum of the per-CTA partials, the rank-one terms of the
-//                  proposed method, the memo copy of a VR step, the FP64 Rayleigh sums and
-//                  (last CTA) λ, err, cos, the next scale and the next step's kind; extra
-//                  CTAs draw the next step's samples (xorshift32 + inverse CDF) meanwhile.
+// A power-method call, all stream-ordered with no host round trip:
+//   init_kernel      x0, the memo pair, the first state
+//   sample_kernel,   every kListWindow steps: the picks (xorshift32 + inverse CDF) of the next
+//   compact_kernel   kListWindow AMM steps and their sorted distinct work lists
+//   panel_kernel     one launch per step (amm_panel.cu): the product over the step's columns,
+//                    the grid-wide reduction into y and the Rayleigh quotient / next state
+//   finalize_kernel  x_final, y_final, the committed sampling states
+// plus the CDF construction of the set-up and the standalone helpers.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -24,14 +22,6 @@ namespace amm {
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
-
-// Weighting (0 = ‖A_j‖², 1 = ‖A_j − α_j‖²) of the first AMM step after step i.
-__device__ __forceinline__ int next_amm_weighting(const CallCfg& cc, int i) {
-  if (cc.method == kMethodPrevious) return 0;
-  if (cc.method == kMethodProposed) return 1;
-  if (cc.method == kMethodProposedV2) return (i + 1 < cc.vr_period - 1) ? 0 : 1;
-  return 0;
-}
 
 
 // First index i in [0, n) with cdf[i] > target, else n-1 (device_memory.h:529-543).
@@ -79,13 +69,14 @@ __device__ __forceinline__ uint32_t search_cdf(const F* __restrict__ cdf, const 
   return static_cast<uint32_t>(idx < n ? idx : n - 1);
 }
 
-// Draw the picks of one AMM step for samples k = k0, k0+kstride, ... < c.
-// Writes the advanced states, the raw picks and the multiplicity histogram.
+// Draw the picks of AMM step number `list` of a call for samples k = k0, k0+kstride, ... < c:
+// sample k uses its call-start state advanced list+1 times (one xorshift32 per AMM step, as the
+// reference's one draw per state per step).  Writes the raw picks and the multiplicity histogram.
 template <typename F>
 __device__ void draw_samples(const Buffers& b, int which, const uint32_t* __restrict__ st_in,
-                             uint32_t* __restrict__ st_out, uint32_t* __restrict__ count,
-                             uint32_t* __restrict__ chunk, uint32_t* __restrict__ samples, int k0,
-                             int kstride, const F* coarse_s) {
+                             int list, uint32_t* __restrict__ count, uint32_t* __restrict__ chunk,
+                             uint32_t* __restrict__ samples, int k0, int kstride,
+                             const F* coarse_s) {
   const F* cdf = nullptr;
   if constexpr (sizeof(F) == 8)
     cdf = reinterpret_cast<const F*>(b.cdf64[which]);
@@ -93,8 +84,8 @@ __device__ void draw_samples(const Buffers& b, int which, const uint32_t* __rest
     cdf = reinterpret_cast<const F*>(b.cdf32[which]);
   const F total = cdf[b.n - 1];
   for (int k = k0; k < b.c; k += kstride) {
-    const uint32_t y = xorshift32(st_in[k]);
-    st_out[k] = y;
+    uint32_t y = st_in[k];
+    for (int r = 0; r <= list; ++r) y = xorshift32(y);
     const float u = uniform_from(y);
     F target;
     if constexpr (sizeof(F) == 8)
@@ -126,42 +117,33 @@ __device__ void load_coarse(const Buffers& b, int which, F* coarse_s) {
 struct SampleArgs {
   Buffers b;
   CallCfg cc;
-  int iter;     // draw the picks of the first AMM step after step `iter` (-1: start of a call)
+  int iter;     // the window is refilled ahead of step `iter` (a multiple of kListWindow)
 };
 
-// For iter >= 0 this runs concurrently with the product of step iter: if that step consumes
-// its picks (an AMM step), the next picks are drawn from the advanced states states[sb^1] into
-// the other buffer (count[pb^1], states[sb]); otherwise the pending picks stay valid and
-// nothing is drawn.  For iter = -1 the first picks are drawn from states[0].
+// List number st.drawn + blockIdx.y of the window ahead of step iter, drawn from the call-start
+// states states[0] into its slot, if the window reaches it (see window_end).  The lists of the
+// window are drawn by independent grid rows.
 template <typename F>
 __global__ void __launch_bounds__(256) sample_kernel(const __grid_constant__ SampleArgs a) {
   __shared__ __align__(16) F coarse_s[kCoarseMax];
   const Buffers& b = a.b;
   const CallCfg& cc = a.cc;
-  int sb_in, pb_out;
-  if (a.iter < 0) {
-    sb_in = 0;
-    pb_out = 0;
-  } else {
-    const IterState& st = b.st[a.iter & 1];
-    const bool consumes = st.mode == kPrevious || st.mode == kProposed;
-    if (st.done || !consumes || a.iter + 1 >= cc.step) return;  // uniform over the grid
-    sb_in = st.sb ^ 1;
-    pb_out = st.pb ^ 1;
-  }
-  const int which = next_amm_weighting(cc, a.iter);
+  const IterState& st = b.st[a.iter & 1];
+  const int list = st.drawn + (int)blockIdx.y;
+  if (st.done || list >= window_end(cc, a.iter, st)) return;  // uniform over the CTA
+  const int slot = list % kListWindow;
+  const int which = list_weighting(cc, list);
   load_coarse<F>(b, which, coarse_s);
-  draw_samples<F>(b, which, b.states[sb_in], b.states[sb_in ^ 1], b.count[pb_out],
-                  b.chunk[pb_out], b.samples[pb_out], blockIdx.x * blockDim.x + threadIdx.x,
-                  gridDim.x * blockDim.x, coarse_s);
+  draw_samples<F>(b, which, b.states[0], list, b.count[slot], b.chunk[slot], b.samples[slot],
+                  blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, coarse_s);
 }
 
-// Sorted distinct work list of the picks just drawn (the product kernel's column list): one CTA
-// per kCompactSpan columns counts the picked columns below its range, scans its own range in
-// column order and writes (column, w_j · multiplicity, α_j) at each picked column's rank; CTA 0
-// also writes the list length.  It makes the same decision as sample_kernel and runs after it on
-// the same stream, so it too overlaps the product of step `iter`.  The picks of the first product
-// of a call are also kept as (index, multiplicity) for the single-product entry points.
+// Sorted distinct work lists of the picks just drawn (the product kernel's column lists): per
+// list (grid row) one CTA per kCompactSpan columns counts the picked columns below its range,
+// scans its own range in column order and writes (column, w_j · multiplicity, α_j) at each picked
+// column's rank; CTA 0 of the row also writes the list length.  It makes the same decision as
+// sample_kernel and runs after it on the same stream.  The picks of the first list of a call are
+// also kept as (index, multiplicity) for the single-product entry points.
 constexpr int kCompactThreads = 256;
 constexpr int kCompactPer = 4;
 constexpr int kCompactSpan = kCompactThreads * kCompactPer;
@@ -170,18 +152,13 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_c
   __shared__ uint32_t scan[40];
   const Buffers& b = a.b;
   const CallCfg& cc = a.cc;
-  int pb_out;
-  if (a.iter < 0) {
-    pb_out = 0;
-  } else {
-    const IterState& st = b.st[a.iter & 1];
-    const bool consumes = st.mode == kPrevious || st.mode == kProposed;
-    if (st.done || !consumes || a.iter + 1 >= cc.step) return;  // uniform over the grid
-    pb_out = st.pb ^ 1;
-  }
-  const int which = next_amm_weighting(cc, a.iter);
-  const uint32_t* __restrict__ cnt = b.count[pb_out];
-  const uint32_t* __restrict__ chunk = b.chunk[pb_out];
+  const IterState& st = b.st[a.iter & 1];
+  const int list = st.drawn + (int)blockIdx.y;
+  if (st.done || list >= window_end(cc, a.iter, st)) return;  // uniform over the CTA
+  const int slot = list % kListWindow;
+  const int which = list_weighting(cc, list);
+  const uint32_t* __restrict__ cnt = b.count[slot];
+  const uint32_t* __restrict__ chunk = b.chunk[slot];
   const int t = threadIdx.x;
   const int start = blockIdx.x * kCompactSpan;
   // picked columns below `start`: the whole chunks, then the columns of the chunk `start` is in
@@ -197,7 +174,7 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_c
     for (int k = t; k < b.nchunks; k += kCompactThreads) all += __ldg(chunk + k);
     uint32_t total;
     block_exclusive_scan(all, scan, &total);
-    if (t == 0) *b.wl_count[pb_out] = total;
+    if (t == 0) b.wl_count[slot] = total;
   }
   uint32_t mult[kCompactPer];
   uint32_t nz = 0;
@@ -211,9 +188,9 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_c
   uint32_t unused;
   uint32_t r = base + block_exclusive_scan(nz, scan, &unused);
   const float* __restrict__ wts = b.wts[which];
-  uint32_t* __restrict__ wl_col = b.wl_col[pb_out];
-  float* __restrict__ wl_wm = b.wl_wm[pb_out];
-  float* __restrict__ wl_al = b.wl_al[pb_out];
+  uint32_t* __restrict__ wl_col = b.wl_col[slot];
+  float* __restrict__ wl_wm = b.wl_wm[slot];
+  float* __restrict__ wl_al = b.wl_al[slot];
 #pragma unroll
   for (int e = 0; e < kCompactPer; ++e) {
     if (mult[e]) {
@@ -221,7 +198,7 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_c
       wl_col[r] = (uint32_t)j;
       wl_wm[r] = __fmul_rn(__ldg(wts + j), (float)mult[e]);
       wl_al[r] = __ldg(b.alpha + j);
-      if (a.iter < 0) {
+      if (list == 0) {
         b.distinct_idx[r] = (uint32_t)j;
         b.distinct_mult[r] = mult[e];
       }
@@ -280,8 +257,8 @@ __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ Init
     st.mode = decide_mode(cc, 0, 0.0, 0, &le);
     st.last_exact = le;
     st.done = 0;
-    st.sb = 0;
-    st.pb = 0;
+    st.used = 0;
+    st.drawn = 0;
     st.steps_run = 0;
     if (!(s > 0.0) || !isfinite(s)) {
       atomicOr(b.status, (uint32_t)kDevNonFinite);
@@ -313,13 +290,21 @@ __global__ void __launch_bounds__(kFinalThreads) finalize_kernel(const __grid_co
     if (a.ydst) a.ydst[k] = yv;
   }
   if (a.cc.uses_amm && !a.cc.sanity) {
-    if (st.sb == 1)
-      for (int k = gt; k < b.c; k += gs) b.states[0][k] = b.states[1][k];
-    // pending (speculative) picks are dropped: their states were never committed
-    uint32_t* cnt = b.count[st.pb];
-    const uint32_t* smp = b.samples[st.pb];
-    for (int k = gt; k < b.c; k += gs) cnt[smp[k]] = 0u;
-    for (int k = gt; k < b.nchunks; k += gs) b.chunk[st.pb][k] = 0u;
+    // commit: each state advanced once per AMM step that ran
+    if (st.used > 0)
+      for (int k = gt; k < b.c; k += gs) {
+        uint32_t y = b.states[0][k];
+        for (int r = 0; r < st.used; ++r) y = xorshift32(y);
+        b.states[0][k] = y;
+      }
+    // pending (drawn ahead, never consumed) lists are dropped: their states are not committed
+    for (int list = st.used; list < st.drawn; ++list) {
+      const int slot = list % kListWindow;
+      uint32_t* cnt = b.count[slot];
+      const uint32_t* smp = b.samples[slot];
+      for (int k = gt; k < b.c; k += gs) cnt[smp[k]] = 0u;
+      for (int k = gt; k < b.nchunks; k += gs) b.chunk[slot][k] = 0u;
+    }
   }
 }
 
@@ -666,10 +651,11 @@ cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStr
   a.iter = iter;
   int blocks = (b.c + 255) / 256;
   if (blocks > 1024) blocks = 1024;
+  const int rows = cc.step < kListWindow ? cc.step : kListWindow;
   if (b.cdf_f32)
-    sample_kernel<float><<<blocks, 256, 0, s>>>(a);
+    sample_kernel<float><<<dim3(blocks, rows), 256, 0, s>>>(a);
   else
-    sample_kernel<double><<<blocks, 256, 0, s>>>(a);
+    sample_kernel<double><<<dim3(blocks, rows), 256, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }
@@ -680,7 +666,8 @@ cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaSt
   a.cc = cc;
   a.iter = iter;
   const int blocks = (b.n + kCompactSpan - 1) / kCompactSpan;
-  compact_kernel<<<blocks, kCompactThreads, 0, s>>>(a);
+  const int rows = cc.step < kListWindow ? cc.step : kListWindow;
+  compact_kernel<<<dim3(blocks, rows), kCompactThreads, 0, s>>>(a);
   count_launch();
   return cudaGetLastError();
 }
@@ -695,6 +682,14 @@ cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, fl
   int blocks = (b.m + kFinalThreads - 1) / kFinalThreads;
   if (blocks > 256) blocks = 256;
   finalize_kernel<<<blocks, kFinalThreads, 0, s>>>(a);
+  count_launch();
+  return cudaGetLastError();
+}
+
+__global__ void clock_kernel(unsigned long long* out) { *out = globaltimer_ns(); }
+
+cudaError_t launch_clock(unsigned long long* out, cudaStream_t s) {
+  clock_kernel<<<1, 1, 0, s>>>(out);
   count_launch();
   return cudaGetLastError();
 }

@@ -5,17 +5,19 @@
 // for one power-method step (all n columns for an exact step, the distinct sampled columns for
 // an AMM step) and for the set-up pass (coef_j = α_j, plus FP64 column statistics).
 //
-// One persistent CTA per SM owns a contiguous range of the column list and all m rows.  A
-// producer warp streams the columns, GC per group, into a ring of NS shared-memory stages with
-// 1-D TMA bulk copies (mbarrier complete_tx; measured on B200: >= 64 KB in flight per SM
-// saturates HBM).  The consumer warps hold dx and their share of y in registers; per group they
+// One persistent CTA per SM owns a contiguous range of the column list and all m rows.  Thread 0
+// streams the columns, GC per group, into a ring of NS shared-memory stages with 1-D TMA bulk
+// copies (mbarrier complete_tx; measured on B200: >= 64 KB in flight per SM saturates HBM),
+// refilling a stage once every thread is past it.  All warps hold dx and their share of y in
+// registers; per group they
 //   1. form the coefficients of group g from the warp partials published at the last barrier,
 //   2. compute the partial dots of group g+1 (their rows),
 //   3. accumulate coef·A_k of group g into y (packed FP32x2 FMAs),
 //   4. warp-reduce and publish the dots of g+1, then meet at one named barrier,
 // so the reduction latency of a group hides behind the next group's math and there is one
 // barrier per group.  Each column is read from HBM once (the reference's kernel1/kernel2 read
-// it twice).  Each CTA writes one partial y; reduce_kernel sums them in a fixed order.
+// it twice).  Each CTA writes one partial y; after a grid barrier every CTA sums its rows of
+// the partials in a fixed order, and the last CTA to finish forms λ and the next step's state.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -253,26 +255,39 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   float* wl_al = reinterpret_cast<float*>(smem + L.wl_al);
   __shared__ IterState st_s;  // the step state, for the last CTA's epilogue
 
+  // A step grid is launched as a programmatic dependent of the grid before it: its CTAs start
+  // on the SMs that the previous step's CTAs leave (all but its last CTA retire after the row
+  // reduction), initialise their barriers, and wait for the previous grid to complete before
+  // touching global memory.  Every CTA of this grid is resident by the time it lets the next
+  // step's grid be scheduled (one CTA per SM), so the grid barrier below is unaffected.
+  if (!SETUP) griddep_launch_dependents();
   if (t == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     fence_barrier_init();
   }
   __syncthreads();  // barrier initialisation visible to every thread
+  if (!SETUP) griddep_wait();
 
   // The loads of the prologue are issued together, before anything depends on them: the step
-  // state, both work-list lengths (the pick buffer is known only with the state) and this
-  // thread's rows of y_{i-1} and x_memo.
-  int mode = kExact, pb = 0, done = 0;
+  // state, every work-list length (the slot is known only with the state) and this thread's
+  // rows of y_{i-1} and x_memo.
+  int mode = kExact, slot = 0, done = 0;
   float scale = 0.f;
-  uint32_t cd_buf[2] = {0u, 0u};
+  uint32_t cd_all[kListWindow];
   if (!SETUP) {
     const IterState& st = b.st[a.iter & 1];
     done = st.done;
     mode = st.mode;
-    pb = st.pb;
+    slot = st.used % kListWindow;
     scale = st.scale;
-    cd_buf[0] = __ldg(b.wl_count[0]);
-    cd_buf[1] = __ldg(b.wl_count[1]);
+#pragma unroll
+    for (int w = 0; w < kListWindow; w += 4) {
+      const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(b.wl_count + w));
+      cd_all[w] = c4.x;
+      cd_all[w + 1] = c4.y;
+      cd_all[w + 2] = c4.z;
+      cd_all[w + 3] = c4.w;
+    }
   }
   const bool amm = !SETUP && (mode == kPrevious || mode == kProposed);
   const bool centred = !SETUP && mode == kProposed;
@@ -284,7 +299,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     lo = (int64_t)q * b.n / G;
     hi = (int64_t)(q + 1) * b.n / G;
   } else {
-    const uint32_t cd = pb ? cd_buf[1] : cd_buf[0];
+    uint32_t cd = cd_all[0];
+#pragma unroll
+    for (int w = 1; w < kListWindow; ++w)
+      if (slot == w) cd = cd_all[w];
     lo = (int64_t)q * cd / G;
     hi = (int64_t)(q + 1) * cd / G;
     if (q == 0 && t == 0 && !done) b.distinct_hist[a.iter] = (int32_t)cd;
@@ -332,7 +350,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     uint32_t first[8 * 8];
     const int nf = min(NS * GC, nb);
     if (sampled)
-      for (int k = 0; k < nf; ++k) first[k] = __ldg(b.wl_col[pb] + lo + k);
+      for (int k = 0; k < nf; ++k) first[k] = __ldg(b.wl_col[slot] + lo + k);
     for (int grp = 0; grp < NS && grp < ngroups; ++grp) issue(grp, first);
   }
   if (!SETUP && t == 0) st_s = b.st[a.iter & 1];
@@ -368,9 +386,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     const int t1 = T > 32 ? t - 32 : t, T1 = T > 32 ? T - 32 : T;
     for (int k = t1; k >= 0 && k < nb; k += T1) {
       if (sampled) {
-        wl_idx[k] = __ldg(b.wl_col[pb] + lo + k);
-        wl_w[k] = __ldg(b.wl_wm[pb] + lo + k);
-        wl_al[k] = __ldg(b.wl_al[pb] + lo + k);
+        wl_idx[k] = __ldg(b.wl_col[slot] + lo + k);
+        wl_w[k] = __ldg(b.wl_wm[slot] + lo + k);
+        wl_al[k] = __ldg(b.wl_al[slot] + lo + k);
       } else {  // sanity mode: identity list, weight 1
         wl_w[k] = 1.0f;
         wl_al[k] = __ldg(b.alpha + lo + k);
@@ -625,12 +643,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   }
   if (sampled) {
     // The picks are consumed: their histogram entries and chunk totals are cleared for the
-    // next draw into this buffer (several CTAs may zero one chunk total: the same value).
+    // next draw into this slot (several CTAs may zero one chunk total: the same value).
     const int cs = b.chunk_shift;
+    uint32_t* cnt = b.count[slot];
+    uint32_t* chk = b.chunk[slot];
     for (int k = t; k < nb; k += T) {
       const uint32_t col = wl_idx[k];  // written before the barriers of the group loop
-      b.count[pb][col] = 0u;
-      b.chunk[pb][col >> cs] = 0u;
+      cnt[col] = 0u;
+      chk[col >> cs] = 0u;
     }
   }
   float* part = b.partials + (size_t)q * m;
@@ -957,9 +977,21 @@ static cudaError_t launch_panel(const PanelArgs& a, bool setup, cudaStream_t s) 
   int smem = 0;
   cudaError_t e = configure(a.g, setup, &fn, &smem);
   if (e != cudaSuccess) return e;
-  fn<<<a.g.nclusters, a.g.threads, smem, s>>>(a);
+  // step grids: programmatic dependent launch (AMM_PDL=0 turns it off, for comparison)
+  static const bool pdl = env_int("AMM_PDL", 1) != 0;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(a.g.nclusters);
+  cfg.blockDim = dim3(a.g.threads);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = (!setup && pdl) ? 1 : 0;
+  e = cudaLaunchKernelEx(&cfg, fn, a);
   count_launch();
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_setup_panel(const Buffers& b, const PanelGeom& g, cudaStream_t s) {

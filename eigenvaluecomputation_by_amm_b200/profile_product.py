@@ -58,6 +58,21 @@ def main():
             print(f"solve {a.solve} rep {rep}: {e0.elapsed_time(e1):.3f} ms, kinds {tr['kinds']}, "
                   f"distinct {tr['distinct'].tolist()}, step us (device clock) "
                   f"{np.round(steps_us, 1).tolist()}")
+        # device-clock timeline of one more solve: stamps before set_matrix, after it, and after
+        # the call, against the call's own stamps (end of its first kernel, end of each step)
+        ctx.set_rng_state(states)
+        stamps = torch.zeros(3, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        ctx.device_clock(stamps[0:1])
+        ctx.set_matrix(A)
+        ctx.device_clock(stamps[1:2])
+        ctx.power_method(a.solve, x0)
+        ctx.device_clock(stamps[2:3])
+        clk = ctx.step_clocks()
+        s0, s1, s2 = (int(v) for v in stamps.cpu())
+        print(f"timeline us: set_matrix (host, GPU idle) {(s1 - s0) / 1e3:.1f}; set-up + CDF + "
+              f"call start {(int(clk[0]) - s1) / 1e3:.1f}; steps {(int(clk[-1]) - int(clk[0])) / 1e3:.1f}; "
+              f"call end {(s2 - int(clk[-1])) / 1e3:.1f}; total {(s2 - s0) / 1e3:.1f}")
         ctx.close()
         return
     ctx = AMMContext(a.m, a.n, c=a.c, step=2, dtype=a.dtype)

@@ -293,6 +293,15 @@ int amm_benchmark_product(amm_ctx *ctx, int kind, int reps, float *ms_per_launch
 int amm_grad_lambda(amm_ctx *ctx, const float *d_v, float *d_grad, int64_t ld_grad,
                     void *stream);
 
+/* Profiling aids (no counterpart in the reference, which has no device timeline):
+ * amm_device_clock enqueues on `stream` a one-thread kernel that writes the device clock
+ * (%globaltimer, ns) to *d_out; amm_get_step_clocks synchronises `stream` and copies the raw
+ * device clock stamps of the last call to the HOST array out (cap >= steps_run + 1): [0] when
+ * the call's first kernel finished, [i + 1] when step i finished.  *count receives how many
+ * were written. */
+int amm_device_clock(uint64_t *d_out, void *stream);
+int amm_get_step_clocks(amm_ctx *ctx, uint64_t *out, int64_t cap, int64_t *count, void *stream);
+
 /* Launch geometry of the fused product kernel chosen for this context, 10 values:
  * {cluster size, rows per CTA, clusters, consumer threads, vector slots per thread,
  *  columns per stage, stages, stage bytes, shared memory bytes, work-list capacity}. */
