@@ -187,14 +187,15 @@ int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normal
   const Buffers& b = ctx->b;
   const bool draws = cc.uses_amm && !cc.sanity;
   AMM_CUDA(amm::launch_init(b, cc, x0, no_normalize, s));
-  for (int i = 0; i < cc.step; ++i) {
-    // the work lists of the next kListWindow AMM steps, drawn before the first of them: the
-    // step kernels then run back to back with nothing else on the SMs
-    if (draws && i % amm::kListWindow == 0) {
+  // One persistent step launch per window of kListWindow steps (the whole call when nothing
+  // is sampled), each preceded by the draw and compaction of the work lists of its AMM steps
+  const int seg = draws ? amm::kListWindow : (cc.step > 0 ? cc.step : 1);
+  for (int i = 0; i < cc.step; i += seg) {
+    if (draws) {
       AMM_CUDA(amm::launch_sample(b, cc, i, s));
       AMM_CUDA(amm::launch_compact(b, cc, i, s));
     }
-    AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, s));
+    AMM_CUDA(amm::launch_iter_panel(b, ctx->geom, cc, i, std::min(i + seg, cc.step), s));
   }
   AMM_CUDA(amm::launch_finalize(b, cc, ctx->x_final, ctx->y_final, s));
   return AMM_OK;
@@ -240,8 +241,9 @@ int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
     it = ctx->graphs.emplace(key, std::make_pair(g, ex)).first;
   }
   AMM_CUDA(cudaGraphLaunch(it->second.second, s));
-  const int refills = (cc.step + amm::kListWindow - 1) / amm::kListWindow;
-  amm::count_launch(2 + cc.step + ((cc.uses_amm && !cc.sanity) ? 2 * refills : 0));
+  const bool draws = cc.uses_amm && !cc.sanity;
+  const int segs = draws ? (cc.step + amm::kListWindow - 1) / amm::kListWindow : 1;
+  amm::count_launch(2 + (draws ? 3 : 1) * segs);
   return AMM_OK;
 }
 
@@ -831,7 +833,7 @@ int amm_benchmark_product(amm_ctx* ctx, int kind, int reps, float* ms_per_launch
   AMM_CUDA(cudaEventCreate(&e0));
   AMM_CUDA(cudaEventCreate(&e1));
   AMM_CUDA(cudaEventRecord(e0, s));
-  for (int r = 0; r < reps; ++r) AMM_CUDA(amm::launch_iter_panel(ctx->b, ctx->geom, cc, 0, s));
+  for (int r = 0; r < reps; ++r) AMM_CUDA(amm::launch_iter_panel(ctx->b, ctx->geom, cc, 0, 1, s));
   AMM_CUDA(cudaEventRecord(e1, s));
   // finalize with step 0 reads the call-start state st[0] (nothing used, nothing pending: the
   // one list drawn was consumed), so states[0] is kept

@@ -278,40 +278,51 @@ __host__ __device__ __forceinline__ int32_t window_end(const CallCfg& cc, int i,
 }
 
 // The step's scalars from the summed x·y, y·y and y·v* (dotProduct_and_generate_x,
-// common.h:103-153): λ = x·y, err = y·v*/‖y‖, cos = λ/‖y‖, the trace entries and the state of
-// the next step (its kind, the tolerance stop).  Run by one thread once the sums are final.
-__device__ __forceinline__ void finish_step(const Buffers& b, const CallCfg& cc, int i,
-                                            const IterState& st, double xy, double yy,
-                                            double yv) {
+// common.h:103-153): λ = x·y, err = y·v*/‖y‖, cos = λ/‖y‖, and the state of the next step (its
+// scale, its kind, the tolerance stop).  A pure function of its arguments: every CTA of the
+// step kernel evaluates it on the same sums and gets the same state.
+struct StepScalars {
+  double lam, err, cosv;
+  bool nonfinite;
+};
+
+__device__ __forceinline__ IterState next_state(const CallCfg& cc, int i, const IterState& st,
+                                                double xy, double yy, double yv,
+                                                StepScalars* sc) {
   const bool consumed = st.mode == kPrevious || st.mode == kProposed;
   const double scale = rsqrt(yy);
   const double lam = xy;
-  const double err = yv * scale;
-  const double cosv = lam * scale;
-  b.eigs[i] = lam;
-  b.errs[i] = err;
-  b.coss[i] = cosv;
-  b.kinds[i] = st.mode;
-  if (!consumed || cc.sanity) b.distinct_hist[i] = b.n;
-  b.tstamp[i + 1] = globaltimer_now();
+  sc->lam = lam;
+  sc->err = yv * scale;
+  sc->cosv = lam * scale;
   IterState nx = st;
   nx.scale = (float)scale;
-  nx.cos_prev = cosv;
+  nx.cos_prev = sc->cosv;
   nx.lam_prev = lam;
   nx.steps_run = i + 1;
   if (consumed && !cc.sanity) nx.used = st.used + 1;
   if (cc.uses_amm && !cc.sanity && i % kListWindow == 0) nx.drawn = window_end(cc, i, st);
-  bool done = false;
-  if (!isfinite(lam) || !isfinite(scale)) {
-    atomicOr(b.status, (uint32_t)kDevNonFinite);
-    done = true;
-  }
+  sc->nonfinite = !isfinite(lam) || !isfinite(scale);
+  bool done = sc->nonfinite;
   if (cc.tol > 0.0 && i >= 1 && fabs(lam - st.lam_prev) <= cc.tol * fabs(lam)) done = true;
   nx.done = done ? 1 : 0;
   int le;
-  nx.mode = decide_mode(cc, i + 1, cosv, st.last_exact, &le);
+  nx.mode = decide_mode(cc, i + 1, sc->cosv, st.last_exact, &le);
   nx.last_exact = le;
-  b.st[(i + 1) & 1] = nx;
+  return nx;
+}
+
+// The trace entries of step i (one thread of the grid).
+__device__ __forceinline__ void record_step(const Buffers& b, const CallCfg& cc, int i,
+                                            const IterState& st, const StepScalars& sc) {
+  const bool consumed = st.mode == kPrevious || st.mode == kProposed;
+  b.eigs[i] = sc.lam;
+  b.errs[i] = sc.err;
+  b.coss[i] = sc.cosv;
+  b.kinds[i] = st.mode;
+  if (!consumed || cc.sanity) b.distinct_hist[i] = b.n;
+  b.tstamp[i + 1] = globaltimer_now();
+  if (sc.nonfinite) atomicOr(b.status, (uint32_t)kDevNonFinite);
 }
 
 // ---- programmatic dependent launch (a grid launched with programmatic stream serialization

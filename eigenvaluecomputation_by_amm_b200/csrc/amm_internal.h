@@ -23,8 +23,9 @@ constexpr int kCoarseMax = 2048;   // coarse CDF table entries held in shared me
 // call (its a-th AMM step) lives in slot a % kListWindow.
 constexpr int kListWindow = 8;
 
-// Iteration state, double-buffered by iteration parity: kernels of iteration i read
-// st[i & 1]; the last CTA of the step kernel of iteration i writes st[(i + 1) & 1].
+// Iteration state, by iteration parity: a launch of the step kernel covering steps [i0, i1)
+// reads st[i0 & 1] and leaves the state after its last step in st[i1 & 1] (the sampler's refill
+// ahead of step i reads st[i & 1]); inside the launch every CTA keeps its own copy.
 struct IterState {
   int32_t mode;        // StepKind of this iteration
   int32_t last_exact;  // proposed AMM: index of the last VR step
@@ -156,10 +157,11 @@ cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStr
 int record_cuda_failure(cudaError_t e, const char* what);
 // Build the sorted distinct work lists of the picks just drawn (same decision as sample_kernel).
 cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s);
-// One step (amm_panel.cu): the product, the grid-wide reduction of the partials into y, the
-// Rayleigh quotient and the next step's state.
+// Steps [iter, iter_end) of a call in one persistent launch (amm_panel.cu): per step the
+// product, the grid-wide reduction of the partials into y, the Rayleigh quotient and the next
+// step's state.
 cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
-                              cudaStream_t s);
+                              int iter_end, cudaStream_t s);
 // x_final = scale * y_last into dst (length m); y_last into ydst (optional); commits the
 // sampling states to states[0] and clears any pending picks.
 cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, float* ydst,

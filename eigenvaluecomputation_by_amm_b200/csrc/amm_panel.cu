@@ -33,7 +33,8 @@ struct PanelArgs {
   Buffers b;
   PanelGeom g;
   CallCfg cc;
-  int iter;
+  int iter;      // first step of the launch
+  int iter_end;  // steps [iter, iter_end) run in this launch (the set-up pass: one pass)
 };
 
 template <bool SETUP>
@@ -58,7 +59,7 @@ __device__ __forceinline__ double2 warp_red(double2 v) {
 
 // Shared memory carve (byte offsets), identical on host and device.
 struct SmemLayout {
-  int stages, bars, redw, wl_idx, wl_w, wl_al, total;
+  int stages, bars, redw, wl_idx, wl_w, wl_al, nxt, red, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup) {
@@ -79,6 +80,11 @@ __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup
   o += 4 * g.wl_cap;
   L.wl_al = o;
   o += 4 * g.wl_cap;
+  o = (o + 127) & ~127;
+  L.nxt = o;  // first column indices of the next step's list: [kGcMax * 8]
+  o += 4 * kGcMax * 8;
+  L.red = o;  // row-reduction scratch: [16 warps][32] double4
+  o += 16 * 32 * 32;
   L.total = (o + 127) & ~127;
   return L;
 }
@@ -234,6 +240,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   constexpr int H = E / 2;  // float2 per vector
   const Buffers& b = a.b;
   const PanelGeom& g = a.g;
+  const CallCfg& cc = a.cc;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int T = blockDim.x;  // threads: all consume; thread 0 also issues the copies
   const int ncw = T >> 5;    // warps
@@ -244,6 +251,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   const int nvec = m / E;
   const int NS = g.nstages;
   const uint32_t col_bytes = (uint32_t)(m * sizeof(Elem));
+  const bool full_slots = (T * R == nvec);  // every vector slot of every thread is a real row
 
   extern __shared__ __align__(128) unsigned char smem[];
   const SmemLayout L = smem_layout(g, SETUP);
@@ -253,13 +261,20 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   uint32_t* wl_idx = reinterpret_cast<uint32_t*>(smem + L.wl_idx);
   float* wl_w = reinterpret_cast<float*>(smem + L.wl_w);
   float* wl_al = reinterpret_cast<float*>(smem + L.wl_al);
-  __shared__ IterState st_s;  // the step state, for the last CTA's epilogue
+  uint32_t* nxt_cols = reinterpret_cast<uint32_t*>(smem + L.nxt);  // [kGcMax * 8]
+  double4* red = reinterpret_cast<double4*>(smem + L.red);          // [16 warps][32]
+  __shared__ IterState st_s;   // state of the current step, identical in every CTA
+  __shared__ int32_t pre_s[2];  // groups of the current step issued ahead, and their list key
+  __shared__ uint32_t cd_s[kListWindow];  // work-list lengths of the slots (fixed per launch)
+  __shared__ int32_t nx_s[4];   // predicted next list: groups to issue ahead, key, length, sampled
+  __shared__ int64_t nxlo_s;    // ... and its first index
+  __shared__ uint32_t iss_s;    // groups issued so far (thread 0)
 
-  // A step grid is launched as a programmatic dependent of the grid before it: its CTAs start
-  // on the SMs that the previous step's CTAs leave (all but its last CTA retire after the row
-  // reduction), initialise their barriers, and wait for the previous grid to complete before
-  // touching global memory.  Every CTA of this grid is resident by the time it lets the next
-  // step's grid be scheduled (one CTA per SM), so the grid barrier below is unaffected.
+  // A launch of the step kernel is a programmatic dependent of the grid before it: its CTAs
+  // start on the SMs that the previous grid leaves, initialise their barriers, and wait for
+  // that grid to complete before touching global memory.  Every CTA of this grid is resident
+  // by the time it lets the next grid be scheduled (one CTA per SM), so the grid barriers
+  // below are unaffected.
   if (!SETUP) griddep_launch_dependents();
   if (t == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
@@ -268,615 +283,717 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   __syncthreads();  // barrier initialisation visible to every thread
   if (!SETUP) griddep_wait();
 
-  // The loads of the prologue are issued together, before anything depends on them: the step
-  // state, every work-list length (the slot is known only with the state) and this thread's
-  // rows of y_{i-1} and x_memo.
-  int mode = kExact, slot = 0, done = 0;
-  float scale = 0.f;
-  uint32_t cd_all[kListWindow];
+  // work-list lengths of every slot (fixed for the launch: the window is refilled between
+  // launches) and the state of the launch's first step; loop-carried values live in shared
+  // memory, so that the group loop keeps its registers
   if (!SETUP) {
-    const IterState& st = b.st[a.iter & 1];
-    done = st.done;
-    mode = st.mode;
-    slot = st.used % kListWindow;
-    scale = st.scale;
-#pragma unroll
-    for (int w = 0; w < kListWindow; w += 4) {
-      const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(b.wl_count + w));
-      cd_all[w] = c4.x;
-      cd_all[w + 1] = c4.y;
-      cd_all[w + 2] = c4.z;
-      cd_all[w + 3] = c4.w;
+    if (t < kListWindow) cd_s[t] = __ldg(b.wl_count + t);
+    if (t == 0) {
+      st_s = b.st[a.iter & 1];
+      pre_s[0] = 0;
+      pre_s[1] = -2;
     }
   }
-  const bool amm = !SETUP && (mode == kPrevious || mode == kProposed);
-  const bool centred = !SETUP && mode == kProposed;
-  const bool sampled = amm && !a.cc.sanity;
+  if (t == 0) iss_s = 0u;
 
-  // ---- this CTA's column list: a contiguous slice of the sorted work list ------------------
-  int64_t lo, hi;
-  if (!sampled) {
-    lo = (int64_t)q * b.n / G;
-    hi = (int64_t)(q + 1) * b.n / G;
-  } else {
-    uint32_t cd = cd_all[0];
-#pragma unroll
-    for (int w = 1; w < kListWindow; ++w)
-      if (slot == w) cd = cd_all[w];
-    lo = (int64_t)q * cd / G;
-    hi = (int64_t)(q + 1) * cd / G;
-    if (q == 0 && t == 0 && !done) b.distinct_hist[a.iter] = (int32_t)cd;
-  }
-  const int nb = (int)(hi - lo);
-  const int ngroups = (nb + GC - 1) / GC;
+  // this CTA's slice [lo, hi) of the column list of a step reading `cd` sampled columns
+  // (sampled) or all n columns
+  auto slice = [&](bool smp, uint32_t cd, int64_t& lo, int64_t& hi) {
+    const int64_t total = smp ? (int64_t)cd : (int64_t)b.n;
+    lo = (int64_t)q * total / G;
+    hi = (int64_t)(q + 1) * total / G;
+  };
 
-  // Stage s of group grp is refilled by thread 0 once every thread is past the group that
-  // last used it (the CTA barrier at the end of each group): there is no producer warp.
+  // Stage ring: group number `pos` (counted over the whole launch) lives in stage pos % NS and
+  // completes phase (pos / NS) of that stage's barrier.  Thread 0 issues; a stage is refilled
+  // once every thread is past the group that last used it (the CTA barrier ending each group).
   const uint64_t policy = l2_evict_first_policy();
   const size_t col_stride = (size_t)b.ld * sizeof(Elem);
   const unsigned char* Abase = reinterpret_cast<const unsigned char*>(b.A);
-  auto issue = [&](int grp, const uint32_t* cols) {
-    const int s = grp % NS;
-    const int c0 = grp * GC;
-    const int cnt = min(GC, nb - c0);
+  auto issue_at = [&](uint32_t pos, int cnt, const uint32_t* cols, int64_t first_col) {
+    const int s = (int)(pos % (uint32_t)NS);
     mbar_arrive_expect_tx(&full[s], (uint32_t)cnt * col_bytes);
     for (int qq = 0; qq < cnt; ++qq) {
-      const uint32_t col = sampled ? cols[c0 + qq] : (uint32_t)(lo + c0 + qq);
+      const uint32_t col = cols ? cols[qq] : (uint32_t)(first_col + qq);
       bulk_g2s(stages + ((size_t)s * GC + qq) * col_bytes, Abase + (size_t)col * col_stride,
                col_bytes, &full[s], policy);
     }
   };
-
-  // ---- dx = x_i − x_memo on this thread's rows, x_i = scale·y_{i−1} (FP32 multiply) ----
-  // The loads are issued before the first copies, the arithmetic after them.
-  float4 ypv[R][E / 4], xmv[R][E / 4];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int vi = t + r * T;
-#pragma unroll
-    for (int h4 = 0; h4 < E / 4; ++h4) {
-      ypv[r][h4] = make_float4(0.f, 0.f, 0.f, 0.f);
-      xmv[r][h4] = ypv[r][h4];
-      if (!SETUP && vi < nvec) {
-        const int o4 = vi * (E / 4) + h4;
-        ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(a.iter + 1) & 1]) + o4);
-        // x_memo is read only by calls that draw samples (it is zero for exact steps, whose
-        // kind is not known before the state arrives)
-        if (a.cc.uses_amm) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
-      }
-    }
-  }
-  if (t == 0 && !done && ngroups > 0) {  // the first NS groups
-    uint32_t first[8 * 8];
-    const int nf = min(NS * GC, nb);
-    if (sampled)
-      for (int k = 0; k < nf; ++k) first[k] = __ldg(b.wl_col[slot] + lo + k);
-    for (int grp = 0; grp < NS && grp < ngroups; ++grp) issue(grp, first);
-  }
-  if (!SETUP && t == 0) st_s = b.st[a.iter & 1];
-  float2 dx[R][H];
-  float2 yacc[R][H];
-  double sum_dx = 0.0, zdx = 0.0;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-#pragma unroll
-    for (int h4 = 0; h4 < E / 4; ++h4) {
-      const float4 yp = ypv[r][h4];
-      const float4 xm = amm ? xmv[r][h4] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float d0 = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
-      const float d1 = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
-      const float d2 = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
-      const float d3 = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
-      dx[r][2 * h4] = make_float2(d0, d1);
-      dx[r][2 * h4 + 1] = make_float2(d2, d3);
-      if (centred) sum_dx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int h = 0; h < H; ++h) yacc[r][h] = make_float2(0.f, 0.f);
-  if (done) {  // uniform over the grid: the state passes on unchanged
-    if (q == 0 && t == 0) b.st[(a.iter + 1) & 1] = b.st[a.iter & 1];
-    return;
-  }
-  if (amm) {
-    // coefficient data of the slice, loaded by the warps after warp 0 (whose thread 0 issues
-    // the copies); published by the CTA barrier ahead of the first group
-    const int t1 = T > 32 ? t - 32 : t, T1 = T > 32 ? T - 32 : T;
-    for (int k = t1; k >= 0 && k < nb; k += T1) {
-      if (sampled) {
-        wl_idx[k] = __ldg(b.wl_col[slot] + lo + k);
-        wl_w[k] = __ldg(b.wl_wm[slot] + lo + k);
-        wl_al[k] = __ldg(b.wl_al[slot] + lo + k);
-      } else {  // sanity mode: identity list, weight 1
-        wl_w[k] = 1.0f;
-        wl_al[k] = __ldg(b.alpha + lo + k);
-      }
-    }
-  }
-  if (centred) {  // Σdx over all m rows (dots, common.h:55-87), identical in every CTA
-    sum_dx = warp_sum(sum_dx);
-    double* wtmp = reinterpret_cast<double*>(redw);
-    if (lane == 0) wtmp[warp] = sum_dx;
-    named_barrier_or(1, T, false);
-    sum_dx = 0.0;
-    for (int w = 0; w < ncw; ++w) sum_dx += wtmp[w];
-    named_barrier_or(1, T, false);  // wtmp (= redw) is reused below
-  }
-  const float sum_dx_f = (float)sum_dx;
-
-  // partial dots of group grp over this thread's rows, warp-reduced into redw[grp & 1]
-  auto wait_group = [&](int grp) -> bool {
-    return mbar_wait_bounded(&full[grp % NS], (uint32_t)((grp / NS) & 1));
+  auto wait_pos = [&](uint32_t pos) -> bool {
+    return mbar_wait_bounded(&full[pos % (uint32_t)NS], (pos / (uint32_t)NS) & 1u);
   };
-  // guarded partial dots of group grp (tail groups, partial slots, the set-up statistics)
-  auto dot_group = [&](int grp, RT (&d)[GC], bool got) -> bool {
-    const int s = grp % NS;
-    const int cnt = got ? min(GC, nb - grp * GC) : 0;
-    const unsigned char* sb = stages + (size_t)s * GC * col_bytes;
-#pragma unroll
-    for (int qq = 0; qq < GC; ++qq) {
-      if constexpr (SETUP) {
-        d[qq] = make_double2(0.0, 0.0);
-      } else {
-        d[qq] = 0.f;
-      }
-      if (qq < cnt) {
-        const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
-        if constexpr (SETUP) {
-          // FP32 partial sums over this thread's vectors, folded into FP64 once (as
-          // fused_block_setup)
-          float2 s2 = make_float2(0.f, 0.f), q2 = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const int vi = t + r * T;
-            if (vi < nvec) {
-              float2 av[H];
-              unpack2(col[vi], av);
-#pragma unroll
-              for (int h = 0; h < H; ++h) {
-                s2 = __fadd2_rn(s2, av[h]);
-                q2 = fma2(av[h], av[h], q2);
-              }
-            }
-          }
-          d[qq] = make_double2((double)s2.x + (double)s2.y, (double)q2.x + (double)q2.y);
-        } else {
-          float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const int vi = t + r * T;
-            if (vi < nvec) {
-              float2 av[H];
-              unpack2(col[vi], av);
-#pragma unroll
-              for (int h = 0; h < H; h += 2) {
-                p0 = fma2(av[h], dx[r][h], p0);
-                if (h + 1 < H) p1 = fma2(av[h + 1], dx[r][h + 1], p1);
-              }
-            }
-          }
-          d[qq] = (p0.x + p0.y) + (p1.x + p1.y);
-        }
-      }
-    }
-    return got;
-  };
-  auto publish = [&](int grp, RT (&d)[GC]) {
-    const int cnt = min(GC, nb - grp * GC);
-    RT* slot = redw + ((grp & 1) * 16 + warp) * GC;
-    if constexpr (!SETUP && GC >= 2) {
-      float v[GC];
-#pragma unroll
-      for (int qq = 0; qq < GC; ++qq) v[qq] = d[qq];
-      const float r = warp_reduce_multi<float, GC>(v, lane);
-      constexpr int L = 32 / GC;
-      const int q = lane / L;
-      if (lane % L == 0 && q < cnt) slot[q] = r;
-    } else if constexpr (SETUP && 2 * GC <= 32) {
-      double v[2 * GC];
-#pragma unroll
-      for (int qq = 0; qq < GC; ++qq) {
-        v[2 * qq] = d[qq].x;
-        v[2 * qq + 1] = d[qq].y;
-      }
-      const double r = warp_reduce_multi<double, 2 * GC>(v, lane);
-      constexpr int L = 32 / (2 * GC);
-      const int idx = lane / L;
-      if (lane % L == 0 && (idx >> 1) < cnt) {
-        double* sd = reinterpret_cast<double*>(slot);
-        sd[idx] = r;  // (Σa, Σa²) of column idx/2
-      }
-    } else {
-#pragma unroll
-      for (int qq = 0; qq < GC; ++qq) {
-        if (qq < cnt) {
-          const RT v = warp_red(d[qq]);
-          if (lane == 0) slot[qq] = v;
-        }
-      }
-    }
-  };
-
-  float sacc = 0.f;    // Σ α_k t_k (proposed)
-  double a2acc = 0.0;  // Σ α_j² (set-up)
+  uint32_t gbase = 0;   // groups through the ring before the current step (every thread)
   bool ok = true;
-  const bool full_slots = (T * R == nvec);  // every vector slot of every thread is a real row
-  RT dn[GC];
-  if (ngroups > 0) {
-    ok = wait_group(0);
-    dot_group(0, dn, ok);
-    publish(0, dn);
-  }
-  if (named_barrier_or(1, T, !ok)) ok = false;
-  for (int grp = 0; ok && grp < ngroups; ++grp) {
-    const int cnt = min(GC, nb - grp * GC);
-    // coefficients of this group (every thread sums the warp partials in the same order)
-    float coef[GC];
-    const RT* rs = redw + (grp & 1) * 16 * GC;
-    float tots[GC];
-    double sxy[2 * GC];
-    if constexpr (SETUP) {
-      const double* rsd = reinterpret_cast<const double*>(rs);
-      if (ncw == 16) {
-        warp_partials_sum<double, 2 * GC>(rsd, 2 * GC, lane, sxy);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 2 * GC; ++i) {
-          double tt = rsd[i];
-          for (int w = 1; w < ncw; ++w) tt += rsd[w * 2 * GC + i];
-          sxy[i] = tt;
+  // on the way out: no copy may still be landing in this CTA's shared memory (the last NS
+  // issued groups cover every stage; waits are bounded)
+  auto drain = [&]() {
+    if (t == 0) {
+      const uint32_t issued = iss_s;
+      for (uint32_t p = issued > (uint32_t)NS ? issued - (uint32_t)NS : 0u; p < issued; ++p)
+        wait_pos(p);
+    }
+  };
+
+  for (int i = a.iter;; ++i) {
+    int mode = kExact, slot = 0;
+    float scale = 0.f;
+    if (!SETUP) {
+      __syncthreads();  // st_s and pre_s of this step; every thread is done with the last one
+      if (i >= a.iter_end || st_s.done) break;  // uniform over the grid
+      mode = st_s.mode;
+      slot = st_s.used % kListWindow;
+      scale = st_s.scale;
+    }
+    const bool amm = !SETUP && (mode == kPrevious || mode == kProposed);
+    const bool centred = !SETUP && mode == kProposed;
+    const bool sampled = amm && !cc.sanity;
+    const int key = sampled ? slot : -1;  // which columns the step reads
+
+    // ---- this CTA's column list: a contiguous slice of the sorted work list ----------------
+    const uint32_t cd = SETUP ? 0u : cd_s[slot];
+    int64_t lo, hi;
+    slice(sampled, cd, lo, hi);
+    if (sampled && q == 0 && t == 0) b.distinct_hist[i] = (int32_t)cd;
+    const int nb = (int)(hi - lo);
+    const int ngroups = (nb + GC - 1) / GC;
+    const uint32_t* list_col = sampled ? b.wl_col[slot] + lo : nullptr;
+
+    // the groups of this step already in flight (issued at the end of the previous step on
+    // the predicted list); a misprediction is drained and the ring position moves past it
+    int pre = 0;
+    if (!SETUP) {
+      const int pn = pre_s[0];
+      if (pn > 0) {
+        if (pre_s[1] == key) {
+          pre = pn;
+        } else {
+          if (t == 0)
+            for (int k = 0; k < pn; ++k) wait_pos(gbase + (uint32_t)k);
+          gbase += (uint32_t)pn;
         }
       }
-    } else {
-      if (ncw == 16) {
-        warp_partials_sum<float, GC>(reinterpret_cast<const float*>(rs), GC, lane, tots);
+    }
+
+    // ---- dx = x_i − x_memo on this thread's rows, x_i = scale·y_{i−1} (FP32 multiply) ----
+    // The loads are issued before the first copies, the arithmetic after them.
+    float4 ypv[R][E / 4], xmv[R][E / 4];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int vi = t + r * T;
+#pragma unroll
+      for (int h4 = 0; h4 < E / 4; ++h4) {
+        ypv[r][h4] = make_float4(0.f, 0.f, 0.f, 0.f);
+        xmv[r][h4] = ypv[r][h4];
+        if (!SETUP && vi < nvec) {
+          const int o4 = vi * (E / 4) + h4;
+          ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(i + 1) & 1]) + o4);
+          if (amm) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
+        }
+      }
+    }
+    if (t == 0 && ngroups > pre) {  // the first NS groups not already in flight
+      uint32_t first[kGcMax * 8];
+      const int nf = min(NS * GC, nb);
+      if (sampled)
+        for (int k = pre * GC; k < nf; ++k) first[k] = __ldg(list_col + k);
+      for (int grp = pre; grp < NS && grp < ngroups; ++grp)
+        issue_at(gbase + (uint32_t)grp, min(GC, nb - grp * GC), sampled ? first + grp * GC : nullptr,
+                 lo + grp * GC);
+      iss_s = gbase + (uint32_t)min(NS, ngroups);
+    }
+
+    // The next step's list, predicted from this step's state (exact unless the adaptive VR
+    // switch, which needs this step's cosine, changes the kind): its first column indices are
+    // staged in shared memory now, and thread 0 issues its first groups as soon as this step's
+    // last group is consumed, so HBM stays busy through the grid-wide epilogue.
+    // (one warp: the warp after thread 0's, or warp 0 alone in a one-warp CTA)
+    if (!SETUP && warp == (ncw > 1 ? 1 : 0)) {
+      int groups = 0, nkey = -2, nnb = 0, nsmp = 0;
+      int64_t nlo = 0;
+      if (i + 1 < a.iter_end) {
+        int le;
+        const int nmode = decide_mode(cc, i + 1, st_s.cos_prev, st_s.last_exact, &le);
+        const int nslot = (st_s.used + (sampled ? 1 : 0)) % kListWindow;
+        nsmp = ((nmode == kPrevious || nmode == kProposed) && !cc.sanity) ? 1 : 0;
+        int64_t nhi;
+        slice(nsmp != 0, cd_s[nslot], nlo, nhi);
+        nnb = (int)(nhi - nlo);
+        groups = min(NS, (nnb + GC - 1) / GC);
+        nkey = nsmp ? nslot : -1;
+        if (nsmp) {
+          const int nf = min(NS * GC, nnb);
+          for (int k = lane; k < nf; k += 32) nxt_cols[k] = __ldg(b.wl_col[nslot] + nlo + k);
+        }
+      }
+      if (lane == 0) {
+        nx_s[0] = groups;
+        nx_s[1] = nkey;
+        nx_s[2] = nnb;
+        nx_s[3] = nsmp;
+        nxlo_s = nlo;
+      }
+    }
+
+    float2 dx[R][H];
+    float2 yacc[R][H];
+    double sum_dx = 0.0, zdx = 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int h4 = 0; h4 < E / 4; ++h4) {
+        const float4 yp = ypv[r][h4];
+        const float4 xm = amm ? xmv[r][h4] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float d0 = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
+        const float d1 = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
+        const float d2 = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
+        const float d3 = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
+        dx[r][2 * h4] = make_float2(d0, d1);
+        dx[r][2 * h4 + 1] = make_float2(d2, d3);
+        if (centred) sum_dx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int h = 0; h < H; ++h) yacc[r][h] = make_float2(0.f, 0.f);
+    if (amm) {
+      // coefficient data of the slice, loaded by the warps after warp 0 (whose thread 0 issues
+      // the copies); published by the CTA barrier ahead of the first group
+      const int t1 = T > 32 ? t - 32 : t, T1 = T > 32 ? T - 32 : T;
+      for (int k = t1; k >= 0 && k < nb; k += T1) {
+        if (sampled) {
+          wl_idx[k] = __ldg(list_col + k);
+          wl_w[k] = __ldg(b.wl_wm[slot] + lo + k);
+          wl_al[k] = __ldg(b.wl_al[slot] + lo + k);
+        } else {  // sanity mode: identity list, weight 1
+          wl_w[k] = 1.0f;
+          wl_al[k] = __ldg(b.alpha + lo + k);
+        }
+      }
+    }
+    if (centred) {  // Σdx over all m rows (dots, common.h:55-87), identical in every CTA
+      sum_dx = warp_sum(sum_dx);
+      double* wtmp = reinterpret_cast<double*>(redw);
+      if (lane == 0) wtmp[warp] = sum_dx;
+      named_barrier_or(1, T, false);
+      sum_dx = 0.0;
+      for (int w = 0; w < ncw; ++w) sum_dx += wtmp[w];
+      named_barrier_or(1, T, false);  // wtmp (= redw) is reused below
+    }
+    const float sum_dx_f = (float)sum_dx;
+
+    // ring slot (stage, phase parity) of group 0 of this step; the group loop advances it
+    const uint32_t stage_bytes = (uint32_t)GC * col_bytes;
+    int s_cur = (int)(gbase % (uint32_t)NS);
+    uint32_t ph_cur = (gbase / (uint32_t)NS) & 1u;
+    // guarded partial dots of the group in stage s (tail groups, partial slots, the set-up
+    // statistics)
+    auto dot_group = [&](int grp, int s, RT (&d)[GC], bool got) -> bool {
+      const int cnt = got ? min(GC, nb - grp * GC) : 0;
+      const unsigned char* sb = stages + (size_t)s * stage_bytes;
+#pragma unroll
+      for (int qq = 0; qq < GC; ++qq) {
+        if constexpr (SETUP) {
+          d[qq] = make_double2(0.0, 0.0);
+        } else {
+          d[qq] = 0.f;
+        }
+        if (qq < cnt) {
+          const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
+          if constexpr (SETUP) {
+            // FP32 partial sums over this thread's vectors, folded into FP64 once (as
+            // fused_block_setup)
+            float2 s2 = make_float2(0.f, 0.f), q2 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int vi = t + r * T;
+              if (vi < nvec) {
+                float2 av[H];
+                unpack2(col[vi], av);
+#pragma unroll
+                for (int h = 0; h < H; ++h) {
+                  s2 = __fadd2_rn(s2, av[h]);
+                  q2 = fma2(av[h], av[h], q2);
+                }
+              }
+            }
+            d[qq] = make_double2((double)s2.x + (double)s2.y, (double)q2.x + (double)q2.y);
+          } else {
+            float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int vi = t + r * T;
+              if (vi < nvec) {
+                float2 av[H];
+                unpack2(col[vi], av);
+#pragma unroll
+                for (int h = 0; h < H; h += 2) {
+                  p0 = fma2(av[h], dx[r][h], p0);
+                  if (h + 1 < H) p1 = fma2(av[h + 1], dx[r][h + 1], p1);
+                }
+              }
+            }
+            d[qq] = (p0.x + p0.y) + (p1.x + p1.y);
+          }
+        }
+      }
+      return got;
+    };
+    auto publish = [&](int grp, RT (&d)[GC]) {
+      const int cnt = min(GC, nb - grp * GC);
+      RT* slotp = redw + ((grp & 1) * 16 + warp) * GC;
+      if constexpr (!SETUP && GC >= 2) {
+        float v[GC];
+#pragma unroll
+        for (int qq = 0; qq < GC; ++qq) v[qq] = d[qq];
+        const float r = warp_reduce_multi<float, GC>(v, lane);
+        constexpr int LL = 32 / GC;
+        const int qv = lane / LL;
+        if (lane % LL == 0 && qv < cnt) slotp[qv] = r;
+      } else if constexpr (SETUP && 2 * GC <= 32) {
+        double v[2 * GC];
+#pragma unroll
+        for (int qq = 0; qq < GC; ++qq) {
+          v[2 * qq] = d[qq].x;
+          v[2 * qq + 1] = d[qq].y;
+        }
+        const double r = warp_reduce_multi<double, 2 * GC>(v, lane);
+        constexpr int LL = 32 / (2 * GC);
+        const int idx = lane / LL;
+        if (lane % LL == 0 && (idx >> 1) < cnt) {
+          double* sd = reinterpret_cast<double*>(slotp);
+          sd[idx] = r;  // (Σa, Σa²) of column idx/2
+        }
       } else {
 #pragma unroll
         for (int qq = 0; qq < GC; ++qq) {
-          float tt = rs[qq];
-          for (int w = 1; w < ncw; ++w) tt += rs[w * GC + qq];
-          tots[qq] = tt;
-        }
-      }
-    }
-#pragma unroll
-    for (int qq = 0; qq < GC; ++qq) {
-      coef[qq] = 0.f;
-      if (qq < cnt) {
-        const int k = grp * GC + qq;
-        if constexpr (SETUP) {
-          // α_j = Σa·(1/m) (exactly Σa/m for a power-of-two m); the sums go to colsum and the
-          // column statistics are formed in the epilogue, off this per-group path
-          const double sx = sxy[2 * qq];
-          const float af = (float)(sx * inv_m);
-          coef[qq] = af;
-          a2acc = fma((double)af, (double)af, a2acc);
-          if (t == qq) b.colsum[lo + k] = make_double2(sx, sxy[2 * qq + 1]);
-        } else {
-          const float tot = tots[qq];
-          if (!amm) {
-            coef[qq] = tot;
-          } else if (centred) {
-            const float al = wl_al[k];
-            const float tq = __fmul_rn(__fsub_rn(tot, __fmul_rn(al, sum_dx_f)), wl_w[k]);
-            coef[qq] = tq;
-            sacc = fmaf(al, tq, sacc);
-          } else {
-            coef[qq] = __fmul_rn(tot, wl_w[k]);
+          if (qq < cnt) {
+            const RT v = warp_red(d[qq]);
+            if (lane == 0) slotp[qq] = v;
           }
         }
       }
+    };
+
+    float sacc = 0.f;    // Σ α_k t_k (proposed)
+    double a2acc = 0.0;  // Σ α_j² (set-up)
+    RT dn[GC];
+    if (ngroups > 0) {
+      ok = mbar_wait_bounded(&full[s_cur], ph_cur);
+      dot_group(0, s_cur, dn, ok);
+      publish(0, dn);
     }
-    const bool more = grp + 1 < ngroups;
-    const int cnt_n = more ? min(GC, nb - (grp + 1) * GC) : 0;
-    bool got = true;
-    if (more) got = wait_group(grp + 1);
-    ok = ok && got;
-    const int s = grp % NS;
-    const unsigned char* sb = stages + (size_t)s * GC * col_bytes;
-    bool fused = false;
-    if (full_slots && cnt == GC && got) {
-      const unsigned char* sn = stages + (size_t)((grp + 1) % NS) * GC * col_bytes;
+    if (named_barrier_or(1, T, !ok)) ok = false;
+    for (int grp = 0; ok && grp < ngroups; ++grp) {
+      const int cnt = min(GC, nb - grp * GC);
+      // coefficients of this group (every thread sums the warp partials in the same order)
+      float coef[GC];
+      const RT* rs = redw + (grp & 1) * 16 * GC;
+      float tots[GC];
+      double sxy[2 * GC];
       if constexpr (SETUP) {
-        if (more && cnt_n == GC) {
-          if (T == 512)
-            fused_block_setup<Elem, R, GC, true, 512>(sb, sn, col_bytes, t, T, coef, yacc, dn);
-          else
-            fused_block_setup<Elem, R, GC, true, 0>(sb, sn, col_bytes, t, T, coef, yacc, dn);
-          fused = true;
-        } else if (!more) {
-          if (T == 512)
-            fused_block_setup<Elem, R, GC, false, 512>(sb, sb, col_bytes, t, T, coef, yacc, dn);
-          else
-            fused_block_setup<Elem, R, GC, false, 0>(sb, sb, col_bytes, t, T, coef, yacc, dn);
-          fused = true;
+        const double* rsd = reinterpret_cast<const double*>(rs);
+        if (ncw == 16) {
+          warp_partials_sum<double, 2 * GC>(rsd, 2 * GC, lane, sxy);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 2 * GC; ++k) {
+            double tt = rsd[k];
+            for (int w = 1; w < ncw; ++w) tt += rsd[w * 2 * GC + k];
+            sxy[k] = tt;
+          }
         }
       } else {
-        if (more && cnt_n == GC) {
-          if (T == 512)
-            fused_block<Elem, R, GC, true, 512>(sb, sn, col_bytes, t, T, coef, dx, yacc, dn);
-          else
-            fused_block<Elem, R, GC, true, 0>(sb, sn, col_bytes, t, T, coef, dx, yacc, dn);
-          fused = true;
-        } else if (!more) {
-          if (T == 512)
-            fused_block<Elem, R, GC, false, 512>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
-          else
-            fused_block<Elem, R, GC, false, 0>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
-          fused = true;
+        if (ncw == 16) {
+          warp_partials_sum<float, GC>(reinterpret_cast<const float*>(rs), GC, lane, tots);
+        } else {
+#pragma unroll
+          for (int qq = 0; qq < GC; ++qq) {
+            float tt = rs[qq];
+            for (int w = 1; w < ncw; ++w) tt += rs[w * GC + qq];
+            tots[qq] = tt;
+          }
         }
       }
-    }
-    if (!fused) {
-      // partial dots of the next group (its reduction latency overlaps this group's axpy)
-      if (more) dot_group(grp + 1, dn, got);
-      // y += coef · A over this thread's rows
 #pragma unroll
       for (int qq = 0; qq < GC; ++qq) {
+        coef[qq] = 0.f;
         if (qq < cnt) {
-          const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
-          const float2 c2 = make_float2(coef[qq], coef[qq]);
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const int vi = t + r * T;
-            if (vi < nvec) {
-              float2 av[H];
-              unpack2(col[vi], av);
-#pragma unroll
-              for (int h = 0; h < H; ++h) yacc[r][h] = fma2(c2, av[h], yacc[r][h]);
+          const int k = grp * GC + qq;
+          if constexpr (SETUP) {
+            // α_j = Σa·(1/m) (exactly Σa/m for a power-of-two m); the sums go to colsum and
+            // the column statistics are formed in the epilogue, off this per-group path
+            const double sx = sxy[2 * qq];
+            const float af = (float)(sx * inv_m);
+            coef[qq] = af;
+            a2acc = fma((double)af, (double)af, a2acc);
+            if (t == qq) b.colsum[lo + k] = make_double2(sx, sxy[2 * qq + 1]);
+          } else {
+            const float tot = tots[qq];
+            if (!amm) {
+              coef[qq] = tot;
+            } else if (centred) {
+              const float al = wl_al[k];
+              const float tq = __fmul_rn(__fsub_rn(tot, __fmul_rn(al, sum_dx_f)), wl_w[k]);
+              coef[qq] = tq;
+              sacc = fmaf(al, tq, sacc);
+            } else {
+              coef[qq] = __fmul_rn(tot, wl_w[k]);
             }
           }
         }
       }
+      const bool more = grp + 1 < ngroups;
+      const int cnt_n = more ? min(GC, nb - (grp + 1) * GC) : 0;
+      const int s_nxt = s_cur + 1 == NS ? 0 : s_cur + 1;
+      const uint32_t ph_nxt = s_nxt == 0 ? ph_cur ^ 1u : ph_cur;
+      bool got = true;
+      if (more) got = mbar_wait_bounded(&full[s_nxt], ph_nxt);
+      ok = ok && got;
+      const unsigned char* sb = stages + (size_t)s_cur * stage_bytes;
+      bool fused = false;
+      if (full_slots && cnt == GC && got) {
+        const unsigned char* sn = more ? stages + (size_t)s_nxt * stage_bytes : sb;
+        if constexpr (SETUP) {
+          if (more && cnt_n == GC) {
+            if (T == 512)
+              fused_block_setup<Elem, R, GC, true, 512>(sb, sn, col_bytes, t, T, coef, yacc, dn);
+            else
+              fused_block_setup<Elem, R, GC, true, 0>(sb, sn, col_bytes, t, T, coef, yacc, dn);
+            fused = true;
+          } else if (!more) {
+            if (T == 512)
+              fused_block_setup<Elem, R, GC, false, 512>(sb, sb, col_bytes, t, T, coef, yacc, dn);
+            else
+              fused_block_setup<Elem, R, GC, false, 0>(sb, sb, col_bytes, t, T, coef, yacc, dn);
+            fused = true;
+          }
+        } else {
+          if (more && cnt_n == GC) {
+            if (T == 512)
+              fused_block<Elem, R, GC, true, 512>(sb, sn, col_bytes, t, T, coef, dx, yacc, dn);
+            else
+              fused_block<Elem, R, GC, true, 0>(sb, sn, col_bytes, t, T, coef, dx, yacc, dn);
+            fused = true;
+          } else if (!more) {
+            if (T == 512)
+              fused_block<Elem, R, GC, false, 512>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
+            else
+              fused_block<Elem, R, GC, false, 0>(sb, sb, col_bytes, t, T, coef, dx, yacc, dn);
+            fused = true;
+          }
+        }
+      }
+      if (!fused) {
+        // partial dots of the next group (its reduction latency overlaps this group's axpy)
+        if (more) dot_group(grp + 1, s_nxt, dn, got);
+        // y += coef · A over this thread's rows
+#pragma unroll
+        for (int qq = 0; qq < GC; ++qq) {
+          if (qq < cnt) {
+            const uint4* col = reinterpret_cast<const uint4*>(sb + (size_t)qq * col_bytes);
+            const float2 c2 = make_float2(coef[qq], coef[qq]);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int vi = t + r * T;
+              if (vi < nvec) {
+                float2 av[H];
+                unpack2(col[vi], av);
+#pragma unroll
+                for (int h = 0; h < H; ++h) yacc[r][h] = fma2(c2, av[h], yacc[r][h]);
+              }
+            }
+          }
+        }
+      }
+      if (more) publish(grp + 1, dn);
+      // partials of grp+1 published; every thread is done with stage grp: thread 0 refills it
+      if (named_barrier_or(1, T, !ok)) ok = false;
+      if (t == 0 && ok && grp + NS < ngroups) {
+        // group grp + NS takes the stage of group grp
+        const int c0 = (grp + NS) * GC;
+        const int cn = min(GC, nb - c0);
+        mbar_arrive_expect_tx(&full[s_cur], (uint32_t)cn * col_bytes);
+        for (int qq = 0; qq < cn; ++qq) {
+          const uint32_t col = sampled ? wl_idx[c0 + qq] : (uint32_t)(lo + c0 + qq);
+          bulk_g2s(stages + (size_t)s_cur * stage_bytes + (size_t)qq * col_bytes,
+                   Abase + (size_t)col * col_stride, col_bytes, &full[s_cur], policy);
+        }
+        iss_s = gbase + (uint32_t)(grp + NS + 1);
+      }
+      s_cur = s_nxt;
+      ph_cur = ph_nxt;
     }
-    if (more) publish(grp + 1, dn);
-    // partials of grp+1 published; every thread is done with stage s: thread 0 refills it
-    if (named_barrier_or(1, T, !ok)) ok = false;
-    if (t == 0 && ok && grp + NS < ngroups) issue(grp + NS, wl_idx);
-  }
+    if (!ok) {
+      drain();
+      if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
+      return;
+    }
+    gbase += (uint32_t)ngroups;
+    // every stage is free: the next step's first groups go out now (thread 0)
+    if (!SETUP && t == 0) {
+      const int groups = nx_s[0], nnb = nx_s[2];
+      const bool nsmp = nx_s[3] != 0;
+      const int64_t nlo = nxlo_s;
+      for (int grp = 0; grp < groups; ++grp)
+        issue_at(gbase + (uint32_t)grp, min(GC, nnb - grp * GC),
+                 nsmp ? nxt_cols + grp * GC : nullptr, nlo + grp * GC);
+      if (groups > 0) iss_s = gbase + (uint32_t)groups;
+      pre_s[0] = groups;
+      pre_s[1] = nx_s[1];
+    }
 
-  if (!ok) {
-    if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
-    return;
-  }
-  if (sampled) {
-    // The picks are consumed: their histogram entries and chunk totals are cleared for the
-    // next draw into this slot (several CTAs may zero one chunk total: the same value).
-    const int cs = b.chunk_shift;
-    uint32_t* cnt = b.count[slot];
-    uint32_t* chk = b.chunk[slot];
-    for (int k = t; k < nb; k += T) {
-      const uint32_t col = wl_idx[k];  // written before the barriers of the group loop
-      cnt[col] = 0u;
-      chk[col >> cs] = 0u;
+    if (sampled) {
+      // The picks are consumed: their histogram entries and chunk totals are cleared for the
+      // next draw into this slot (several CTAs may zero one chunk total: the same value).
+      const int cs = b.chunk_shift;
+      uint32_t* cnt = b.count[slot];
+      uint32_t* chk = b.chunk[slot];
+      for (int k = t; k < nb; k += T) {
+        const uint32_t col = wl_idx[k];  // written before the barriers of the group loop
+        cnt[col] = 0u;
+        chk[col >> cs] = 0u;
+      }
     }
-  }
-  float* part = b.partials + (size_t)q * m;
+    float* part = b.partials + (size_t)q * m;
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int vi = t + r * T;
-    if (vi < nvec) {
+    for (int r = 0; r < R; ++r) {
+      const int vi = t + r * T;
+      if (vi < nvec) {
 #pragma unroll
-      for (int h4 = 0; h4 < E / 4; ++h4)
-        reinterpret_cast<float4*>(part)[vi * (E / 4) + h4] =
-            make_float4(yacc[r][2 * h4].x, yacc[r][2 * h4].y, yacc[r][2 * h4 + 1].x,
-                        yacc[r][2 * h4 + 1].y);
+        for (int h4 = 0; h4 < E / 4; ++h4)
+          reinterpret_cast<float4*>(part)[vi * (E / 4) + h4] =
+              make_float4(yacc[r][2 * h4].x, yacc[r][2 * h4].y, yacc[r][2 * h4 + 1].x,
+                          yacc[r][2 * h4 + 1].y);
+      }
     }
-  }
-  if (t == 0) {
-    b.spart[q] = sacc;
-    b.spart64[q] = a2acc;
-  }
+    if (t == 0) {
+      b.spart[q] = sacc;
+      b.spart64[q] = a2acc;
+    }
 
-  // ======================= the step's epilogue, fused (grid-wide) =======================
-  // Every CTA is resident (one per SM), so after a grid barrier the nsm partials are summed
-  // where they sit in L2: CTA q owns float4 row groups [g0, g1) and sums them over the CTAs in
-  // a fixed order (FP64); then the new y rows, and the Rayleigh quotient by the last CTA to
-  // finish (dotProduct_and_generate_x, common.h:103-153).
-  const int RG = m >> 2;
-  const int g0 = (int)((int64_t)q * RG / G), g1 = (int)((int64_t)(q + 1) * RG / G);
-  const float* yprev = b.y[(a.iter + 1) & 1];
-  float* ynew = b.y[a.iter & 1];
-  // the epilogue's own inputs for the first row chunk, fetched before the barrier
-  float4 pre_yp = make_float4(0.f, 0.f, 0.f, 0.f), pre_ym = pre_yp, pre_v = pre_yp;
-  double pre_vs[4] = {0.0, 0.0, 0.0, 0.0};
-  if (!SETUP && warp == 0 && g0 + lane < g1) {
-    const int row = 4 * (g0 + lane);
-    pre_yp = __ldcg(reinterpret_cast<const float4*>(yprev + row));
-    pre_ym = __ldcg(reinterpret_cast<const float4*>(b.y_memo + row));
-    pre_v = __ldcg(reinterpret_cast<const float4*>(b.v + row));
-    if (b.has_vstar)
+    // ====================== the step's epilogue, fused (grid-wide) ======================
+    // Every CTA is resident (one per SM), so after a grid barrier the G partials are summed
+    // where they sit in L2: CTA q owns float4 row groups [g0, g1) and sums them over the CTAs
+    // in a fixed order (FP64); then the new y rows and this CTA's share of the Rayleigh sums
+    // (dotProduct_and_generate_x, common.h:103-153); after a second grid barrier every CTA
+    // forms λ and the next step's state from the CTA shares, in the same order.
+    const int RG = m >> 2;
+    const int g0 = (int)((int64_t)q * RG / G), g1 = (int)((int64_t)(q + 1) * RG / G);
+    const float* yprev = b.y[(i + 1) & 1];
+    float* ynew = b.y[i & 1];
+    // the epilogue's own inputs for the first row chunk, fetched before the barrier
+    float4 pre_yp = make_float4(0.f, 0.f, 0.f, 0.f), pre_ym = pre_yp, pre_v = pre_yp;
+    double pre_vs[4] = {0.0, 0.0, 0.0, 0.0};
+    if (!SETUP && warp == 0 && g0 + lane < g1) {
+      const int row = 4 * (g0 + lane);
+      pre_yp = __ldcg(reinterpret_cast<const float4*>(yprev + row));
+      pre_ym = __ldcg(reinterpret_cast<const float4*>(b.y_memo + row));
+      pre_v = __ldcg(reinterpret_cast<const float4*>(b.v + row));
+      if (b.has_vstar)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) pre_vs[e] = __ldcg(b.vstar + row + e);
-  }
-  // z·dx (dots, common.h:55-87) is needed only here: each CTA sums it over its own rows into
-  // rpart[4q+3]; after the barrier the CTA partials are summed in a fixed order
-  if (centred && warp == 0) {
+        for (int e = 0; e < 4; ++e) pre_vs[e] = __ldcg(b.vstar + row + e);
+    }
+    // z·dx (dots, common.h:55-87) is needed only here: each CTA sums it over its own rows
+    // into rpart[4q+3]; after the barrier the CTA partials are summed in a fixed order
+    if (centred && warp == 0) {
+      for (int c0 = g0; c0 < g1; c0 += 32) {
+        const int gi = c0 + lane;
+        if (gi < g1) {
+          const int row = 4 * gi;
+          const float4 yp =
+              c0 == g0 ? pre_yp : __ldcg(reinterpret_cast<const float4*>(yprev + row));
+          const float4 xm = __ldcg(reinterpret_cast<const float4*>(b.x_memo + row));
+          const float4 z4 = __ldcg(reinterpret_cast<const float4*>(b.z + row));
+          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.x), xm.x), (double)z4.x, zdx);
+          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.y), xm.y), (double)z4.y, zdx);
+          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.z), xm.z), (double)z4.z, zdx);
+          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.w), xm.w), (double)z4.w, zdx);
+        }
+      }
+      zdx = warp_sum(zdx);
+      if (lane == 0) b.rpart[4 * q + 3] = zdx;
+    }
+    named_barrier_or(1, T, false);  // this CTA's partials are written
+    bool bar_ok = true;
+    if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
+    if (named_barrier_or(1, T, !bar_ok)) {
+      drain();
+      if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
+      return;
+    }
+    double S = 0.0;  // Σ over the CTAs of the per-CTA scalar (fixed order, the same everywhere)
+    double xy = 0.0, yy = 0.0, yv = 0.0;
+    constexpr int kU = 10;
     for (int c0 = g0; c0 < g1; c0 += 32) {
       const int gi = c0 + lane;
+      const bool first = (c0 == g0);
+      double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
       if (gi < g1) {
-        const int row = 4 * gi;
-        const float4 yp =
-            c0 == g0 ? pre_yp : __ldcg(reinterpret_cast<const float4*>(yprev + row));
-        const float4 xm = __ldcg(reinterpret_cast<const float4*>(b.x_memo + row));
-        const float4 z4 = __ldcg(reinterpret_cast<const float4*>(b.z + row));
-        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.x), xm.x), (double)z4.x, zdx);
-        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.y), xm.y), (double)z4.y, zdx);
-        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.z), xm.z), (double)z4.z, zdx);
-        zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.w), xm.w), (double)z4.w, zdx);
-      }
-    }
-    zdx = warp_sum(zdx);
-    if (lane == 0) b.rpart[4 * q + 3] = zdx;
-  }
-  named_barrier_or(1, T, false);  // this CTA's partials are written
-  bool bar_ok = true;
-  if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
-  if (named_barrier_or(1, T, !bar_ok)) {
-    if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
-    return;
-  }
-  double4* red = reinterpret_cast<double4*>(stages);  // [warps][32]; the stages are drained
-  double S = 0.0;  // Σ over the CTAs of the per-CTA scalar (fixed order, the same everywhere)
-  double xy = 0.0, yy = 0.0, yv = 0.0;
-  constexpr int kU = 10;
-  for (int c0 = g0; c0 < g1; c0 += 32) {
-    const int gi = c0 + lane;
-    const bool first = (c0 == g0);
-    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (gi < g1) {
-      const float* P = b.partials + 4 * (size_t)gi;
-      for (int k0 = warp; k0 < G; k0 += ncw * kU) {
-        float4 v[kU];
+        const float* P = b.partials + 4 * (size_t)gi;
+        for (int k0 = warp; k0 < G; k0 += ncw * kU) {
+          float4 v[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const int k = k0 + u * ncw;
-          v[u] = k < G ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * m))
-                       : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        if (first && k0 == warp && warp == 0 && (SETUP || centred)) {
-          zdx = 0.0;
-          for (int k = lane; k < G; k += 32) {
-            S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
-            if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
+          for (int u = 0; u < kU; ++u) {
+            const int k = k0 + u * ncw;
+            v[u] = k < G ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * m))
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
           }
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          acc.x += v[u].x;
-          acc.y += v[u].y;
-          acc.z += v[u].z;
-          acc.w += v[u].w;
-        }
-      }
-    } else if (first && warp == 0 && (SETUP || centred)) {
-      zdx = 0.0;
-      for (int k = lane; k < G; k += 32) {
-        S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
-        if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
-      }
-    }
-    if (first && warp == 0) {
-      S = warp_sum(S);
-      zdx = warp_sum(zdx);
-    }
-    red[warp * 32 + lane] = acc;
-    named_barrier_or(1, T, false);
-    if (warp == 0 && gi < g1) {
-      double4 tot = red[lane];
-      for (int w = 1; w < ncw; ++w) {
-        const double4 r4 = red[w * 32 + lane];
-        tot.x += r4.x;
-        tot.y += r4.y;
-        tot.z += r4.z;
-        tot.w += r4.w;
-      }
-      const int row = 4 * gi;
-      const double tv[4] = {tot.x, tot.y, tot.z, tot.w};
-      if constexpr (SETUP) {
-        // z = A·α and v = z − ‖α‖² (generate_v, core_proposedAMM.cuh:4-15)
-        float zf[4], vf[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          zf[e] = (float)tv[e];
-          vf[e] = (float)((double)zf[e] - S);
-        }
-        *reinterpret_cast<float4*>(b.z + row) = make_float4(zf[0], zf[1], zf[2], zf[3]);
-        *reinterpret_cast<float4*>(b.v + row) = make_float4(vf[0], vf[1], vf[2], vf[3]);
-      } else {
-        const float4 yp = first ? pre_yp : *reinterpret_cast<const float4*>(yprev + row);
-        const float xa[4] = {__fmul_rn(scale, yp.x), __fmul_rn(scale, yp.y),
-                             __fmul_rn(scale, yp.z), __fmul_rn(scale, yp.w)};
-        float yo[4];
-        if (!amm) {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) yo[e] = (float)tv[e];
-        } else {
-          const float4 ym = first ? pre_ym : *reinterpret_cast<const float4*>(b.y_memo + row);
-          const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
-          if (!centred) {  // previous: y_memo + A_S·tmp (core_previousAMM.cuh:225-232)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) yo[e] = (float)((double)ymv[e] + tv[e]);
-          } else {
-            // y_memo + Σdx·v + z·dx in FP64, rounded (core_proposedAMM.cuh:198-212)
-            const float4 vv = first ? pre_v : *reinterpret_cast<const float4*>(b.v + row);
-            const float va[4] = {vv.x, vv.y, vv.z, vv.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const float base = (float)(fma(sum_dx, (double)va[e], zdx) + (double)ymv[e]);
-              yo[e] = (float)((double)base + (tv[e] - S));
+          if (first && k0 == warp && warp == 0 && (SETUP || centred)) {
+            zdx = 0.0;
+            for (int k = lane; k < G; k += 32) {
+              S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
+              if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
             }
           }
-        }
-        *reinterpret_cast<float4*>(ynew + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
-        if (mode == kExactMemo) {
-          *reinterpret_cast<float4*>(b.x_memo + row) = make_float4(xa[0], xa[1], xa[2], xa[3]);
-          *reinterpret_cast<float4*>(b.y_memo + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
-        }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const double yd = (double)yo[e];
-          xy = fma(yd, (double)xa[e], xy);
-          yy = fma(yd, yd, yy);
-          if (b.has_vstar) yv = fma(yd, first ? pre_vs[e] : b.vstar[row + e], yv);
+          for (int u = 0; u < kU; ++u) {
+            acc.x += v[u].x;
+            acc.y += v[u].y;
+            acc.z += v[u].z;
+            acc.w += v[u].w;
+          }
+        }
+      } else if (first && warp == 0 && (SETUP || centred)) {
+        zdx = 0.0;
+        for (int k = lane; k < G; k += 32) {
+          S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
+          if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
+        }
+      }
+      if (first && warp == 0) {
+        S = warp_sum(S);
+        zdx = warp_sum(zdx);
+      }
+      red[warp * 32 + lane] = acc;
+      named_barrier_or(1, T, false);
+      if (warp == 0 && gi < g1) {
+        double4 tot = red[lane];
+        for (int w = 1; w < ncw; ++w) {
+          const double4 r4 = red[w * 32 + lane];
+          tot.x += r4.x;
+          tot.y += r4.y;
+          tot.z += r4.z;
+          tot.w += r4.w;
+        }
+        const int row = 4 * gi;
+        const double tv[4] = {tot.x, tot.y, tot.z, tot.w};
+        if constexpr (SETUP) {
+          // z = A·α and v = z − ‖α‖² (generate_v, core_proposedAMM.cuh:4-15)
+          float zf[4], vf[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            zf[e] = (float)tv[e];
+            vf[e] = (float)((double)zf[e] - S);
+          }
+          *reinterpret_cast<float4*>(b.z + row) = make_float4(zf[0], zf[1], zf[2], zf[3]);
+          *reinterpret_cast<float4*>(b.v + row) = make_float4(vf[0], vf[1], vf[2], vf[3]);
+        } else {
+          const float4 yp = first ? pre_yp : *reinterpret_cast<const float4*>(yprev + row);
+          const float xa[4] = {__fmul_rn(scale, yp.x), __fmul_rn(scale, yp.y),
+                               __fmul_rn(scale, yp.z), __fmul_rn(scale, yp.w)};
+          float yo[4];
+          if (!amm) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) yo[e] = (float)tv[e];
+          } else {
+            const float4 ym = first ? pre_ym : *reinterpret_cast<const float4*>(b.y_memo + row);
+            const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
+            if (!centred) {  // previous: y_memo + A_S·tmp (core_previousAMM.cuh:225-232)
+#pragma unroll
+              for (int e = 0; e < 4; ++e) yo[e] = (float)((double)ymv[e] + tv[e]);
+            } else {
+              // y_memo + Σdx·v + z·dx in FP64, rounded (core_proposedAMM.cuh:198-212)
+              const float4 vv = first ? pre_v : *reinterpret_cast<const float4*>(b.v + row);
+              const float va[4] = {vv.x, vv.y, vv.z, vv.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const float base = (float)(fma(sum_dx, (double)va[e], zdx) + (double)ymv[e]);
+                yo[e] = (float)((double)base + (tv[e] - S));
+              }
+            }
+          }
+          *reinterpret_cast<float4*>(ynew + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
+          if (mode == kExactMemo) {
+            *reinterpret_cast<float4*>(b.x_memo + row) = make_float4(xa[0], xa[1], xa[2], xa[3]);
+            *reinterpret_cast<float4*>(b.y_memo + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
+          }
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const double yd = (double)yo[e];
+            xy = fma(yd, (double)xa[e], xy);
+            yy = fma(yd, yd, yy);
+            if (b.has_vstar) yv = fma(yd, first ? pre_vs[e] : b.vstar[row + e], yv);
+          }
+        }
+      }
+      named_barrier_or(1, T, false);  // red is reused by the next row chunk
+    }
+    if constexpr (SETUP) {
+      // the column statistics (get_norms, device_memory.h:34-59) from the column sums: α =
+      // Σa/m (as the coefficient above), ‖A_j‖ = sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² −
+      // mean²·m) clamped at 0 (the reference stores NaN when cancellation makes it negative)
+      for (int j = q * T + t; j < b.n; j += G * T) {
+        const double2 s = __ldcg(b.colsum + j);
+        const double mean = s.x / (double)m;
+        b.alpha[j] = (float)(s.x * inv_m);
+        b.norm[j] = (float)sqrt(s.y);
+        b.normp[j] = (float)sqrt(fmax(s.y - mean * mean * (double)m, 0.0));
+      }
+      if (q == 0 && warp == 0) {
+        if (g0 >= g1) {  // no rows here (m/4 < number of CTAs): ‖α‖² is summed separately
+          for (int k = lane; k < G; k += 32) S += __ldcg(b.spart64 + k);
+          S = warp_sum(S);
+        }
+        if (lane == 0) *b.alpha2 = S;
+      }
+      return;
+    } else {
+      if (warp == 0) {
+        xy = warp_sum(xy);
+        yy = warp_sum(yy);
+        yv = warp_sum(yv);
+        if (lane == 0) {
+          b.rpart[4 * q + 0] = xy;
+          b.rpart[4 * q + 1] = yy;
+          b.rpart[4 * q + 2] = yv;
+        }
+      }
+      named_barrier_or(1, T, false);  // this CTA's Rayleigh shares are written
+      if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
+      if (named_barrier_or(1, T, !bar_ok)) {
+        drain();
+        if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
+        return;
+      }
+      // λ and the next step, formed by every CTA from the CTA shares: warp 0 sums them
+      // lane-strided and then by an xor butterfly (a fixed association order)
+      if (warp == 0) {
+        xy = 0.0;
+        yy = 0.0;
+        yv = 0.0;
+        for (int k = lane; k < G; k += 32) {
+          xy += __ldcg(b.rpart + 4 * k + 0);
+          yy += __ldcg(b.rpart + 4 * k + 1);
+          yv += __ldcg(b.rpart + 4 * k + 2);
+        }
+        xy = warp_sum(xy);
+        yy = warp_sum(yy);
+        yv = warp_sum(yv);
+        if (lane == 0) {
+          StepScalars sc;
+          const IterState nx = next_state(cc, i, st_s, xy, yy, yv, &sc);
+          if (q == 0) record_step(b, cc, i, st_s, sc);
+          st_s = nx;  // published by the barrier at the top of the next step
         }
       }
     }
-    named_barrier_or(1, T, false);  // red is reused by the next row chunk
   }
-  if constexpr (SETUP) {
-    // the column statistics (get_norms, device_memory.h:34-59) from the column sums: α = Σa/m
-    // (as the coefficient above), ‖A_j‖ = sqrt(Σa²), ‖A_j − α_j‖ = sqrt(Σa² − mean²·m) clamped
-    // at 0 (the reference stores NaN when cancellation makes it negative)
-    for (int j = q * T + t; j < b.n; j += G * T) {
-      const double2 s = __ldcg(b.colsum + j);
-      const double mean = s.x / (double)m;
-      b.alpha[j] = (float)(s.x * inv_m);
-      b.norm[j] = (float)sqrt(s.y);
-      b.normp[j] = (float)sqrt(fmax(s.y - mean * mean * (double)m, 0.0));
-    }
-    if (q == 0 && warp == 0) {
-      if (g0 >= g1) {  // no rows here (m/4 < number of CTAs): ‖α‖² is summed separately
-        for (int k = lane; k < G; k += 32) S += __ldcg(b.spart64 + k);
-        S = warp_sum(S);
-      }
-      if (lane == 0) *b.alpha2 = S;
-    }
-    return;
-  } else {
-    if (warp != 0) return;
-    xy = warp_sum(xy);
-    yy = warp_sum(yy);
-    yv = warp_sum(yv);
-    uint32_t last = 0;
-    if (lane == 0) {
-      b.rpart[4 * q + 0] = xy;
-      b.rpart[4 * q + 1] = yy;
-      b.rpart[4 * q + 2] = yv;
-      __threadfence();
-      last = (atomicAdd(b.ticket, 1u) == (uint32_t)(G - 1)) ? 1u : 0u;
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (!last) return;
-    __threadfence();
-    // the last CTA: Rayleigh quotient and the next step.  Warp 0 sums the CTA partials
-    // lane-strided and then by an xor butterfly: a fixed association order.
-    xy = 0.0;
-    yy = 0.0;
-    yv = 0.0;
-    for (int k = lane; k < G; k += 32) {
-      xy += __ldcg(b.rpart + 4 * k + 0);
-      yy += __ldcg(b.rpart + 4 * k + 1);
-      yv += __ldcg(b.rpart + 4 * k + 2);
-    }
-    xy = warp_sum(xy);
-    yy = warp_sum(yy);
-    yv = warp_sum(yv);
-    if (lane != 0) return;
-    b.ticket[0] = 0u;
-    finish_step(b, a.cc, a.iter, st_s, xy, yy, yv);
+  // past the last step of the launch (or the early stop): the state the next launch (or the
+  // call's end) reads, and no copy still in flight
+  if (!SETUP) {
+    drain();
+    if (q == 0 && t == 0) b.st[a.iter_end & 1] = st_s;
   }
 }
 
@@ -947,7 +1064,13 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   const int fgc = env_int("AMM_PANEL_GC", 0);
   if (fgc > 0) gc = fgc;
   const int stage = gc * colb;
-  int ns = (192 * 1024) / stage;
+  const int maxlist = c < n ? c : n;
+  // the stages take what the rest of the carve leaves of 227 KB (at most 8)
+  PanelGeom probe{};
+  probe.gc = gc;
+  probe.wl_cap = (maxlist + nsm - 1) / nsm + 1;
+  const int rest = smem_layout(probe, true).total;
+  int ns = (227 * 1024 - rest) / stage;
   if (ns > 8) ns = 8;
   const int fns = env_int("AMM_PANEL_STAGES", 0);
   if (fns > 0 && fns < ns) ns = fns;
@@ -965,8 +1088,7 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   b.nstages = ns;
   b.stage_bytes = stage;
   b.stage_area = ns * stage;
-  const int maxlist = c < n ? c : n;
-  b.wl_cap = (maxlist + nsm - 1) / nsm + 1;
+  b.wl_cap = probe.wl_cap;
   b.smem_bytes = smem_layout(b, true).total;
   *g = b;
   return b.smem_bytes <= 227 * 1024;
@@ -999,16 +1121,18 @@ cudaError_t launch_setup_panel(const Buffers& b, const PanelGeom& g, cudaStream_
   a.b = b;
   a.g = g;
   a.iter = 0;
+  a.iter_end = 1;
   return launch_panel(a, true, s);
 }
 
 cudaError_t launch_iter_panel(const Buffers& b, const PanelGeom& g, const CallCfg& cc, int iter,
-                              cudaStream_t s) {
+                              int iter_end, cudaStream_t s) {
   PanelArgs a{};
   a.b = b;
   a.g = g;
   a.cc = cc;
   a.iter = iter;
+  a.iter_end = iter_end;
   return launch_panel(a, false, s);
 }
 
