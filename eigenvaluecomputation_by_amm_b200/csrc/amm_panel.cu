@@ -59,7 +59,7 @@ __device__ __forceinline__ double2 warp_red(double2 v) {
 
 // Shared memory carve (byte offsets), identical on host and device.
 struct SmemLayout {
-  int stages, bars, redw, wl_idx, wl_w, wl_al, nxt, red, total;
+  int stages, bars, redw, wl_idx, wl_w, wl_al, nxt, red, epi, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup) {
@@ -85,6 +85,8 @@ __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup
   o += 4 * kGcMax * 8;
   L.red = o;  // row-reduction scratch: [16 warps][32] double4
   o += 16 * 32 * 32;
+  L.epi = o;  // this CTA's first 32 row groups of y_{i-1}, y_memo, v, x_memo, z (float4)
+  o += 5 * 32 * 16 + 32 * 32;  // and v* (4 doubles)
   L.total = (o + 127) & ~127;
   return L;
 }
@@ -263,12 +265,20 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   float* wl_al = reinterpret_cast<float*>(smem + L.wl_al);
   uint32_t* nxt_cols = reinterpret_cast<uint32_t*>(smem + L.nxt);  // [kGcMax * 8]
   double4* red = reinterpret_cast<double4*>(smem + L.red);          // [16 warps][32]
+  float4* epi_yp = reinterpret_cast<float4*>(smem + L.epi);          // [32] each
+  float4* epi_ym = epi_yp + 32;
+  float4* epi_v = epi_yp + 64;
+  float4* epi_xm = epi_yp + 96;
+  float4* epi_z = epi_yp + 128;
+  double* epi_vs = reinterpret_cast<double*>(epi_yp + 160);          // [32][4]
   __shared__ IterState st_s;   // state of the current step, identical in every CTA
   __shared__ int32_t pre_s[2];  // groups of the current step issued ahead, and their list key
   __shared__ uint32_t cd_s[kListWindow];  // work-list lengths of the slots (fixed per launch)
   __shared__ int32_t nx_s[4];   // predicted next list: groups to issue ahead, key, length, sampled
   __shared__ int64_t nxlo_s;    // ... and its first index
   __shared__ uint32_t iss_s;    // groups issued so far (thread 0)
+  __shared__ IterState nxs_s;   // the next state, formed by warp 0
+  __shared__ int32_t wlkey_s;   // slot of the coefficient slice copied ahead into wl_* (-2: none)
 
   // A launch of the step kernel is a programmatic dependent of the grid before it: its CTAs
   // start on the SMs that the previous grid leaves, initialise their barriers, and wait for
@@ -292,9 +302,44 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       st_s = b.st[a.iter & 1];
       pre_s[0] = 0;
       pre_s[1] = -2;
+      wlkey_s = -2;
     }
   }
   if (t == 0) iss_s = 0u;
+  // this CTA's rows of the grid-wide epilogue: float4 row groups [g0, g1)
+  const int RG = m >> 2;
+  const int g0 = (int)((int64_t)q * RG / G), g1 = (int)((int64_t)(q + 1) * RG / G);
+  // The first 32 of them are kept in shared memory for the whole launch: y_{i-1}, y_memo,
+  // x_memo (the epilogue rewrites them as it produces y_i and a new memo pair), v, z and v*.
+  if (!SETUP && warp == (ncw > 2 ? 2 : 0) && g0 + lane < g1) {
+    const int row = 4 * (g0 + lane);
+    epi_yp[lane] = __ldcg(reinterpret_cast<const float4*>(b.y[(a.iter + 1) & 1] + row));
+    epi_ym[lane] = __ldcg(reinterpret_cast<const float4*>(b.y_memo + row));
+    epi_xm[lane] = __ldcg(reinterpret_cast<const float4*>(b.x_memo + row));
+    epi_v[lane] = __ldcg(reinterpret_cast<const float4*>(b.v + row));
+    epi_z[lane] = __ldcg(reinterpret_cast<const float4*>(b.z + row));
+#pragma unroll
+    for (int e = 0; e < 4; ++e) epi_vs[lane * 4 + e] = b.has_vstar ? __ldcg(b.vstar + row + e) : 0.0;
+  }
+  // this thread's rows of y_{j-1} (and x_memo in calls that sample) for step j
+  float4 ypv[R][E / 4], xmv[R][E / 4];
+  auto load_vecs = [&](int j) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int vi = t + r * T;
+#pragma unroll
+      for (int h4 = 0; h4 < E / 4; ++h4) {
+        ypv[r][h4] = make_float4(0.f, 0.f, 0.f, 0.f);
+        xmv[r][h4] = ypv[r][h4];
+        if (!SETUP && vi < nvec) {
+          const int o4 = vi * (E / 4) + h4;
+          ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(j + 1) & 1]) + o4);
+          if (cc.uses_amm) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
+        }
+      }
+    }
+  };
+
 
   // this CTA's slice [lo, hi) of the column list of a step reading `cd` sampled columns
   // (sampled) or all n columns
@@ -333,6 +378,121 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         wait_pos(p);
     }
   };
+
+  // ---- everything step j needs that does not depend on the product of the step before ----
+  // dx = x_j − x_memo on this thread's rows (x_j = scale·y_{j−1}, FP32 multiply) and the CTA's
+  // Σdx; one warp's z·dx over this CTA's rows (dots, common.h:55-87, into rpart[4q+3]) and the
+  // epilogue's inputs of its first 32 row groups; the coefficient slice of the step's list; and
+  // the list predicted for step j+1 (exact unless the adaptive VR switch, which needs step j's
+  // cosine, changes the kind), whose first column indices thread 0 issues as soon as step j's
+  // last group is consumed, so that HBM stays busy through the grid-wide epilogue.  Run for the
+  // first step of the launch, and for each later step right after the state is formed.
+  float2 dx[R][H];
+  double sum_dx = 0.0;
+  auto prepare = [&](int j, const IterState& sj) {
+    const bool jamm = sj.mode == kPrevious || sj.mode == kProposed;
+    const bool jcentred = sj.mode == kProposed;
+    const bool jsampled = jamm && !cc.sanity;
+    const int jslot = sj.used % kListWindow;
+    const float jscale = sj.scale;
+    int64_t jlo, jhi;
+    slice(jsampled, cd_s[jslot], jlo, jhi);
+    const int jnb = (int)(jhi - jlo);
+    const float* yprev = b.y[(j + 1) & 1];
+    load_vecs(j);
+    if (warp == (ncw > 2 ? 2 : 0)) {
+      if (jcentred) {
+        double zp = 0.0;
+        for (int c0 = g0; c0 < g1; c0 += 32) {
+          const int gi = c0 + lane;
+          if (gi < g1) {
+            const int row = 4 * gi;
+            const bool st0 = c0 == g0;  // the first 32 row groups are in shared memory
+            const float4 yp = st0 ? epi_yp[lane] : __ldcg(reinterpret_cast<const float4*>(yprev + row));
+            const float4 xm = st0 ? epi_xm[lane] : __ldcg(reinterpret_cast<const float4*>(b.x_memo + row));
+            const float4 z4 = st0 ? epi_z[lane] : __ldcg(reinterpret_cast<const float4*>(b.z + row));
+            zp = fma((double)__fsub_rn(__fmul_rn(jscale, yp.x), xm.x), (double)z4.x, zp);
+            zp = fma((double)__fsub_rn(__fmul_rn(jscale, yp.y), xm.y), (double)z4.y, zp);
+            zp = fma((double)__fsub_rn(__fmul_rn(jscale, yp.z), xm.z), (double)z4.z, zp);
+            zp = fma((double)__fsub_rn(__fmul_rn(jscale, yp.w), xm.w), (double)z4.w, zp);
+          }
+        }
+        zp = warp_sum(zp);
+        if (lane == 0) b.rpart[4 * q + 3] = zp;
+      }
+    }
+    // the coefficient slice, unless copied ahead on the right prediction (the warps after warp
+    // 0, all of a one-warp CTA)
+    if (jamm && !(jsampled && wlkey_s == jslot)) {
+      cp_async_wait_all();  // no copy ahead may still land in wl_*
+      const int t1 = T > 32 ? t - 32 : t, T1 = T > 32 ? T - 32 : T;
+      for (int k = t1; k >= 0 && k < jnb; k += T1) {
+        if (jsampled) {
+          wl_idx[k] = __ldg(b.wl_col[jslot] + jlo + k);
+          wl_w[k] = __ldg(b.wl_wm[jslot] + jlo + k);
+          wl_al[k] = __ldg(b.wl_al[jslot] + jlo + k);
+        } else {  // sanity mode: identity list, weight 1
+          wl_w[k] = 1.0f;
+          wl_al[k] = __ldg(b.alpha + jlo + k);
+        }
+      }
+    }
+    if (warp == (ncw > 1 ? 1 : 0)) {
+      int groups = 0, nkey = -2, nnb = 0, nsmp = 0;
+      int64_t nlo = 0;
+      if (j + 1 < a.iter_end) {
+        int le;
+        const int nmode = decide_mode(cc, j + 1, sj.cos_prev, sj.last_exact, &le);
+        const int nslot = (sj.used + (jsampled ? 1 : 0)) % kListWindow;
+        nsmp = ((nmode == kPrevious || nmode == kProposed) && !cc.sanity) ? 1 : 0;
+        int64_t nhi;
+        slice(nsmp != 0, cd_s[nslot], nlo, nhi);
+        nnb = (int)(nhi - nlo);
+        groups = min(NS, (nnb + GC - 1) / GC);
+        nkey = nsmp ? nslot : -1;
+        if (nsmp) {
+          const int nf = min(NS * GC, nnb);
+          for (int k = lane; k < nf; k += 32) cp_async4(nxt_cols + k, b.wl_col[nslot] + nlo + k);
+        }
+      }
+      if (lane == 0) {
+        nx_s[0] = groups;
+        nx_s[1] = nkey;
+        nx_s[2] = nnb;
+        nx_s[3] = nsmp;
+        nxlo_s = nlo;
+      }
+    }
+    double sdx = 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int h4 = 0; h4 < E / 4; ++h4) {
+        const float4 yp = ypv[r][h4];
+        const float4 xm = jamm ? xmv[r][h4] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float d0 = __fsub_rn(__fmul_rn(jscale, yp.x), xm.x);
+        const float d1 = __fsub_rn(__fmul_rn(jscale, yp.y), xm.y);
+        const float d2 = __fsub_rn(__fmul_rn(jscale, yp.z), xm.z);
+        const float d3 = __fsub_rn(__fmul_rn(jscale, yp.w), xm.w);
+        dx[r][2 * h4] = make_float2(d0, d1);
+        dx[r][2 * h4 + 1] = make_float2(d2, d3);
+        if (jcentred) sdx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
+      }
+    }
+    sum_dx = 0.0;
+    if (jcentred) {  // Σdx over all m rows (dots, common.h:55-87), identical in every CTA
+      sdx = warp_sum(sdx);
+      double* wtmp = reinterpret_cast<double*>(redw);
+      if (lane == 0) wtmp[warp] = sdx;
+      named_barrier_or(1, T, false);
+      for (int w = 0; w < ncw; ++w) sum_dx += wtmp[w];
+      named_barrier_or(1, T, false);  // wtmp (= redw) is reused by the group loop
+    }
+  };
+  if (!SETUP) {
+    __syncthreads();  // st_s
+    if (a.iter < a.iter_end && !st_s.done) prepare(a.iter, st_s);  // uniform over the grid
+  }
 
   for (int i = a.iter;; ++i) {
     int mode = kExact, slot = 0;
@@ -374,23 +534,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       }
     }
 
-    // ---- dx = x_i − x_memo on this thread's rows, x_i = scale·y_{i−1} (FP32 multiply) ----
-    // The loads are issued before the first copies, the arithmetic after them.
-    float4 ypv[R][E / 4], xmv[R][E / 4];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int vi = t + r * T;
-#pragma unroll
-      for (int h4 = 0; h4 < E / 4; ++h4) {
-        ypv[r][h4] = make_float4(0.f, 0.f, 0.f, 0.f);
-        xmv[r][h4] = ypv[r][h4];
-        if (!SETUP && vi < nvec) {
-          const int o4 = vi * (E / 4) + h4;
-          ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(i + 1) & 1]) + o4);
-          if (amm) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
-        }
-      }
-    }
     if (t == 0 && ngroups > pre) {  // the first NS groups not already in flight
       uint32_t first[kGcMax * 8];
       const int nf = min(NS * GC, nb);
@@ -402,84 +545,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       iss_s = gbase + (uint32_t)min(NS, ngroups);
     }
 
-    // The next step's list, predicted from this step's state (exact unless the adaptive VR
-    // switch, which needs this step's cosine, changes the kind): its first column indices are
-    // staged in shared memory now, and thread 0 issues its first groups as soon as this step's
-    // last group is consumed, so HBM stays busy through the grid-wide epilogue.
-    // (one warp: the warp after thread 0's, or warp 0 alone in a one-warp CTA)
-    if (!SETUP && warp == (ncw > 1 ? 1 : 0)) {
-      int groups = 0, nkey = -2, nnb = 0, nsmp = 0;
-      int64_t nlo = 0;
-      if (i + 1 < a.iter_end) {
-        int le;
-        const int nmode = decide_mode(cc, i + 1, st_s.cos_prev, st_s.last_exact, &le);
-        const int nslot = (st_s.used + (sampled ? 1 : 0)) % kListWindow;
-        nsmp = ((nmode == kPrevious || nmode == kProposed) && !cc.sanity) ? 1 : 0;
-        int64_t nhi;
-        slice(nsmp != 0, cd_s[nslot], nlo, nhi);
-        nnb = (int)(nhi - nlo);
-        groups = min(NS, (nnb + GC - 1) / GC);
-        nkey = nsmp ? nslot : -1;
-        if (nsmp) {
-          const int nf = min(NS * GC, nnb);
-          for (int k = lane; k < nf; k += 32) nxt_cols[k] = __ldg(b.wl_col[nslot] + nlo + k);
-        }
-      }
-      if (lane == 0) {
-        nx_s[0] = groups;
-        nx_s[1] = nkey;
-        nx_s[2] = nnb;
-        nx_s[3] = nsmp;
-        nxlo_s = nlo;
-      }
-    }
-
-    float2 dx[R][H];
     float2 yacc[R][H];
-    double sum_dx = 0.0, zdx = 0.0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-#pragma unroll
-      for (int h4 = 0; h4 < E / 4; ++h4) {
-        const float4 yp = ypv[r][h4];
-        const float4 xm = amm ? xmv[r][h4] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float d0 = __fsub_rn(__fmul_rn(scale, yp.x), xm.x);
-        const float d1 = __fsub_rn(__fmul_rn(scale, yp.y), xm.y);
-        const float d2 = __fsub_rn(__fmul_rn(scale, yp.z), xm.z);
-        const float d3 = __fsub_rn(__fmul_rn(scale, yp.w), xm.w);
-        dx[r][2 * h4] = make_float2(d0, d1);
-        dx[r][2 * h4 + 1] = make_float2(d2, d3);
-        if (centred) sum_dx += ((double)d0 + (double)d1) + ((double)d2 + (double)d3);
-      }
-    }
 #pragma unroll
     for (int r = 0; r < R; ++r)
 #pragma unroll
       for (int h = 0; h < H; ++h) yacc[r][h] = make_float2(0.f, 0.f);
-    if (amm) {
-      // coefficient data of the slice, loaded by the warps after warp 0 (whose thread 0 issues
-      // the copies); published by the CTA barrier ahead of the first group
-      const int t1 = T > 32 ? t - 32 : t, T1 = T > 32 ? T - 32 : T;
-      for (int k = t1; k >= 0 && k < nb; k += T1) {
-        if (sampled) {
-          wl_idx[k] = __ldg(list_col + k);
-          wl_w[k] = __ldg(b.wl_wm[slot] + lo + k);
-          wl_al[k] = __ldg(b.wl_al[slot] + lo + k);
-        } else {  // sanity mode: identity list, weight 1
-          wl_w[k] = 1.0f;
-          wl_al[k] = __ldg(b.alpha + lo + k);
-        }
-      }
-    }
-    if (centred) {  // Σdx over all m rows (dots, common.h:55-87), identical in every CTA
-      sum_dx = warp_sum(sum_dx);
-      double* wtmp = reinterpret_cast<double*>(redw);
-      if (lane == 0) wtmp[warp] = sum_dx;
-      named_barrier_or(1, T, false);
-      sum_dx = 0.0;
-      for (int w = 0; w < ncw; ++w) sum_dx += wtmp[w];
-      named_barrier_or(1, T, false);  // wtmp (= redw) is reused below
-    }
+    double zdx = 0.0;
     const float sum_dx_f = (float)sum_dx;
 
     // ring slot (stage, phase parity) of group 0 of this step; the group loop advances it
@@ -583,6 +654,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       dot_group(0, s_cur, dn, ok);
       publish(0, dn);
     }
+    cp_async_wait_all();  // the slice and next-list indices copied ahead, published below
     if (named_barrier_or(1, T, !ok)) ok = false;
     for (int grp = 0; ok && grp < ngroups; ++grp) {
       const int cnt = min(GC, nb - grp * GC);
@@ -778,42 +850,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     // in a fixed order (FP64); then the new y rows and this CTA's share of the Rayleigh sums
     // (dotProduct_and_generate_x, common.h:103-153); after a second grid barrier every CTA
     // forms λ and the next step's state from the CTA shares, in the same order.
-    const int RG = m >> 2;
-    const int g0 = (int)((int64_t)q * RG / G), g1 = (int)((int64_t)(q + 1) * RG / G);
     const float* yprev = b.y[(i + 1) & 1];
     float* ynew = b.y[i & 1];
-    // the epilogue's own inputs for the first row chunk, fetched before the barrier
-    float4 pre_yp = make_float4(0.f, 0.f, 0.f, 0.f), pre_ym = pre_yp, pre_v = pre_yp;
-    double pre_vs[4] = {0.0, 0.0, 0.0, 0.0};
-    if (!SETUP && warp == 0 && g0 + lane < g1) {
-      const int row = 4 * (g0 + lane);
-      pre_yp = __ldcg(reinterpret_cast<const float4*>(yprev + row));
-      pre_ym = __ldcg(reinterpret_cast<const float4*>(b.y_memo + row));
-      pre_v = __ldcg(reinterpret_cast<const float4*>(b.v + row));
-      if (b.has_vstar)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) pre_vs[e] = __ldcg(b.vstar + row + e);
-    }
-    // z·dx (dots, common.h:55-87) is needed only here: each CTA sums it over its own rows
-    // into rpart[4q+3]; after the barrier the CTA partials are summed in a fixed order
-    if (centred && warp == 0) {
-      for (int c0 = g0; c0 < g1; c0 += 32) {
-        const int gi = c0 + lane;
-        if (gi < g1) {
-          const int row = 4 * gi;
-          const float4 yp =
-              c0 == g0 ? pre_yp : __ldcg(reinterpret_cast<const float4*>(yprev + row));
-          const float4 xm = __ldcg(reinterpret_cast<const float4*>(b.x_memo + row));
-          const float4 z4 = __ldcg(reinterpret_cast<const float4*>(b.z + row));
-          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.x), xm.x), (double)z4.x, zdx);
-          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.y), xm.y), (double)z4.y, zdx);
-          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.z), xm.z), (double)z4.z, zdx);
-          zdx = fma((double)__fsub_rn(__fmul_rn(scale, yp.w), xm.w), (double)z4.w, zdx);
-        }
-      }
-      zdx = warp_sum(zdx);
-      if (lane == 0) b.rpart[4 * q + 3] = zdx;
-    }
     named_barrier_or(1, T, false);  // this CTA's partials are written
     bool bar_ok = true;
     if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
@@ -889,7 +927,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
           *reinterpret_cast<float4*>(b.z + row) = make_float4(zf[0], zf[1], zf[2], zf[3]);
           *reinterpret_cast<float4*>(b.v + row) = make_float4(vf[0], vf[1], vf[2], vf[3]);
         } else {
-          const float4 yp = first ? pre_yp : *reinterpret_cast<const float4*>(yprev + row);
+          const float4 yp = first ? epi_yp[lane] : *reinterpret_cast<const float4*>(yprev + row);
           const float xa[4] = {__fmul_rn(scale, yp.x), __fmul_rn(scale, yp.y),
                                __fmul_rn(scale, yp.z), __fmul_rn(scale, yp.w)};
           float yo[4];
@@ -897,14 +935,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
 #pragma unroll
             for (int e = 0; e < 4; ++e) yo[e] = (float)tv[e];
           } else {
-            const float4 ym = first ? pre_ym : *reinterpret_cast<const float4*>(b.y_memo + row);
+            const float4 ym = first ? epi_ym[lane] : *reinterpret_cast<const float4*>(b.y_memo + row);
             const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
             if (!centred) {  // previous: y_memo + A_S·tmp (core_previousAMM.cuh:225-232)
 #pragma unroll
               for (int e = 0; e < 4; ++e) yo[e] = (float)((double)ymv[e] + tv[e]);
             } else {
               // y_memo + Σdx·v + z·dx in FP64, rounded (core_proposedAMM.cuh:198-212)
-              const float4 vv = first ? pre_v : *reinterpret_cast<const float4*>(b.v + row);
+              const float4 vv = first ? epi_v[lane] : *reinterpret_cast<const float4*>(b.v + row);
               const float va[4] = {vv.x, vv.y, vv.z, vv.w};
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
@@ -918,12 +956,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
             *reinterpret_cast<float4*>(b.x_memo + row) = make_float4(xa[0], xa[1], xa[2], xa[3]);
             *reinterpret_cast<float4*>(b.y_memo + row) = make_float4(yo[0], yo[1], yo[2], yo[3]);
           }
+          if (first) {  // the next step's copy of these rows
+            epi_yp[lane] = make_float4(yo[0], yo[1], yo[2], yo[3]);
+            if (mode == kExactMemo) {
+              epi_xm[lane] = make_float4(xa[0], xa[1], xa[2], xa[3]);
+              epi_ym[lane] = epi_yp[lane];
+            }
+          }
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const double yd = (double)yo[e];
             xy = fma(yd, (double)xa[e], xy);
             yy = fma(yd, yd, yy);
-            if (b.has_vstar) yv = fma(yd, first ? pre_vs[e] : b.vstar[row + e], yv);
+            if (b.has_vstar) yv = fma(yd, first ? epi_vs[lane * 4 + e] : b.vstar[row + e], yv);
           }
         }
       }
@@ -958,6 +1003,20 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
           b.rpart[4 * q + 1] = yy;
           b.rpart[4 * q + 2] = yv;
         }
+      } else if (i + 1 < a.iter_end) {
+        // the coefficient slice of the predicted next list, copied ahead (checked in prepare)
+        const bool smp = nx_s[3] != 0;
+        if (smp) {
+          const int nslot = nx_s[1];
+          const int64_t nlo = nxlo_s;
+          const int nnb = nx_s[2];
+          for (int k = t - 32; k < nnb; k += T - 32) {
+            cp_async4(wl_idx + k, b.wl_col[nslot] + nlo + k);
+            cp_async4(wl_w + k, b.wl_wm[nslot] + nlo + k);
+            cp_async4(wl_al + k, b.wl_al[nslot] + nlo + k);
+          }
+        }
+        if (t == 32) wlkey_s = smp ? nx_s[1] : -2;
       }
       named_barrier_or(1, T, false);  // this CTA's Rayleigh shares are written
       if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
@@ -966,8 +1025,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
         return;
       }
-      // λ and the next step, formed by every CTA from the CTA shares: warp 0 sums them
-      // lane-strided and then by an xor butterfly (a fixed association order)
+      // λ and the next step, formed by warp 0 from the CTA shares (summed lane-strided and then
+      // by an xor butterfly: the same order in every CTA)
       if (warp == 0) {
         xy = 0.0;
         yy = 0.0;
@@ -982,11 +1041,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         yv = warp_sum(yv);
         if (lane == 0) {
           StepScalars sc;
-          const IterState nx = next_state(cc, i, st_s, xy, yy, yv, &sc);
+          nxs_s = next_state(cc, i, st_s, xy, yy, yv, &sc);
           if (q == 0) record_step(b, cc, i, st_s, sc);
-          st_s = nx;  // published by the barrier at the top of the next step
         }
       }
+      named_barrier_or(1, T, false);  // nxs_s
+      const IterState nx = nxs_s;
+      if (i + 1 < a.iter_end && !nx.done) prepare(i + 1, nx);  // uniform over the grid
+      if (t == 0) st_s = nx;  // published by the barrier at the top of the next step
     }
   }
   // past the last step of the launch (or the early stop): the state the next launch (or the
