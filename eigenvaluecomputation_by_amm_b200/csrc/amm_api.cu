@@ -149,7 +149,7 @@ void layout(amm_ctx* ctx, Carver& cv) {
   b.ticket = cv.take<uint32_t>(4);
   b.alpha2 = cv.take<double>(1);
   b.colvec = cv.take<float>(n);
-  b.cdf_tsum = cv.take<double>(2 * ((n + 4095) / 4096));
+  b.cdf_tsum = cv.take<double>(2 * ((n + amm::kCdfTile - 1) / amm::kCdfTile));
   b.st = cv.take<amm::IterState>(2);
   b.eigs = cv.take<double>(step);
   b.errs = cv.take<double>(step);

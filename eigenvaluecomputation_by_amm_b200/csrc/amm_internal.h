@@ -17,6 +17,7 @@ constexpr int kMaxThreads = 512;   // panel kernel block size limit
 constexpr int kGcMax = 8;          // columns per pipeline stage, upper bound
 constexpr int kSeg = 32;           // fine-search window of the sampler (elements)
 constexpr int kCoarseMax = 2048;   // coarse CDF table entries held in shared memory
+constexpr int kCdfTile = 1024;     // columns per block of the CDF construction
 // AMM work lists drawn ahead.  The picks of an AMM step depend only on the sampling states and
 // the CDF, never on x, so the lists of up to kListWindow consecutive AMM steps are drawn and
 // compacted together before the first of them (one refill every kListWindow steps); list a of a
@@ -107,7 +108,7 @@ struct Buffers {
                        // [1], [3]: spare
   double* alpha2;      // ‖α‖²
   float* colvec;       // n floats of scratch (vᵀA for the gradient)
-  double* cdf_tsum;    // 2 x ceil(n/4096) tile sums of the CDF build
+  double* cdf_tsum;    // 2 x ceil(n/kCdfTile) tile sums of the CDF build
   // iteration state and traces
   IterState* st;       // [2]
   double* eigs;

@@ -13,6 +13,8 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
+#include <utility>
 
 #include "amm_device.cuh"
 #include "amm_internal.h"
@@ -22,6 +24,35 @@ namespace amm {
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// The per-call kernels are launched as programmatic dependents of the kernel before them in the
+// stream (each waits for it with griddep_wait before touching global memory), so that their
+// launch overlaps the previous kernel's tail.  AMM_PDL=0 turns it off, for comparison.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = getenv("AMM_PDL");
+    return !(v && *v && atoi(v) == 0);
+  }();
+  return on;
+}
+
+template <typename... P, typename... A>
+static cudaError_t launch_pdl(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t s,
+                              A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+  count_launch();
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
 
 
 // First index i in [0, n) with cdf[i] > target, else n-1 (device_memory.h:529-543).
@@ -125,6 +156,8 @@ struct SampleArgs {
 // window are drawn by independent grid rows.
 template <typename F>
 __global__ void __launch_bounds__(256) sample_kernel(const __grid_constant__ SampleArgs a) {
+  griddep_wait();
+  griddep_launch_dependents();
   __shared__ __align__(16) F coarse_s[kCoarseMax];
   const Buffers& b = a.b;
   const CallCfg& cc = a.cc;
@@ -149,6 +182,8 @@ constexpr int kCompactPer = 4;
 constexpr int kCompactSpan = kCompactThreads * kCompactPer;
 
 __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_constant__ SampleArgs a) {
+  griddep_wait();
+  griddep_launch_dependents();
   __shared__ uint32_t scan[40];
   const Buffers& b = a.b;
   const CallCfg& cc = a.cc;
@@ -218,6 +253,8 @@ struct InitArgs {
 };
 
 __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ InitArgs a) {
+  griddep_wait();
+  griddep_launch_dependents();
   const Buffers& b = a.b;
   const CallCfg& cc = a.cc;
   const int t = threadIdx.x;
@@ -279,6 +316,8 @@ struct FinalArgs {
 };
 
 __global__ void __launch_bounds__(kFinalThreads) finalize_kernel(const __grid_constant__ FinalArgs a) {
+  griddep_wait();
+  griddep_launch_dependents();
   const Buffers& b = a.b;
   const IterState st = b.st[a.cc.step & 1];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
@@ -316,8 +355,7 @@ __global__ void __launch_bounds__(kFinalThreads) finalize_kernel(const __grid_co
 // table of the sampler.
 // ------------------------------------------------------------------------------------------
 constexpr int kCdfThreads = 256;
-constexpr int kCdfPer = 16;
-constexpr int kCdfTile = kCdfThreads * kCdfPer;
+constexpr int kCdfPer = kCdfTile / kCdfThreads;  // kCdfTile: amm_internal.h
 
 
 // Block-wide exclusive scan of one double per thread (kCdfThreads threads); total in *total.
@@ -392,6 +430,8 @@ __device__ void tile_local_prefix(const Buffers& b, const float* base, int t0, i
 // grid (ntiles, weightings): the total of each tile
 __global__ void __launch_bounds__(kCdfThreads) cdf_tile_sums_kernel(const __grid_constant__ Buffers b,
                                                                    int which0, int sanity) {
+  griddep_wait();
+  griddep_launch_dependents();
   __shared__ double ws[34];
   __shared__ float tile[kCdfTile];
   const int which = which0 + blockIdx.y;
@@ -404,6 +444,8 @@ __global__ void __launch_bounds__(kCdfThreads) cdf_tile_sums_kernel(const __grid
 // grid (ntiles, weightings): CDF of each tile (unless imported), weights w_j
 __global__ void __launch_bounds__(kCdfThreads) cdf_scan_kernel(const __grid_constant__ Buffers b,
                                                                int which0, int keep_cdf, int sanity) {
+  griddep_wait();
+  griddep_launch_dependents();
   __shared__ double ws[34];
   __shared__ float tile[kCdfTile];
   __shared__ double pre_s, total_s;
@@ -437,15 +479,31 @@ __global__ void __launch_bounds__(kCdfThreads) cdf_scan_kernel(const __grid_cons
     for (int e = 0; e < kCdfPer; ++e) {
       const int j = t0 + threadIdx.x * kCdfPer + e;
       if (j < n) {
-        if (b.cdf_f32)
-          b.cdf32[which][j] = (float)(pre + lp[e]);
-        else
-          b.cdf64[which][j] = pre + lp[e];
+        const bool seg_end = ((j + 1) & (b.seg - 1)) == 0 && (j + 1) / b.seg <= b.ncoarse;
+        if (b.cdf_f32) {
+          const float cv = (float)(pre + lp[e]);
+          b.cdf32[which][j] = cv;
+          if (seg_end) b.coarse32[which][(j + 1) / b.seg - 1] = cv;
+        } else {
+          const double cv = pre + lp[e];
+          b.cdf64[which][j] = cv;
+          if (seg_end) b.coarse64[which][(j + 1) / b.seg - 1] = cv;
+        }
       }
     }
     total64 = total_s;
   } else {
     total64 = b.cdf_f32 ? (double)b.cdf32[which][n - 1] : b.cdf64[which][n - 1];
+    // the coarse table of the imported CDF: the last value of each full segment
+    for (int k = threadIdx.x; k < kCdfTile; k += kCdfThreads) {
+      const int j = t0 + k;
+      if (j < n && ((j + 1) & (b.seg - 1)) == 0 && (j + 1) / b.seg <= b.ncoarse) {
+        if (b.cdf_f32)
+          b.coarse32[which][(j + 1) / b.seg - 1] = b.cdf32[which][j];
+        else
+          b.coarse64[which][(j + 1) / b.seg - 1] = b.cdf64[which][j];
+      }
+    }
   }
   const float total32 = b.cdf_f32 ? (float)total64 : 0.f;
   for (int k = threadIdx.x; k < kCdfTile; k += kCdfThreads) {
@@ -466,22 +524,6 @@ __global__ void __launch_bounds__(kCdfThreads) cdf_scan_kernel(const __grid_cons
     atomicOr(b.status, (uint32_t)kDevNonFinite);
 }
 
-// coarse table (after the CDF is complete)
-__global__ void __launch_bounds__(256) cdf_coarse_kernel(const __grid_constant__ Buffers b,
-                                                         int which0) {
-  const int which = which0 + blockIdx.y;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.ncoarse; s += gridDim.x * blockDim.x) {
-    const int j = (s + 1) * b.seg - 1;
-    if (b.cdf_f32)
-      b.coarse32[which][s] = b.cdf32[which][j];
-    else
-      b.coarse64[which][s] = b.cdf64[which][j];
-  }
-}
-
-// ------------------------------------------------------------------------------------------
-// Standalone helpers (not on the iteration path)
-// ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) normalize_kernel(float* x, int m) {
   __shared__ double ws[16];
   __shared__ float scale_s;
@@ -622,14 +664,10 @@ cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sani
   const dim3 grid(ntiles, which >= 0 ? 1 : 2);
   const int w0 = which >= 0 ? which : 0;
   if (!keep_cdf) {
-    cdf_tile_sums_kernel<<<grid, kCdfThreads, 0, s>>>(b, w0, sanity);
-    count_launch();
+    const cudaError_t e = launch_pdl(cdf_tile_sums_kernel, grid, dim3(kCdfThreads), s, b, w0, sanity);
+    if (e != cudaSuccess) return e;
   }
-  cdf_scan_kernel<<<grid, kCdfThreads, 0, s>>>(b, w0, keep_cdf, sanity);
-  const int cb = (b.ncoarse + 255) / 256;
-  cdf_coarse_kernel<<<dim3(cb > 0 ? cb : 1, grid.y), 256, 0, s>>>(b, w0);
-  count_launch(2);
-  return cudaGetLastError();
+  return launch_pdl(cdf_scan_kernel, grid, dim3(kCdfThreads), s, b, w0, keep_cdf, sanity);
 }
 
 cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, int no_normalize,
@@ -639,9 +677,7 @@ cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, in
   a.cc = cc;
   a.x0 = x0;
   a.no_normalize = no_normalize;
-  init_kernel<<<1, 1024, 0, s>>>(a);
-  count_launch();
-  return cudaGetLastError();
+  return launch_pdl(init_kernel, dim3(1), dim3(1024), s, a);
 }
 
 cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s) {
@@ -652,12 +688,8 @@ cudaError_t launch_sample(const Buffers& b, const CallCfg& cc, int iter, cudaStr
   int blocks = (b.c + 255) / 256;
   if (blocks > 1024) blocks = 1024;
   const int rows = cc.step < kListWindow ? cc.step : kListWindow;
-  if (b.cdf_f32)
-    sample_kernel<float><<<dim3(blocks, rows), 256, 0, s>>>(a);
-  else
-    sample_kernel<double><<<dim3(blocks, rows), 256, 0, s>>>(a);
-  count_launch();
-  return cudaGetLastError();
+  if (b.cdf_f32) return launch_pdl(sample_kernel<float>, dim3(blocks, rows), dim3(256), s, a);
+  return launch_pdl(sample_kernel<double>, dim3(blocks, rows), dim3(256), s, a);
 }
 
 cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaStream_t s) {
@@ -667,9 +699,7 @@ cudaError_t launch_compact(const Buffers& b, const CallCfg& cc, int iter, cudaSt
   a.iter = iter;
   const int blocks = (b.n + kCompactSpan - 1) / kCompactSpan;
   const int rows = cc.step < kListWindow ? cc.step : kListWindow;
-  compact_kernel<<<dim3(blocks, rows), kCompactThreads, 0, s>>>(a);
-  count_launch();
-  return cudaGetLastError();
+  return launch_pdl(compact_kernel, dim3(blocks, rows), dim3(kCompactThreads), s, a);
 }
 
 cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, float* ydst,
@@ -681,9 +711,7 @@ cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, fl
   a.ydst = ydst;
   int blocks = (b.m + kFinalThreads - 1) / kFinalThreads;
   if (blocks > 256) blocks = 256;
-  finalize_kernel<<<blocks, kFinalThreads, 0, s>>>(a);
-  count_launch();
-  return cudaGetLastError();
+  return launch_pdl(finalize_kernel, dim3(blocks), dim3(kFinalThreads), s, a);
 }
 
 __global__ void clock_kernel(unsigned long long* out) { *out = globaltimer_ns(); }
