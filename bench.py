@@ -457,8 +457,10 @@ def run_ours(args, rank, world):
         "speedup_vs_exact_fp32": ms_exact / ms,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "traffic": traffic, "peak_source": src,
-                     "kernel": f"panel_kernel<bf16> step kernel, launch mix of one solve "
-                               f"({n_vr} exact + {n_amm} proposed AMM)",
+                     "kernel": f"panel_kernel<bf16> step kernel, step mix of one solve "
+                               f"({n_vr} exact + {n_amm} proposed AMM); each kind timed as "
+                               "single-step launches (in a solve the steps run back to back "
+                               "inside one persistent launch)",
                      "bytes_per_launch": bytes_mix, "ms_per_launch": t_mix},
         "roofline_amm_step": {"achieved": ach_amm, "frac": ach_amm / hbm, "ms_per_launch": t_amm,
                               "bytes_per_launch": bytes_amm, "distinct_columns": cd},
