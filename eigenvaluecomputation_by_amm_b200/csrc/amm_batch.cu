@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <tuple>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -134,7 +135,10 @@ __device__ void jacobi_warp(double* H, double* V, double* cs, int lane) {
     }
     off = warp_sum(off);
     dia = warp_sum(dia);
-    if (!(off > 1e-30 * dia)) break;  // also stops on NaN
+    // off-diagonal entries below ~1e-13 of the matrix: the eigenvalue error left is their
+    // square over the gap (the FP64 rounding floor of `off` is ~K²·eps²·dia, so a tighter test
+    // would never be met and run every sweep); also stops on NaN
+    if (!(off > 1e-26 * dia)) break;
     for (int r = 0; r < K - 1; ++r) {
       if (lane < K / 2) {
         int p, q;
@@ -246,12 +250,14 @@ __device__ __forceinline__ float team_allreduce(float (&d)[NV], float* part, int
 template <int K>
 __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm, double* Hm,
                                        double* Vm, double* cs, double* ritz, float* Rinv,
-                                       float* qv, int* ctl, int lane, bool writer) {
+                                       float* qv, int* ctl, double* scratch, int lane,
+                                       bool writer) {
   const bool first = (it == 0);
   const bool rr = !first && ((K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter));
   if (rr) jacobi_warp<K>(Hm, Vm, cs, lane);
+  // the Ritz values (lane 0: K entries)
+  int st = 0;
   if (lane == 0) {
-    int st = 0;
     ctl[2] = rr ? 1 : 0;
     if (rr) {
       int best = 0;
@@ -272,75 +278,92 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
       ritz[kMaxK] = lam;
       if (!isfinite(lam)) st = 2;
     }
-    if (st == 0) {
-      double Gp[kMaxK][kMaxK];
-      if (rr) {  // VᵀGV
-        double T[kMaxK][kMaxK];
-        for (int i = 0; i < K; ++i)
-          for (int j = 0; j < K; ++j) {
-            double s = 0.0;
-            for (int k = 0; k < K; ++k) s += Gm[i * K + k] * Vm[k * K + j];
-            T[i][j] = s;
-          }
-        for (int i = 0; i < K; ++i)
-          for (int j = 0; j < K; ++j) {
-            double s = 0.0;
-            for (int k = 0; k < K; ++k) s += Vm[k * K + i] * T[k][j];
-            Gp[i][j] = s;
-          }
-      } else {
-        for (int i = 0; i < K; ++i)
-          for (int j = 0; j < K; ++j) Gp[i][j] = Gm[i * K + j];
+  }
+  st = __shfl_sync(0xffffffffu, st, 0);
+  // The next basis, by the whole warp with the K x K matrices in shared memory (`scratch`:
+  // 4·K² doubles); each entry is summed in the same order as a sequential loop would.
+  double* Gp = scratch;              // VᵀGV (or G)
+  double* T = scratch + K * K;       // G·V
+  double* L = scratch + 2 * K * K;   // Cholesky factor (lower)
+  double* Li = scratch + 3 * K * K;  // L⁻¹ (lower)
+  if (st == 0) {
+    if (rr) {
+      for (int idx = lane; idx < K * K; idx += 32) {
+        const int i = idx / K, j = idx % K;
+        double acc = 0.0;
+        for (int k = 0; k < K; ++k) acc += Gm[i * K + k] * Vm[k * K + j];
+        T[idx] = acc;
       }
-      double L[kMaxK][kMaxK];
-      double tr = 0.0;
-      for (int i = 0; i < K; ++i) tr += Gp[i][i];
-      bool ok = tr > 0.0 && isfinite(tr);
-      for (int j = 0; j < K && ok; ++j) {
-        double d = Gp[j][j];
-        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
-        if (!(d > 1e-24 * tr)) {
-          ok = false;
-          break;
-        }
-        L[j][j] = sqrt(d);
+      __syncwarp();
+      for (int idx = lane; idx < K * K; idx += 32) {
+        const int i = idx / K, j = idx % K;
+        double acc = 0.0;
+        for (int k = 0; k < K; ++k) acc += Vm[k * K + i] * T[k * K + j];
+        Gp[idx] = acc;
+      }
+    } else {
+      for (int idx = lane; idx < K * K; idx += 32) Gp[idx] = Gm[idx];
+    }
+    for (int idx = lane; idx < K * K; idx += 32) L[idx] = 0.0;
+    __syncwarp();
+    double tr = 0.0;
+    for (int i = 0; i < K; ++i) tr += Gp[i * K + i];
+    bool ok = tr > 0.0 && isfinite(tr);
+    // Cholesky, column by column: the diagonal by lane 0, the column below it by lanes j+1..
+    for (int j = 0; j < K && ok; ++j) {
+      if (lane == 0) {
+        double d = Gp[j * K + j];
+        for (int k = 0; k < j; ++k) d -= L[j * K + k] * L[j * K + k];
+        const bool good = d > 1e-24 * tr;
+        L[j * K + j] = good ? sqrt(d) : 0.0;
+        cs[0] = good ? 1.0 : 0.0;
+      }
+      __syncwarp();
+      ok = cs[0] != 0.0;
+      if (ok && lane > j && lane < K) {
+        const int i = lane;
+        double sv = Gp[i * K + j];
+        for (int k = 0; k < j; ++k) sv -= L[i * K + k] * L[j * K + k];
+        L[i * K + j] = sv / L[j * K + j];
+      }
+      __syncwarp();
+    }
+    if (!ok) {  // rank-deficient block: no result for this matrix
+      st = 2;
+    } else {
+      // L⁻¹, column j by lane j (forward substitution)
+      if (lane < K) {
+        const int j = lane;
+        for (int i = 0; i < K; ++i) Li[i * K + j] = 0.0;
+        Li[j * K + j] = 1.0 / L[j * K + j];
         for (int i = j + 1; i < K; ++i) {
-          double s = Gp[i][j];
-          for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
-          L[i][j] = s / L[j][j];
+          double sv = 0.0;
+          for (int k = j; k < i; ++k) sv += L[i * K + k] * Li[k * K + j];
+          Li[i * K + j] = -sv / L[i * K + i];
         }
       }
-      if (!ok) {  // rank-deficient block: no result for this matrix
-        st = 2;
-      } else {
-        double Li[kMaxK][kMaxK];  // L⁻¹ (lower)
-        for (int j = 0; j < K; ++j) {
-          Li[j][j] = 1.0 / L[j][j];
-          for (int i = j + 1; i < K; ++i) {
-            double s = 0.0;
-            for (int k = j; k < i; ++k) s += L[i][k] * Li[k][j];
-            Li[i][j] = -s / L[i][i];
-          }
+      __syncwarp();
+      // M = V·L⁻ᵀ (or L⁻ᵀ without a rotation); (L⁻ᵀ)[k][j] = Li[j][k] for k <= j
+      for (int idx = lane; idx < K * K; idx += 32) {
+        const int i = idx / K, j = idx % K;
+        double sv = 0.0;
+        if (rr) {
+          for (int k = 0; k <= j; ++k) sv += Vm[i * K + k] * Li[j * K + k];
+        } else {
+          sv = (i <= j) ? Li[j * K + i] : 0.0;
         }
-        // M = V·L⁻ᵀ (or L⁻ᵀ without a rotation); (L⁻ᵀ)[k][j] = Li[j][k] for k <= j
-        for (int i = 0; i < K; ++i)
-          for (int j = 0; j < K; ++j) {
-            double s = 0.0;
-            if (rr) {
-              for (int k = 0; k <= j; ++k) s += Vm[i * K + k] * Li[j][k];
-            } else {
-              s = (i <= j) ? Li[j][i] : 0.0;
-            }
-            Rinv[i * K + j] = (float)s;
-          }
+        Rinv[i * K + j] = (float)sv;
       }
     }
+  }
+  if (lane == 0) {
     if (st == 2 && writer) {
       for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = nan("");
       a.iters[mi] = -1;
     }
     ctl[1] = st;
   }
+  __syncwarp();
 }
 
 template <int K, int GC>
@@ -525,7 +548,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         }
         __syncthreads();
       }
-      if (warp == 0) ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, lane, writer);
+      // (gpart, summed into Gm and Hm above, is the Ritz step's scratch)
+      if (warp == 0)
+        ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, gpart, lane, writer);
       __syncthreads();
       if (ctl[2] && ctl[1] == 0) {
         // residual of the top Ritz pair, r = C·v − λ·v = (Y − λ·X)·q, over team 0's rows (FP64)
@@ -761,7 +786,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             for (int v = 0; v < K; ++v) yred[((team * 4 * P) + r0 + e) * K + v] = Y[e][v];
         }
         __syncthreads();
-        if (rows) {
+        if (rows && team == 0) {  // only team 0 uses the summed Y (Gram, residual, X, v)
 #pragma unroll
           for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -783,7 +808,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             for (int v = 0; v < K; ++v) yred[(r0 + e) * K + v] = Y[e][v];
         }
         cluster.sync();
-        if (rows) {
+        if (rows && team == 0) {
 #pragma unroll
           for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -999,7 +1024,9 @@ int launch(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_
 }
 
 // Tile-shape autotuner: every (columns per group, cluster size) pair with the requested K runs
-// the whole batch for a few iterations; the fastest (CUDA events) is kept for the context.
+// the whole batch for up to 20 iterations (enough for the per-matrix set-up, which favours
+// larger clusters, to weigh as it does in a real run); the fastest of two timed runs (CUDA
+// events) is kept for the context.
 int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaStream_t s) {
   if (b->variant >= 0) return AMM_OK;
   int best = -1, best_cl = 1, best_grid = 0;
@@ -1008,29 +1035,47 @@ int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaSt
   BATCH_CUDA(cudaEventCreate(&e0));
   BATCH_CUDA(cudaEventCreate(&e1));
   const int n_var = (int)(sizeof(amm::batch::kVariants) / sizeof(amm::batch::kVariants[0]));
+  // the candidates; a single one (tile and cluster size fixed by the caller) is taken untimed
+  std::vector<std::tuple<int, int, int>> cand;  // (variant, cluster size, grid)
   for (int v = 0; v < n_var; ++v) {
     if (amm::batch::kVariants[v].K != b->cfg.nvec) continue;
     if (b->cfg.tile_gc > 0 && amm::batch::kVariants[v].GC != b->cfg.tile_gc) continue;
     for (int cl : amm::batch::kClusterSizes) {
       if (b->cfg.cluster > 0 && cl != b->cfg.cluster) continue;
       const int grid = persistent_grid(b, v, cl);
-      if (grid <= 0) continue;
-      int rc = launch(b, v, cl, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);
-      if (rc) return rc;
+      if (grid > 0) cand.emplace_back(v, cl, grid);
+    }
+  }
+  if (cand.size() == 1) {
+    b->variant = std::get<0>(cand[0]);
+    b->cluster = std::get<1>(cand[0]);
+    b->grid = std::get<2>(cand[0]);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return AMM_OK;
+  }
+  for (const auto& cd : cand) {
+    const int v = std::get<0>(cd), cl = std::get<1>(cd), grid = std::get<2>(cd);
+    const int iters = (int)std::min<int64_t>(b->cfg.max_iter, 20);
+    int rc = launch(b, v, cl, grid, d_lam, d_vec, d_iters, iters, b->d_order, (int)b->count, s);
+    if (rc) return rc;
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
       BATCH_CUDA(cudaEventRecord(e0, s));
-      rc = launch(b, v, cl, grid, d_lam, d_vec, d_iters, 3, b->d_order, (int)b->count, s);
+      rc = launch(b, v, cl, grid, d_lam, d_vec, d_iters, iters, b->d_order, (int)b->count, s);
       if (rc) return rc;
       BATCH_CUDA(cudaEventRecord(e1, s));
       BATCH_CUDA(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      b->tune_ms[{v, cl}] = ms;
-      if (best < 0 || ms < best_ms) {
-        best = v;
-        best_cl = cl;
-        best_grid = grid;
-        best_ms = ms;
-      }
+      float t = 0.f;
+      BATCH_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      ms = rep == 0 ? t : std::min(ms, t);
+    }
+    b->tune_ms[{v, cl}] = ms;
+    if (best < 0 || ms < best_ms) {
+      best = v;
+      best_cl = cl;
+      best_grid = grid;
+      best_ms = ms;
     }
   }
   cudaEventDestroy(e0);
