@@ -137,8 +137,13 @@ __device__ void load_coarse(const Buffers& b, int which, F* coarse_s) {
     src = reinterpret_cast<const F*>(b.coarse64[which]);
   else
     src = reinterpret_cast<const F*>(b.coarse32[which]);
-  const F* __restrict__ csrc = src;
-  for (int k = threadIdx.x; k < b.ncoarse; k += blockDim.x) coarse_s[k] = __ldg(csrc + k);
+  // asynchronous 16-byte copies (every copy in flight at once; the table and its shared-memory
+  // copy are 16-byte aligned), the odd tail by plain loads
+  constexpr int V = 16 / (int)sizeof(F);
+  const int nv = b.ncoarse / V;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) cp_async16(coarse_s + k * V, src + k * V);
+  for (int k = nv * V + threadIdx.x; k < b.ncoarse; k += blockDim.x) coarse_s[k] = __ldg(src + k);
+  cp_async_wait_all();
   __syncthreads();
 }
 
@@ -266,6 +271,7 @@ __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ Init
   // 345-355, called first by every powerMethod_by_*); the single-product entry points keep
   // the memo their caller supplied
   const bool clear_memo = !a.no_normalize;
+#pragma unroll 4
   for (int k0 = 4 * t; k0 < b.m; k0 += 4 * blockDim.x) {  // m % 4 == 0
     const float4 v = __ldg(reinterpret_cast<const float4*>(x0 + k0));
     *reinterpret_cast<float4*>(y1 + k0) = v;
