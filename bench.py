@@ -195,6 +195,24 @@ def cpu_exact_solve(At, x0, k):
 # ------------------------------------------------------------------------------------------
 # reference arm
 # ------------------------------------------------------------------------------------------
+def max_over_ranks(ms, world, device=None):
+    """The slowest rank's time (all ranks take part; one process per GPU, or gloo on CPU)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# D2H bytes of one trace read (amm_get_trace after a call of k steps): the iteration state
+# (56 bytes), λ, err, cos (FP64) and kind, distinct count (int32) per step, k+1 FP64 clock
+# stamps, and the 4-byte status word
+def trace_d2h_bytes(k):
+    return 56 + k * (3 * 8 + 4 + 4) + 8 * (k + 1) + 4
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -355,12 +373,7 @@ def run_ours(args, rank, world):
             timed_solve(ctx, A16, "proposed", 1, 0)
     tr = ctx.trace()
     lam_amm = float(tr["eigs"][-1])
-    ms = max(ts)
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(max(ts), world, dev)
     value = world * 1000.0 / ms
 
     # ---- roofline of the step kernel (live CUDA-event timing) ----
@@ -412,15 +425,15 @@ def run_ours(args, rank, world):
             ctx.set_rng_state(state_sets[r % len(state_sets)])
             ctx.set_matrix(A16_buf.t())
             ctx.power_method("proposed", x0_buf)
+            eig = ctx.trace()["eigs"][-1]          # D2H of the λ trace (synchronises)
             e1.record(stream)
             e1.synchronize()
-            eig = ctx.trace()["eigs"][-1]          # D2H of the λ trace
             if r >= 1:
                 te.append(e0.elapsed_time(e1))
-        ms_e2e = max(te)
+        ms_e2e = max_over_ranks(max(te), world, dev)
         e2e = {"value": world * 1000.0 / ms_e2e, "unit": "solves/s",
                "h2d_bytes_per_step": int(A16_h.numel() * 2 + m * 4),
-               "d2h_bytes_per_step": int(8 * amm_steps * 3 + 4 * amm_steps * 2),
+               "d2h_bytes_per_step": trace_d2h_bytes(amm_steps),
                "ms_per_step": ms_e2e, "lambda": float(eig)}
         del A16_buf
 

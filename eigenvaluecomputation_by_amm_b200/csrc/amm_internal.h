@@ -41,6 +41,7 @@ struct IterState {
   double cos_prev;     // cos of the previous step (adaptive VR)
   double lam_prev;     // λ of the previous step (tolerance stop)
 };
+static_assert(sizeof(IterState) == 56, "the trace read copies 56 bytes of state");
 
 // Static description of one power-method call, passed by value to the kernels.
 struct CallCfg {
