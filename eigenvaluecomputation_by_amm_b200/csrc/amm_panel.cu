@@ -29,6 +29,9 @@
 
 namespace amm {
 
+// column groups of the next step issued at the end of a step's last group
+constexpr int kPrefetchGroups = 2;
+
 struct PanelArgs {
   Buffers b;
   PanelGeom g;
@@ -802,9 +805,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       return;
     }
     gbase += (uint32_t)ngroups;
-    // every stage is free: the next step's first groups go out now (thread 0)
+    // every stage is free: the next step's first groups go out now (thread 0).  Two groups
+    // (about 128 KB per CTA): measured on the B200, a third one slows the partial-sum writes
+    // and the grid barrier that follow by more than it saves, and issuing them after the
+    // barrier arrival gains nothing.
     if (!SETUP && t == 0) {
-      const int groups = nx_s[0], nnb = nx_s[2];
+      const int groups = min(nx_s[0], kPrefetchGroups), nnb = nx_s[2];
       const bool nsmp = nx_s[3] != 0;
       const int64_t nlo = nxlo_s;
       for (int grp = 0; grp < groups; ++grp)
