@@ -313,6 +313,7 @@ __device__ __forceinline__ IterState next_state(const CallCfg& cc, int i, const 
   nx.lam_prev = lam;
   nx.steps_run = i + 1;
   if (consumed && !cc.sanity) nx.used = st.used + 1;
+  if (st.mode == kExactMemo) nx.memo_zero = 0;  // this step wrote the memo pair
   if (cc.uses_amm && !cc.sanity && i % kListWindow == 0) nx.drawn = window_end(cc, i, st);
   sc->nonfinite = !isfinite(lam) || !isfinite(scale);
   bool done = sc->nonfinite;

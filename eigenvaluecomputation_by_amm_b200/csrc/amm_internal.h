@@ -35,7 +35,7 @@ struct IterState {
   int32_t drawn;       // work lists drawn so far: lists [used, drawn) are pending
   int32_t steps_run;   // completed steps
   int32_t distinct;    // distinct columns of the last AMM product (written by the panel kernel)
-  int32_t pad;
+  int32_t memo_zero;   // the memo pair is zero (call start, until the first VR step)
   float scale;         // x_i = scale * y_{i-1} (FP32 multiply)
   float pad2;
   double cos_prev;     // cos of the previous step (adaptive VR)

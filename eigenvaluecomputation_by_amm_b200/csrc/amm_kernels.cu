@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ Init
     st.used = 0;
     st.drawn = 0;
     st.steps_run = 0;
+    st.memo_zero = clear_memo ? 1 : 0;
     if (!(s > 0.0) || !isfinite(s)) {
       atomicOr(b.status, (uint32_t)kDevNonFinite);
       st.done = 1;

@@ -324,9 +324,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
 #pragma unroll
     for (int e = 0; e < 4; ++e) epi_vs[lane * 4 + e] = b.has_vstar ? __ldcg(b.vstar + row + e) : 0.0;
   }
-  // this thread's rows of y_{j-1} (and x_memo in calls that sample) for step j
+  // this thread's rows of y_{j-1} (and of x_memo when it is not known to be zero) for step j
   float4 ypv[R][E / 4], xmv[R][E / 4];
-  auto load_vecs = [&](int j) {
+  auto load_vecs = [&](int j, bool memo) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int vi = t + r * T;
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         if (!SETUP && vi < nvec) {
           const int o4 = vi * (E / 4) + h4;
           ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(j + 1) & 1]) + o4);
-          if (cc.uses_amm) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
+          if (memo) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
         }
       }
     }
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     slice(jsampled, cd_s[jslot], jlo, jhi);
     const int jnb = (int)(jhi - jlo);
     const float* yprev = b.y[(j + 1) & 1];
-    load_vecs(j);
+    load_vecs(j, jamm && !sj.memo_zero);
     if (warp == (ncw > 2 ? 2 : 0)) {
       if (jcentred) {
         double zp = 0.0;
