@@ -105,8 +105,8 @@ struct Buffers {
   double* spart64;     // nsm  (Σ α_j² of each CTA, set-up)
   double2* colsum;     // n (Σa, Σa²) of each column from the set-up pass
   double* rpart;       // nsm x 4 (x·y, y·y, y·v*, z·dx) of each CTA
-  uint32_t* ticket;    // [0]: last-CTA ticket of a step, [2]: grid-barrier arrivals,
-                       // [1], [3]: spare
+  uint32_t* ticket;    // [2]: grid-barrier arrivals of the step kernel and the set-up pass;
+                       // [0], [1], [3]: spare
   double* alpha2;      // ‖α‖²
   float* colvec;       // n floats of scratch (vᵀA for the gradient)
   double* cdf_tsum;    // 2 x ceil(n/kCdfTile) tile sums of the CDF build

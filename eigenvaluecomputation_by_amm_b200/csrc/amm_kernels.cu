@@ -288,8 +288,7 @@ __global__ void __launch_bounds__(1024) init_kernel(const __grid_constant__ Init
   if ((t & 31) == 0) ws[t >> 5] = ss;
   __syncthreads();
   if (t == 0) {
-    b.ticket[0] = 0u;  // the step kernels' last-CTA ticket and grid-barrier count
-    b.ticket[2] = 0u;
+    b.ticket[2] = 0u;  // the step kernels' grid-barrier count
     double s = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += ws[w];
     IterState st{};
