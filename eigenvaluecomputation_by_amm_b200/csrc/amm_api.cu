@@ -207,9 +207,7 @@ int run_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
     int rc = ensure_setup(ctx, s);
     if (rc) return rc;
   }
-  if (x0 != ctx->x0_buf)
-    AMM_CUDA(cudaMemcpyAsync(ctx->x0_buf, x0, sizeof(float) * ctx->cfg.m,
-                             cudaMemcpyDeviceToDevice, s));
+  if (x0 != ctx->x0_buf) AMM_CUDA(amm::launch_copy(ctx->x0_buf, x0, (int)ctx->cfg.m, s));
   ctx->last_cc = cc;
   ctx->last_step = cc.step;
   ctx->has_run = true;

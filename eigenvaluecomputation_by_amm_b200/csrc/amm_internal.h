@@ -170,6 +170,8 @@ cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, fl
                             cudaStream_t s);
 // Standalone helpers.
 cudaError_t launch_normalize(float* x, int m, cudaStream_t s);
+// Device-to-device copy of n floats by a kernel (a memcpy when unaligned).
+cudaError_t launch_copy(float* dst, const float* src, int n, cudaStream_t s);
 cudaError_t launch_clock(unsigned long long* out, cudaStream_t s);
 cudaError_t launch_rayleigh(const float* x_in, float* x_out, const float* y, const double* vstar,
                             int m, double* out3, cudaStream_t s);

@@ -728,6 +728,26 @@ cudaError_t launch_clock(unsigned long long* out, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// n floats (n % 4 == 0, both 16-byte aligned), as a programmatic dependent of the kernel before
+// it: a device copy that does not leave the chain of kernel launches
+__global__ void __launch_bounds__(256) copy4_kernel(float4* __restrict__ dst,
+                                                    const float4* __restrict__ src, int n4) {
+  griddep_wait();
+  griddep_launch_dependents();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+cudaError_t launch_copy(float* dst, const float* src, int n, cudaStream_t s) {
+  if ((n & 3) || ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15))
+    return cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+  const int n4 = n / 4;
+  int blocks = (n4 + 255) / 256;
+  if (blocks > 64) blocks = 64;
+  return launch_pdl(copy4_kernel, dim3(blocks), dim3(256), s, reinterpret_cast<float4*>(dst),
+                    reinterpret_cast<const float4*>(src), n4);
+}
+
 cudaError_t launch_normalize(float* x, int m, cudaStream_t s) {
   normalize_kernel<<<1, 512, 0, s>>>(x, m);
   count_launch();
