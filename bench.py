@@ -121,6 +121,12 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's own start-up (driver queries) must not overlap the timed solves: begin
+            # once it has delivered its first sample (it keeps sampling through the timed region)
+            t_end = time.time() + 3.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
+            time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
