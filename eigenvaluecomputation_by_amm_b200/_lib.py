@@ -57,6 +57,7 @@ class amm_batch_config(C.Structure):
         ("tile_gc", C.c_int32),
         ("c_divisor", C.c_int32),
         ("cluster", C.c_int32),
+        ("wide", C.c_int32),
     ]
 
 
@@ -117,6 +118,7 @@ _SIGS = {
     "amm_batch_run_each": [_P, _P, _P, _P, _P],
     "amm_batch_grad": [_P, _P, _P, _P, _P, _P],
     "amm_batch_tile_choice": [_P, _P, _P, _P],
+    "amm_batch_wide_plan": [_P, _P, _P, _P, _P],
     "amm_benchmark_product": [_P, C.c_int, C.c_int, _P, _P, _P],
     "amm_grad_lambda": [_P, _P, _P, _I64, _P],
     "amm_get_geometry": [_P, _P],

@@ -313,7 +313,8 @@ class BatchSolver:
 
     def __init__(self, mats, nvec: int = 8, max_iter: int = 500, tol: float = 1e-6,
                  rr_period: int = 1, seed: int = 1234, use_graph: bool = True, tile_gc: int = 0,
-                 c_divisor: int = 0, cluster: int = 0, device: Optional[int] = None):
+                 c_divisor: int = 0, cluster: int = 0, wide: int = 0,
+                 device: Optional[int] = None):
         self.lib = _lib.load()
         self.mats = list(mats)
         self.count = len(self.mats)
@@ -334,6 +335,7 @@ class BatchSolver:
         cfg.use_graph, cfg.tile_gc = (1 if use_graph else 0), int(tile_gc)
         cfg.c_divisor = int(c_divisor)
         cfg.cluster = int(cluster)
+        cfg.wide = int(wide)
         self._b = C.c_void_p()
         check(self.lib.amm_batch_create(C.byref(self._b), descs, self.count, C.byref(cfg),
                                         self.device), "amm_batch_create")
@@ -371,6 +373,17 @@ class BatchSolver:
         check(self.lib.amm_batch_tile_choice(self._b, C.byref(k), C.byref(gc), C.byref(cl)),
               "amm_batch_tile_choice")
         return int(k.value), int(gc.value), int(cl.value)
+
+    def wide_plan(self) -> dict:
+        """The autotuner's launch plan for uneven batches: the heaviest `count` matrices on a
+        first launch with clusters of `cluster` CTAs (`ctas` in all), the rest shared with a
+        second launch queued behind it; count 0 means one launch per run.  `ms`: the plan's time
+        in the autotuner (0 if it was not timed)."""
+        n, cl, g, ms = C.c_int32(0), C.c_int32(0), C.c_int32(0), C.c_float(0.0)
+        check(self.lib.amm_batch_wide_plan(self._b, C.byref(n), C.byref(cl), C.byref(g),
+                                           C.byref(ms)), "amm_batch_wide_plan")
+        return {"count": int(n.value), "cluster": int(cl.value), "ctas": int(g.value),
+                "ms": float(ms.value)}
 
     def close(self):
         if self._b:

@@ -80,8 +80,12 @@ def bench_batch(args):
                                   f"{args.iters} products per matrix, 8 vectors",
                       "total_bytes": bytes_per_product}}
     hbm, src = _peak()
-    for mode, cdiv in (("exact", 0), ("amm_c_n_over_8", 8)):
-        bs = BatchSolver(mats, nvec=8, max_iter=args.iters, tol=0.0, c_divisor=cdiv)
+    fix_gc, fix_cl = (int(v) for v in args.tiles.split(",")) if args.tiles else (0, 0)
+    modes = [(md, cd) for md, cd in (("exact", 0), ("amm_c_n_over_8", 8))
+             if md.split("_")[0] in args.modes.split(",")]
+    for mode, cdiv in modes:
+        bs = BatchSolver(mats, nvec=8, max_iter=args.iters, tol=0.0, c_divisor=cdiv,
+                         tile_gc=fix_gc, cluster=fix_cl)
         t_one = time_runs(bs, each=False)
         t_each = time_runs(bs, each=True)
         k, gc, cl = bs.tile_choice()
@@ -94,7 +98,8 @@ def bench_batch(args):
         res = {"matrices_per_s": args.count * 1000.0 / t_one, "ms_per_launch": t_one,
                "one_launch_per_matrix_matrices_per_s": args.count * 1000.0 / t_each,
                "ms_one_launch_per_matrix": t_each, "speedup_vs_launch_per_matrix": t_each / t_one,
-               "tile_cols_per_group": gc, "ctas_per_matrix": cl, "lambda_rel_err_max": max(errs),
+               "tile_cols_per_group": gc, "ctas_per_matrix": cl, "wide_plan": bs.wide_plan(),
+               "lambda_rel_err_max": max(errs),
                "lambda_rel_err_median": float(np.median(errs)), "checked": len(errs)}
         if cdiv == 0:
             ach = bytes_per_product * args.iters / (t_one * 1e-3) / 1e9
@@ -102,7 +107,7 @@ def bench_batch(args):
                                "frac": ach / hbm, "peak_source": src}
         out[mode] = res
         bs.close()
-    out["value"] = out["exact"]["matrices_per_s"]
+    out["value"] = out[modes[0][0]]["matrices_per_s"]
     print(json.dumps(out), flush=True)
 
 
@@ -158,6 +163,9 @@ def main():
     p.add_argument("--count", type=int, default=512)
     p.add_argument("--iters", type=int, default=20)
     p.add_argument("--check", type=int, default=32, help="matrices checked against FP64")
+    p.add_argument("--modes", default="exact,amm", help="batch products: exact, amm or both")
+    p.add_argument("--tiles", default="",
+                   help="fixed tile shape 'cols_per_group,ctas_per_matrix' (default: autotuned)")
     args = p.parse_args()
     for w in args.which.split(","):
         {"batch": bench_batch, "grad": bench_grad}[w](args)

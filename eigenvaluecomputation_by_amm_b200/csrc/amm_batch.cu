@@ -56,15 +56,16 @@ struct Mat {
 
 struct Args {
   const Mat* mats;
-  const int32_t* order;  // processing order (largest first)
+  const int32_t* order;  // processing order (largest first), shared by the launches of a run
   int32_t count;
   int32_t max_iter;
   double tol;
   int32_t rr_period;
-  int32_t pad;
+  int32_t count0;        // matrices of this launch's own list, taken before the shared one
+  const int32_t* order0;
   uint64_t seed;
   uint32_t* states;  // AMM mode: xorshift32 states of every matrix (advanced in place)
-  uint32_t* queue;  // [0]: next work item; zero before the launch
+  uint32_t* queue;  // [0]: next item of the shared list, [1]: of the own list; zero at the start
   double* lam;      // count x K Ritz values, descending ([0] = λ_max)
   float* vec;       // Σ m: v of each matrix (top Ritz vector, unit)
   int32_t* iters;   // iterations run (-1: rank-deficient block, no result)
@@ -397,14 +398,32 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   const int CL = (int)cluster.num_blocks();   // CTAs sharing one matrix
   const int crank = (int)cluster.block_rank();
   const bool writer = (crank == 0);           // rank 0 writes the results
+  // a launch queued behind this one as a programmatic dependent may now take the SMs left
+  griddep_launch_dependents();
   for (;;) {
-    // rank 0 takes the next matrix from the queue; the cluster reads it from rank 0
-    if (writer && t == 0) ctl[0] = (int)atomicAdd(a.queue, 1u);
+    // rank 0 takes the next matrix, from this launch's own list first, then from the list it
+    // shares with the other launch of the run; the cluster reads it from rank 0
+    if (writer && t == 0) {
+      int next = -1;
+      if (a.count0 > 0) {
+        const uint32_t k = atomicAdd(a.queue + 1, 1u);
+        if (k < (uint32_t)a.count0) next = a.order0[k];
+      }
+      if (next < 0) {
+        const uint32_t k = atomicAdd(a.queue, 1u);
+        if (k < (uint32_t)a.count) next = a.order[k];
+      }
+      ctl[0] = next;
+    }
     cluster.sync();
-    const int item = *cluster.map_shared_rank(&ctl[0], 0);
+    const int mi = *cluster.map_shared_rank(&ctl[0], 0);
     cluster.sync();
-    if (item >= a.count) return;
-    const int mi = a.order[item];
+    if (mi < 0) {
+      // a launch queued behind another (programmatic dependent) ends only after it, so that
+      // the work after it in the stream sees both; returns at once in any other launch
+      griddep_wait();
+      return;
+    }
     const Mat M = a.mats[mi];
     const int m = M.m, n = M.n;
     int P = 32;
@@ -918,6 +937,14 @@ struct amm_batch {
   int variant = -1;  // chosen tile shape (index into kVariants)
   int cluster = 1;   // CTAs per matrix (cluster size)
   int grid = 0;      // CTAs of the persistent launch for that cluster size
+  // The heaviest matrices on a wide-cluster launch (wide_count 0: one launch per run): it takes
+  // the first wide_count matrices of the order on clusters of wide_cluster CTAs, then joins
+  // the launch queued behind it (clusters of `cluster`, narrow_grid CTAs) on the rest.
+  int wide_count = 0;
+  int wide_cluster = 0;
+  int wide_grid = 0;
+  int narrow_grid = 0;
+  float wide_ms = 0.f;   // the plan's time in the autotuner (0: not timed)
   std::map<std::pair<int, int>, float> tune_ms;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -950,9 +977,9 @@ struct Guard {
   }
 };
 
-// CTAs of a persistent launch with clusters of cl CTAs: as many clusters as fit at once (one
-// CTA per SM), and no more than there are matrices.  0 if that cluster size cannot run.
-int persistent_grid(amm_batch* b, int variant, int cl) {
+// Clusters of cl CTAs of the given tile shape that are resident at once (one CTA per SM); 0 if
+// that cluster size cannot run.
+int max_clusters(amm_batch* b, int variant, int cl) {
   const auto& V = amm::batch::kVariants[variant];
   const int sm = amm::batch::smem_bytes(V.K, b->amm);
   if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
@@ -976,13 +1003,34 @@ int persistent_grid(amm_batch* b, int variant, int cl) {
     cudaGetLastError();
     return 0;
   }
+  return nclusters > 0 ? nclusters : 0;
+}
+
+// CTAs of a persistent launch with clusters of cl CTAs: as many clusters as fit at once, and
+// no more than there are matrices.  0 if that cluster size cannot run.
+int persistent_grid(amm_batch* b, int variant, int cl) {
+  const int nclusters = max_clusters(b, variant, cl);
   if (nclusters < 1) return 0;
   const int64_t use = std::min<int64_t>(nclusters, b->count);
   return (int)use * cl;
 }
 
-int launch(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_vec,
-           int32_t* d_iters, int max_iter, const int32_t* order, int count, cudaStream_t s) {
+// Start of a run: both work-list counters zeroed and, in AMM mode, the seeded states restored
+// (every run draws the same picks).
+int run_prologue(amm_batch* b, cudaStream_t s) {
+  BATCH_CUDA(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(uint32_t), s));
+  if (b->amm)
+    BATCH_CUDA(cudaMemcpyAsync(b->d_states, b->d_states0, sizeof(uint32_t) * b->n_states,
+                               cudaMemcpyDeviceToDevice, s));
+  return AMM_OK;
+}
+
+// One persistent launch over the shared list (order, count), after its own list (order0,
+// count0).  dependent: launched as a programmatic dependent of the launch before it in the
+// stream, so that it starts on the SMs that launch leaves free.
+int launch_kernel(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_vec,
+                  int32_t* d_iters, int max_iter, const int32_t* order, int count,
+                  const int32_t* order0, int count0, bool dependent, cudaStream_t s) {
   const auto& V = amm::batch::kVariants[variant];
   const int sm = amm::batch::smem_bytes(V.K, b->amm);
   BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -992,6 +1040,8 @@ int launch(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_
   a.mats = b->d_mats;
   a.order = order;
   a.count = count;
+  a.order0 = order0;
+  a.count0 = count0;
   a.max_iter = max_iter;
   a.tol = b->cfg.tol;
   a.rr_period = b->cfg.rr_period > 0 ? b->cfg.rr_period : 1;
@@ -1001,26 +1051,98 @@ int launch(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_
   a.lam = d_lam;
   a.vec = d_vec;
   a.iters = d_iters;
-  BATCH_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(uint32_t), s));
-  if (b->amm)  // every run draws from the seeded states
-    BATCH_CUDA(cudaMemcpyAsync(b->d_states, b->d_states0, sizeof(uint32_t) * b->n_states,
-                               cudaMemcpyDeviceToDevice, s));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(amm::batch::kThreads, 1, 1);
   cfg.dynamicSmemBytes = sm;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = cl;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = dependent ? 2 : 1;
   BATCH_CUDA(cudaLaunchKernelEx(&cfg, V.fn, a));
   amm::count_launch(1);
   BATCH_CUDA(cudaGetLastError());
   return AMM_OK;
+}
+
+// A run as one launch over the order list (or a slice of it).
+int launch(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_vec,
+           int32_t* d_iters, int max_iter, const int32_t* order, int count, cudaStream_t s) {
+  const int rc = run_prologue(b, s);
+  if (rc) return rc;
+  return launch_kernel(b, variant, cl, grid, d_lam, d_vec, d_iters, max_iter, order, count,
+                       nullptr, 0, false, s);
+}
+
+// A run with the wide-cluster plan: the wide launch takes the heaviest matrices first, the
+// launch queued behind it (programmatic dependent) takes the SMs left, and both share the rest
+// of the order list.
+int launch_wide(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, int max_iter,
+                cudaStream_t s) {
+  int rc = run_prologue(b, s);
+  if (rc) return rc;
+  const int32_t* rest = b->d_order + b->wide_count;
+  const int nrest = (int)b->count - b->wide_count;
+  rc = launch_kernel(b, b->variant, b->wide_cluster, b->wide_grid, d_lam, d_vec, d_iters,
+                     max_iter, rest, nrest, b->d_order, b->wide_count, false, s);
+  if (rc) return rc;
+  return launch_kernel(b, b->variant, b->cluster, b->narrow_grid, d_lam, d_vec, d_iters,
+                       max_iter, rest, nrest, nullptr, 0, true, s);
+}
+
+// The run of the chosen plan.
+int launch_run(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaStream_t s) {
+  if (b->wide_count > 0) return launch_wide(b, d_lam, d_vec, d_iters, (int)b->cfg.max_iter, s);
+  return launch(b, b->variant, b->cluster, b->grid, d_lam, d_vec, d_iters,
+                (int)b->cfg.max_iter, b->d_order, (int)b->count, s);
+}
+
+// Wide-cluster plan for a batch of uneven matrices.  With one cluster size for all, a matrix
+// whose work alone, on one cluster, exceeds an even share of the whole batch per cluster sets
+// the run's time (the queue hands it out first, but nothing can help with it).  Those leading
+// matrices of the order go to a launch with clusters large enough for the heaviest (the next
+// sizes up, at most 8) on at most half the SMs; it then helps with the rest.  Needs
+// programmatic dependent launch (both launches resident at once).  With the default setting
+// (wide = 0) only for an autotuned cluster size; wide = 1 plans it for a fixed one too, and
+// wide = -1 never.
+void plan_wide(amm_batch* b) {
+  b->wide_count = 0;
+  if (!amm::pdl_enabled() || b->cfg.wide < 0 || b->count < 2) return;
+  if (b->cfg.cluster > 0 && b->cfg.wide == 0) return;
+  double total = 0.0;
+  for (const Mat& x : b->mats) total += (double)x.m * (double)x.n;
+  // work per SM of an even split, with a margin: the per-CTA rate falls with the row count,
+  // so the heaviest matrices are also the slowest per element
+  const double share = 0.75 * total / (double)b->nsm;
+  auto work = [&](int k) { const Mat& x = b->mats[b->order[k]]; return (double)x.m * x.n; };
+  int nwide = 0;
+  while (nwide < b->count && work(nwide) > (double)b->cluster * share) ++nwide;
+  if (nwide == 0) return;
+  int wcl = 0;
+  for (int cl : amm::batch::kClusterSizes) {
+    if (cl <= b->cluster) continue;
+    wcl = cl;
+    if (work(0) <= (double)cl * share) break;
+  }
+  if (wcl == 0) return;
+  int nclusters = std::min(max_clusters(b, b->variant, wcl), (b->nsm / 2) / wcl);
+  nclusters = std::min(nclusters, nwide);
+  if (nclusters < 1) return;
+  const int wide_grid = nclusters * wcl;
+  int narrow = (b->nsm - wide_grid) / b->cluster;
+  narrow = std::min(narrow, max_clusters(b, b->variant, b->cluster));
+  narrow = (int)std::min<int64_t>(narrow, b->count - nwide);
+  if (narrow < 1) return;
+  b->wide_count = nwide;
+  b->wide_cluster = wcl;
+  b->wide_grid = wide_grid;
+  b->narrow_grid = narrow * b->cluster;
 }
 
 // Tile-shape autotuner: every (columns per group, cluster size) pair with the requested K runs
@@ -1050,6 +1172,7 @@ int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaSt
     b->variant = std::get<0>(cand[0]);
     b->cluster = std::get<1>(cand[0]);
     b->grid = std::get<2>(cand[0]);
+    plan_wide(b);  // only with wide = 1 (the cluster size is the caller's); untimed
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return AMM_OK;
@@ -1078,12 +1201,41 @@ int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaSt
       best_ms = ms;
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (best < 0) return AMM_ERR_UNSUPPORTED;
+  if (best < 0) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return AMM_ERR_UNSUPPORTED;
+  }
   b->variant = best;
   b->cluster = best_cl;
   b->grid = best_grid;
+  // the wide-cluster plan, kept only if it runs faster (same iterations, best of two), or
+  // untimed with wide = 1
+  plan_wide(b);
+  if (b->wide_count > 0 && b->cfg.wide == 0) {
+    const int iters = (int)std::min<int64_t>(b->cfg.max_iter, 20);
+    int rc = launch_wide(b, d_lam, d_vec, d_iters, iters, s);
+    float ms = 0.f;
+    for (int rep = 0; rc == AMM_OK && rep < 2; ++rep) {
+      BATCH_CUDA(cudaEventRecord(e0, s));
+      rc = launch_wide(b, d_lam, d_vec, d_iters, iters, s);
+      if (rc) break;
+      BATCH_CUDA(cudaEventRecord(e1, s));
+      BATCH_CUDA(cudaEventSynchronize(e1));
+      float t = 0.f;
+      BATCH_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      ms = rep == 0 ? t : std::min(ms, t);
+    }
+    b->wide_ms = ms;
+    if (rc || !(ms < best_ms)) b->wide_count = 0;
+    if (rc) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return rc;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return AMM_OK;
 }
 
@@ -1110,7 +1262,8 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   if (!out || !mats || !cfg || count < 1 || count > (1 << 20)) return AMM_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   if (cfg->nvec != 1 && cfg->nvec != 4 && cfg->nvec != 8) return AMM_ERR_UNSUPPORTED;
-  if (cfg->max_iter < 1 || !(cfg->tol >= 0.0) || cfg->rr_period < 0 || cfg->c_divisor < 0)
+  if (cfg->max_iter < 1 || !(cfg->tol >= 0.0) || cfg->rr_period < 0 || cfg->c_divisor < 0 ||
+      cfg->wide < -1 || cfg->wide > 1)
     return AMM_ERR_INVALID_ARGUMENT;
   const bool amm_mode = cfg->c_divisor > 0;
   int ndev = 0;
@@ -1245,9 +1398,7 @@ int amm_batch_run(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_i
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   int rc = autotune(b, d_lambda, d_vectors, d_iters, s);
   if (rc) return rc;
-  if (!b->cfg.use_graph)
-    return launch(b, b->variant, b->cluster, b->grid, d_lambda, d_vectors, d_iters,
-                  (int)b->cfg.max_iter, b->d_order, (int)b->count, s);
+  if (!b->cfg.use_graph) return launch_run(b, d_lambda, d_vectors, d_iters, s);
   if (b->gexec && (b->g_lam != d_lambda || b->g_vec != d_vectors || b->g_iters != d_iters)) {
     cudaGraphExecDestroy(b->gexec);
     cudaGraphDestroy(b->graph);
@@ -1258,8 +1409,7 @@ int amm_batch_run(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_i
     if (!b->cap) BATCH_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
     BATCH_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed));
     const int64_t before = amm::launch_count();
-    rc = launch(b, b->variant, b->cluster, b->grid, d_lambda, d_vectors, d_iters,
-                (int)b->cfg.max_iter, b->d_order, (int)b->count, b->cap);
+    rc = launch_run(b, d_lambda, d_vectors, d_iters, b->cap);
     cudaGraph_t gr = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(b->cap, &gr);
     amm::count_launch(-(int)(amm::launch_count() - before));
@@ -1279,7 +1429,7 @@ int amm_batch_run(amm_batch* b, double* d_lambda, float* d_vectors, int32_t* d_i
     b->g_iters = d_iters;
   }
   BATCH_CUDA(cudaGraphLaunch(b->gexec, s));
-  amm::count_launch(1);
+  amm::count_launch(b->wide_count > 0 ? 2 : 1);
   return AMM_OK;
 }
 
@@ -1337,6 +1487,17 @@ int amm_batch_tile_choice(amm_batch* b, int32_t* k_out, int32_t* gc_out, int32_t
   *k_out = amm::batch::kVariants[b->variant].K;
   *gc_out = amm::batch::kVariants[b->variant].GC;
   if (cl_out) *cl_out = b->cluster;
+  return AMM_OK;
+}
+
+int amm_batch_wide_plan(amm_batch* b, int32_t* count, int32_t* cluster_size, int32_t* ctas,
+                        float* ms) {
+  if (!b || !count || !cluster_size || !ctas || !ms) return AMM_ERR_INVALID_ARGUMENT;
+  if (b->variant < 0) return AMM_ERR_NOT_READY;
+  *count = b->wide_count;
+  *cluster_size = b->wide_count > 0 ? b->wide_cluster : 0;
+  *ctas = b->wide_count > 0 ? b->wide_grid : 0;
+  *ms = b->wide_ms;
   return AMM_OK;
 }
 

@@ -184,5 +184,7 @@ cudaError_t launch_grad(const Buffers& b, const float* v, float* grad, int64_t l
 // Count of this library's launches (for the bench's gpu_launches field).
 void count_launch(int k = 1);
 int64_t launch_count();
+// Programmatic dependent launch in use (AMM_PDL=0 turns it off).
+bool pdl_enabled();
 
 }  // namespace amm

@@ -247,6 +247,9 @@ typedef struct amm_batch_config {
                       /* samples per step (n <= 8192, c <= 1024), drawn as pick_index does */
                       /* from a seeded xorshift32 state per sample, every run from the seed */
   int32_t cluster;    /* CTAs (a thread-block cluster) per matrix: 1, 2, 4, 8; 0 = autotune */
+  int32_t wide;       /* two-launch plan for uneven batches (amm_batch_wide_plan): 0 = with */
+                      /* an autotuned cluster size, kept if it times faster; 1 = whenever   */
+                      /* the batch is uneven enough, untimed; -1 = never                    */
 } amm_batch_config;
 
 void amm_batch_config_default(amm_batch_config *cfg);
@@ -274,6 +277,15 @@ int amm_batch_grad(amm_batch *b, const float *d_vectors, void *const *grad_ptrs,
  * (cluster size; cluster_size may be NULL).  AMM_ERR_NOT_READY before the first run. */
 int amm_batch_tile_choice(amm_batch *b, int32_t *nvec, int32_t *cols_per_group,
                           int32_t *cluster_size);
+/* The launch plan the autotuner kept for uneven batches (cluster size autotuned only): when a
+ * few matrices would each take longer on one cluster than the rest of the batch takes spread
+ * over the GPU, a run is two launches.  The first takes those *count heaviest matrices on
+ * clusters of *cluster_size CTAs (*ctas in all), the second is queued behind it as a
+ * programmatic dependent launch on the SMs left, and both then share the rest of the batch.
+ * *count = 0: one launch per run.  *ms: the plan's time in the autotuner (0 if not timed).
+ * AMM_ERR_NOT_READY before the first run. */
+int amm_batch_wide_plan(amm_batch *b, int32_t *count, int32_t *cluster_size, int32_t *ctas,
+                        float *ms);
 
 /* Measurement hook: time `reps` back-to-back launches of the fused product kernel for one
  * step kind (AMM_STEP_EXACT, AMM_STEP_PREVIOUS or AMM_STEP_PROPOSED) on the bound matrix,

@@ -56,6 +56,10 @@ def test_batch_config_validation(amm_lib):
     bad.nvec, bad.max_iter = 8, 0
     assert amm_lib.amm_batch_create(C.byref(b), mats, 1, C.byref(bad), 0) == \
         _lib.AMM_ERR_INVALID_ARGUMENT
+    bad.max_iter, bad.wide = 10, 2
+    assert amm_lib.amm_batch_create(C.byref(b), mats, 1, C.byref(bad), 0) == \
+        _lib.AMM_ERR_INVALID_ARGUMENT
+    assert cfg.wide == 0
 
 
 @pytest.mark.gpu
@@ -221,4 +225,50 @@ def test_batch_every_cluster_size_agrees(amm_lib, cluster):
     torch.cuda.synchronize()
     np.testing.assert_allclose(ga.lam[:, 0].cpu().numpy(), ra.lam[:, 0].cpu().numpy(), rtol=1e-4)
     for s in (ref, got, ra, ga):
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_wide_plan_agrees(amm_lib, use_graph):
+    """An uneven batch (one matrix holding most of the work) run as two launches — the heavy
+    matrix first on a wide cluster, the rest shared with a programmatic dependent launch queued
+    behind it — gives the λ of one launch per run (within 1e-5, exact mode; 1e-4 in AMM mode,
+    the same picks) and of FP64 LAPACK; the plan is reported by amm_batch_wide_plan."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver
+    sizes = [(1536, 4096)] + [(64 + 16 * k, 256 + 32 * k) for k in range(40)]
+    host = _mats(sizes, seed=41)
+    keep = [_device_col_major(A) for A in host]
+    mats = [v for _, v in keep]
+    one = BatchSolver(mats, nvec=8, max_iter=3000, tol=1e-6, tile_gc=4, cluster=2, wide=-1,
+                      use_graph=use_graph)
+    two = BatchSolver(mats, nvec=8, max_iter=3000, tol=1e-6, tile_gc=4, cluster=2, wide=1,
+                      use_graph=use_graph)
+    one.run()
+    two.run()
+    torch.cuda.synchronize()
+    assert one.wide_plan()["count"] == 0
+    plan = two.wide_plan()
+    assert plan["count"] >= 1 and plan["cluster"] > 2 and plan["ctas"] % plan["cluster"] == 0
+    np.testing.assert_allclose(two.lam[:, 0].cpu().numpy(), one.lam[:, 0].cpu().numpy(),
+                               rtol=1e-5)
+    assert (two.iters.cpu().numpy() > 0).all()
+    for i in (0, 1, 20, 40):
+        w, _ = _eigh_top(host[i])
+        assert abs(two.lam[i, 0].item() - w[0]) <= 1e-5 * w[0]
+    # a second run of the same context (queues and states reset by the run's prologue)
+    two.run()
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(two.lam[:, 0].cpu().numpy(), one.lam[:, 0].cpu().numpy(),
+                               rtol=1e-5)
+    ra = BatchSolver(mats, nvec=8, max_iter=6, tol=0.0, c_divisor=8, tile_gc=4, cluster=2,
+                     wide=-1, use_graph=use_graph)
+    ga = BatchSolver(mats, nvec=8, max_iter=6, tol=0.0, c_divisor=8, tile_gc=4, cluster=2,
+                     wide=1, use_graph=use_graph)
+    ra.run()
+    ga.run()
+    torch.cuda.synchronize()
+    assert ga.wide_plan()["count"] >= 1
+    np.testing.assert_allclose(ga.lam[:, 0].cpu().numpy(), ra.lam[:, 0].cpu().numpy(), rtol=1e-4)
+    for s in (one, two, ra, ga):
         s.close()
