@@ -445,7 +445,7 @@ def run_ours(args, rank, world):
     t_mix = (n_vr * t_ex16 + n_amm * t_amm) / launches_mix
     ach = bytes_mix / (t_mix * 1e-3) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "panel_traffic.json"
+    tf = ROOT / "profiles" / "step_kernel_bf16_16384x65536_traffic.json"
     if tf.exists():
         try:
             tj = json.loads(tf.read_text())
