@@ -119,6 +119,7 @@ _SIGS = {
     "amm_batch_grad": [_P, _P, _P, _P, _P, _P],
     "amm_batch_tile_choice": [_P, _P, _P, _P],
     "amm_batch_wide_plan": [_P, _P, _P, _P, _P],
+    "amm_probe_bounded_waits": [_P, _P, _P],
     "amm_benchmark_product": [_P, C.c_int, C.c_int, _P, _P, _P],
     "amm_grad_lambda": [_P, _P, _P, _I64, _P],
     "amm_get_geometry": [_P, _P],

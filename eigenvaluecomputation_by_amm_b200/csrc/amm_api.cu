@@ -655,6 +655,18 @@ int amm_device_clock(uint64_t* d_out, void* stream) {
   return AMM_OK;
 }
 
+int amm_probe_bounded_waits(amm_ctx* ctx, uint32_t* result3, void* stream) {
+  if (!ctx || !result3) return AMM_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(ctx->device);
+  cudaStream_t s = as_stream(stream);
+  uint32_t* dout = reinterpret_cast<uint32_t*>(ctx->b.partials);  // scratch between steps
+  AMM_CUDA(cudaMemsetAsync(ctx->b.ticket + 3, 0, sizeof(uint32_t), s));
+  AMM_CUDA(amm::launch_wait_probe(ctx->b.status, ctx->b.ticket + 3, dout, s));
+  AMM_CUDA(cudaMemcpyAsync(result3, dout, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  // the status word the step kernels set on a timeout: reported and cleared as after one
+  return read_status(ctx, s);
+}
+
 int amm_get_step_clocks(amm_ctx* ctx, uint64_t* out, int64_t cap, int64_t* count, void* stream) {
   if (!ctx || !out || cap < 1) return AMM_ERR_INVALID_ARGUMENT;
   if (!ctx->has_run) return AMM_ERR_NOT_READY;

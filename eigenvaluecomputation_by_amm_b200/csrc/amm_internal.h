@@ -106,7 +106,7 @@ struct Buffers {
   double2* colsum;     // n (Σa, Σa²) of each column from the set-up pass
   double* rpart;       // nsm x 4 (x·y, y·y, y·v*, z·dx) of each CTA
   uint32_t* ticket;    // [2]: grid-barrier arrivals of the step kernel and the set-up pass;
-                       // [0], [1], [3]: spare
+                       // [3]: the wait probe's barrier; [0], [1]: spare
   double* alpha2;      // ‖α‖²
   float* colvec;       // n floats of scratch (vᵀA for the gradient)
   double* cdf_tsum;    // 2 x ceil(n/kCdfTile) tile sums of the CDF build
@@ -173,6 +173,9 @@ cudaError_t launch_normalize(float* x, int m, cudaStream_t s);
 // Device-to-device copy of n floats by a kernel (a memcpy when unaligned).
 cudaError_t launch_copy(float* dst, const float* src, int n, cudaStream_t s);
 cudaError_t launch_clock(unsigned long long* out, cudaStream_t s);
+// The failure path of the bounded waits, on purpose (one CTA; out: 3 words, see the kernel).
+cudaError_t launch_wait_probe(uint32_t* status, uint32_t* counter, uint32_t* out,
+                              cudaStream_t s);
 cudaError_t launch_rayleigh(const float* x_in, float* x_out, const float* y, const double* vstar,
                             int m, double* out3, cudaStream_t s);
 cudaError_t launch_sample_only(const Buffers& b, int which, uint32_t* idx, cudaStream_t s);

@@ -722,6 +722,34 @@ cudaError_t launch_finalize(const Buffers& b, const CallCfg& cc, float* xdst, fl
 
 __global__ void clock_kernel(unsigned long long* out) { *out = globaltimer_ns(); }
 
+// The failure path of the library's bounded waits, run on purpose: one CTA waits on an mbarrier
+// that nothing arrives on, then on a grid barrier that counts one CTA more than the grid.  Each
+// wait gives up after kWaitLimitNs and the kernel records kDevTimeout in the status word, as the
+// step kernels do; out[0..1]: whether each wait completed (0: gave up), out[2]: µs spent.
+__global__ void wait_probe_kernel(uint32_t* status, uint32_t* counter, uint32_t* out) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const unsigned long long t0 = globaltimer_now();
+  const bool a = mbar_wait_bounded(&bar, 0u);
+  const bool g = grid_barrier(counter, gridDim.x + 1u);
+  out[0] = a ? 1u : 0u;
+  out[1] = g ? 1u : 0u;
+  out[2] = (uint32_t)((globaltimer_now() - t0) / 1000ull);
+  if (!a || !g) atomicOr(status, (uint32_t)kDevTimeout);
+}
+
+cudaError_t launch_wait_probe(uint32_t* status, uint32_t* counter, uint32_t* out,
+                              cudaStream_t s) {
+  wait_probe_kernel<<<1, 32, 0, s>>>(status, counter, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_clock(unsigned long long* out, cudaStream_t s) {
   clock_kernel<<<1, 1, 0, s>>>(out);
   count_launch();

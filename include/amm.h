@@ -312,6 +312,14 @@ int amm_grad_lambda(amm_ctx *ctx, const float *d_v, float *d_grad, int64_t ld_gr
  * the call's first kernel finished, [i + 1] when step i finished.  *count receives how many
  * were written. */
 int amm_device_clock(uint64_t *d_out, void *stream);
+/* Failure-path check of the device-side waits (no counterpart in the reference, which has no
+ * device-side error reporting): enqueues on `stream` a one-CTA kernel that waits on an mbarrier
+ * that nothing arrives on and on a grid barrier one CTA short, each giving up after the
+ * library's wait limit (2 s), and synchronises `stream`.  Returns AMM_ERR_DEVICE_TIMEOUT, the
+ * status of a step kernel whose wait gave up, with the HOST array result3 = {mbarrier wait
+ * completed, grid barrier completed, µs spent}; the status is cleared and the context stays
+ * usable. */
+int amm_probe_bounded_waits(amm_ctx *ctx, uint32_t *result3, void *stream);
 int amm_get_step_clocks(amm_ctx *ctx, uint64_t *out, int64_t cap, int64_t *count, void *stream);
 
 /* Launch geometry of the fused product kernel chosen for this context, 10 values:

@@ -350,3 +350,28 @@ def test_error_paths():
     with pytest.raises(AmmError) as e:
         ctx.trace()
     assert e.value.status == _lib.AMM_ERR_DEGENERATE
+
+
+def test_bounded_waits_give_up_and_the_context_stays_usable():
+    """The device-side waits are bounded: a kernel waiting on an mbarrier that nothing arrives
+    on and on a grid barrier one CTA short gives up after the wait limit (2 s each), the host
+    reads AMM_ERR_DEVICE_TIMEOUT, and the same context then solves as a fresh one does."""
+    import ctypes as C
+    from eigenvaluecomputation_by_amm_b200 import _lib
+    A = scaled_gaussian(256, 1024, seed=77, shift=0.1)
+    x0 = torch.from_numpy(np.random.default_rng(78).standard_normal(256).astype(np.float32)).cuda()
+    ref = ctx_for(A, c=128, step=6, vr_period=3)
+    ref.set_rng_state(tu32(states(128, 79)))
+    ref.power_method("proposed", x0)
+    want = ref.trace()["eigs"]
+    ctx = ctx_for(A, c=128, step=6, vr_period=3)
+    out = (C.c_uint32 * 3)()
+    rc = ctx.lib.amm_probe_bounded_waits(ctx._ctx, out, None)
+    assert rc == _lib.AMM_ERR_DEVICE_TIMEOUT
+    assert out[0] == 0 and out[1] == 0
+    assert 3.9e6 <= out[2] <= 30e6                      # two waits of 2 s, in µs
+    ctx.set_rng_state(tu32(states(128, 79)))
+    ctx.power_method("proposed", x0)
+    assert np.array_equal(ctx.trace()["eigs"], want)   # deterministic, as from a fresh context
+    ref.close()
+    ctx.close()
