@@ -199,6 +199,34 @@ def test_power_method_trace(method, kw, use_graph):
     assert vec_rel(x.cpu().numpy(), ref.x) < 1e-4
 
 
+EDGE_SHAPES = [(4, 1, 1), (8, 3, 5), (12, 37, 37), (1028, 513, 64), (16, 100003, 4096)]
+
+
+@pytest.mark.parametrize("m,n,c", EDGE_SHAPES)
+@pytest.mark.parametrize("method,kw", [("exact", dict()), ("previous", dict(vr_period=2)),
+                                       ("proposed", dict(vr_period=3)),
+                                       ("proposed_v2", dict(vr_period=2))])
+def test_power_method_edge_shapes(m, n, c, method, kw):
+    """One column, more picks than columns, ragged row and column counts, many short columns:
+    the trace (λ, kinds), the advanced states and the final vector against the oracle."""
+    step = 6
+    A = scaled_gaussian(m, n, seed=m * 7 + n, shift=0.05)
+    ctx = ctx_for(A, c=c, step=step, **kw)
+    st = states(c, m + n + c)
+    ctx.set_rng_state(tu32(st))
+    x0 = np.random.default_rng(m + 3).standard_normal(m).astype(np.float32)
+    ctx.power_method(method, t32(x0))
+    tr = ctx.trace()
+    ref = O.power_method(A, x0, method=method, step=step, c=c, states=st, **kw)
+    assert tr["steps_run"] == step
+    assert tr["kinds"] == ref.modes
+    assert np.all(rel(tr["eigs"], ref.eigs) < RTOL_LAMBDA_F32), (tr["eigs"], ref.eigs)
+    assert np.array_equal(np_u32(ctx.get_rng_state(c)), ref.states[:c])
+    x, _ = ctx.vectors()
+    assert vec_rel(x.cpu().numpy(), ref.x) < 1e-4
+    ctx.close()
+
+
 def test_adaptive_variance_reduction():
     m, n, c, step, thr = 512, 2048, 256, 24, 2e-3
     A = scaled_gaussian(m, n, seed=51)
