@@ -403,3 +403,56 @@ def test_bounded_waits_give_up_and_the_context_stays_usable():
     assert np.array_equal(ctx.trace()["eigs"], want)   # deterministic, as from a fresh context
     ref.close()
     ctx.close()
+
+
+_KNOB_SCRIPT = r"""
+import json, sys
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
+from helpers import scaled_gaussian, states
+from eigenvaluecomputation_by_amm_b200 import AMMContext, column_major
+A = scaled_gaussian(512, 2048, seed=91, shift=0.05)
+ctx = AMMContext(512, 2048, c=256, step=9, vr_period=4)
+ctx.set_matrix(column_major(torch.from_numpy(A).cuda()))
+ctx.set_rng_state(torch.from_numpy(states(256, 92).view(np.int32)).cuda())
+x0 = torch.from_numpy(np.random.default_rng(93).standard_normal(512).astype(np.float32)).cuda()
+ctx.power_method("proposed", x0)
+tr = ctx.trace()
+print(json.dumps({"eigs": tr["eigs"].tolist(), "kinds": tr["kinds"],
+                  "states": ctx.get_rng_state(256).cpu().numpy().view(np.uint32).tolist(),
+                  "geometry": ctx.geometry()}))
+"""
+
+
+@pytest.mark.parametrize("env", [{}, {"AMM_PDL": "0"}, {"AMM_PANEL_GC": "4"},
+                                 {"AMM_PANEL_STAGES": "4", "AMM_PDL": "0"}])
+def test_launch_knobs_agree(env):
+    """The environment knobs (no programmatic dependent launch, 4 instead of 8 columns per stage,
+    a shallower ring) change only the launch shape: the same picks and step kinds, λ within the
+    FP32 tolerance of the default configuration (run in separate processes: the knobs are read
+    once per process)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = str(Path(__file__).resolve().parents[1])
+
+    def run(extra):
+        e = dict(os.environ)
+        for k in ("AMM_PDL", "AMM_PANEL_GC", "AMM_PANEL_STAGES"):
+            e.pop(k, None)
+        e.update(extra)
+        r = subprocess.run([sys.executable, "-c", _KNOB_SCRIPT, root], env=e, capture_output=True,
+                           text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    base, got = run({}), run(env)
+    assert got["kinds"] == base["kinds"]
+    assert got["states"] == base["states"]
+    assert np.all(rel(got["eigs"], base["eigs"]) < RTOL_LAMBDA_F32)
+    if "AMM_PANEL_GC" in env:
+        assert got["geometry"]["cols_per_stage"] == int(env["AMM_PANEL_GC"])
+    if "AMM_PANEL_STAGES" in env:
+        assert got["geometry"]["stages"] == int(env["AMM_PANEL_STAGES"])
