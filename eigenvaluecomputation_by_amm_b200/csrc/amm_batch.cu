@@ -204,7 +204,8 @@ struct Smem {
   // byte offsets into dynamic shared memory, each 16-byte aligned
   static constexpr int yred = 0;                                         // float [4*kThreads][K]
   static constexpr int part = align16(yred + 4 * kThreads * K * 4);      // float [2][kWarps][32]
-  static constexpr int gpart = align16(part + 2 * kWarps * 32 * 4);      // double [kWarps][2*K*K]
+  static constexpr int bcast = align16(part + 2 * kWarps * 32 * 4);      // float [kWarps][32]
+  static constexpr int gpart = align16(bcast + kWarps * 32 * 4);         // double [kWarps][2*K*K]
   static constexpr int gram = align16(gpart + kWarps * 2 * K * K * 8);   // double G[K*K], H[K*K]
   static constexpr int vmat = align16(gram + 2 * K * K * 8);             // double V[K*K]
   static constexpr int rinv = align16(vmat + K * K * 8);                 // float Rinv[K*K]
@@ -375,6 +376,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   extern __shared__ __align__(16) unsigned char smem[];
   float* yred = reinterpret_cast<float*>(smem + SL::yred);
   float* part = reinterpret_cast<float*>(smem + SL::part);
+  float* bcast = reinterpret_cast<float*>(smem + SL::bcast);
   double* gpart = reinterpret_cast<double*>(smem + SL::gpart);
   double* Gm = reinterpret_cast<double*>(smem + SL::gram);
   double* Hm = Gm + K * K;
@@ -757,14 +759,18 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           }
         }
         const float red = team_allreduce<NV>(d, part, buf, warp, lane, P, team, team_warp0);
+        // the NV totals to every lane through this warp's shared-memory slot: one store and
+        // broadcast loads instead of NV shuffles (measured on the B200: 7 % off the batch)
+        float* bcw = bcast + warp * 32;
+        __syncwarp();
+        if ((lane % (32 / NV)) == 0) bcw[lane / (32 / NV)] = red;
+        __syncwarp();
         if constexpr (K % 2 == 0) {
 #pragma unroll
           for (int c = 0; c < GC; ++c)
 #pragma unroll
             for (int vp = 0; vp < K / 2; ++vp) {
-              float2 tc = make_float2(
-                  __shfl_sync(0xffffffffu, red, (c * K + 2 * vp) * (32 / NV)),
-                  __shfl_sync(0xffffffffu, red, (c * K + 2 * vp + 1) * (32 / NV)));
+              float2 tc = *reinterpret_cast<const float2*>(bcw + c * K + 2 * vp);
               if (amm) tc = __fmul2_rn(tc, make_float2(wt[c], wt[c]));
               const float ae[4] = {av[c].x, av[c].y, av[c].z, av[c].w};
 #pragma unroll
@@ -780,7 +786,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           for (int c = 0; c < GC; ++c)
 #pragma unroll
             for (int v = 0; v < K; ++v) {
-              const float tc = __shfl_sync(0xffffffffu, red, (c * K + v) * (32 / NV)) * wt[c];
+              const float tc = bcw[c * K + v] * wt[c];
               Y[0][v] = fmaf(av[c].x, tc, Y[0][v]);
               Y[1][v] = fmaf(av[c].y, tc, Y[1][v]);
               Y[2][v] = fmaf(av[c].z, tc, Y[2][v]);
