@@ -185,3 +185,49 @@ def test_eigenfaces_shape_indices_bit_exact_vs_reference(kernel):
     short.power_method("previous", torch.from_numpy(x0s).cuda())
     picks = np.sort(short.sample_indices(0).cpu().numpy().view(np.uint32))
     assert np.array_equal(picks, ref["sorted"])
+
+
+@pytest.mark.parametrize("kernel,kw,steps", [("exact", {}, 6),
+                                             ("proposedAMM", dict(vr_period=6), 7)])
+def test_time_against_the_reference_driver(kernel, kw, steps):
+    """The reference's own driver (powerMethod_by_exact / _proposed, compiled for sm_100a, its
+    per-step host synchronisations included, its column norms computed before the timed call)
+    against libamm's call (its set-up pass included) on the same symmetric 16384 x 16384 FP32
+    matrix, c = 4096: libamm is faster with FP32 storage; the BF16 time is reported beside it."""
+    import json
+    from eigenvaluecomputation_by_amm_b200 import AMMContext, column_major
+    m, c = 16384, 4096
+    rng = np.random.default_rng(12)
+    B = rng.standard_normal((m, m), dtype=np.float32)
+    B *= np.exp(rng.standard_normal(m)).astype(np.float32)[None, :]
+    A = B + B.T
+    del B
+    st = rng.integers(1, 2**32, size=m, dtype=np.uint64).astype(np.uint32)
+    ref_ms = min(float(R.power_method(kernel, A, 1276, st, c=c, step=steps, **kw)["time_ms"][0])
+                 for _ in range(2))
+    x0 = torch.from_numpy(R.draw_x0(m, 1276)).cuda()
+    tA = torch.from_numpy(A).cuda()
+    got = {}
+    for dtype in ("f32", "bf16"):
+        Ad = column_major(tA if dtype == "f32" else tA.to(torch.bfloat16))
+        ctx = AMMContext(m, m, c=c, step=steps, dtype=dtype, **kw)
+        ts = []
+        for r in range(4):
+            ctx.set_rng_state(tu32(st[:c]))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            ctx.set_matrix(Ad)
+            ctx.power_method(KERNEL_TO_METHOD[kernel], x0)
+            e1.record()
+            e1.synchronize()
+            if r:
+                ts.append(e0.elapsed_time(e1))
+        assert np.all(np.isfinite(ctx.trace()["eigs"]))
+        got[dtype] = min(ts)
+        ctx.close()
+    print(json.dumps({"kernel": kernel, "m": m, "c": c, "steps": steps, "reference_ms": ref_ms,
+                      "libamm_f32_ms": got["f32"], "libamm_bf16_ms": got["bf16"],
+                      "speedup_f32": ref_ms / got["f32"], "speedup_bf16": ref_ms / got["bf16"]}))
+    assert got["f32"] < ref_ms
