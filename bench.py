@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-c-big", action="store_true", help="skip the 4c sample-count report")
+    p.add_argument("--no-small", action="store_true", help="skip the 1024x4096 exact report")
     p.add_argument("--trace-out", default=None, help="write the calibration λ traces (JSON)")
     p.add_argument("--seeds", type=int, default=5, help="sampling-state seeds for calibration")
     return p.parse_args()
@@ -497,6 +498,56 @@ def run_ours(args, rank, world):
                                                        else None)}
             cbx.close()
 
+    # ---- the reference's CPU-checkable size, 1024 x 4096 FP32 exact (A = N(0,1) x lognormal(0,1)
+    # column scales from seed 0, x0 from seed 1), stopped at |Δλ|/λ <= 1e-6 or 200 steps: the
+    # GPU solve beside the CPU baselines (LAPACK eigh of C = A·Aᵀ in FP64, as the reference's
+    # calculate_largest_eigenvalue.py does, and the numpy FP32 power method) ----
+    small = None
+    if rank == 0 and not args.no_small:
+        from eigenvaluecomputation_by_amm_b200 import column_major
+        m1, n1 = 1024, 4096
+        g1 = np.random.default_rng(0)
+        A1 = (g1.standard_normal((m1, n1)) * g1.lognormal(0.0, 1.0, n1)).astype(np.float32)
+        x1 = np.random.default_rng(1).standard_normal(m1).astype(np.float32)
+        c1x = AMMContext(m1, n1, step=200, tol=1e-6, dtype="f32")
+        A1d = column_major(torch.from_numpy(A1).to(dev))
+        x1d = torch.from_numpy(x1).to(dev)
+        t1 = []
+        for r in range(6):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            c1x.set_matrix(A1d)
+            c1x.power_method("exact", x1d)
+            e1.record(stream)
+            e1.synchronize()
+            if r:
+                t1.append(e0.elapsed_time(e1))
+        tr1 = c1x.trace()
+        c1x.close()
+        t0 = time.perf_counter()
+        A64 = A1.astype(np.float64)
+        lam_eigh = float(np.linalg.eigvalsh(A64 @ A64.T)[-1])
+        eigh_ms = 1000.0 * (time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        xc = x1 / np.linalg.norm(x1)
+        lam_prev, lam_c, kc = 0.0, 0.0, 0
+        for kc in range(1, 201):
+            yc = A1 @ (A1.T @ xc)
+            lam_c = float(np.dot(xc.astype(np.float64), yc.astype(np.float64)))
+            xc = yc / np.linalg.norm(yc)
+            if kc > 1 and abs(lam_c - lam_prev) <= 1e-6 * abs(lam_c):
+                break
+            lam_prev = lam_c
+        cpu_pm_ms = 1000.0 * (time.perf_counter() - t0)
+        lam_gpu = float(tr1["eigs"][-1])
+        small = {"workload": "exact FP32, A 1024x4096, |Δλ|/λ <= 1e-6 or 200 steps",
+                 "gpu_ms": statistics.median(t1), "gpu_steps": int(tr1["steps_run"]),
+                 "gpu_rel_err_vs_eigh": abs(lam_gpu - lam_eigh) / lam_eigh,
+                 "cpu_eigh_ms": eigh_ms, "cpu_power_method_ms": cpu_pm_ms, "cpu_power_steps": kc,
+                 "cpu_threads": os.cpu_count()}
+
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -564,6 +615,7 @@ def run_ours(args, rank, world):
         "speedup_vs_exact_fp32": ms_exact / ms,
         "cublas_sgemv_fp32": blas,
         "c_large": c_big,
+        "small_exact_1024x4096": small,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "traffic": traffic, "peak_source": src,
                      "kernel": f"panel_kernel<bf16> step kernel, step mix of one solve "
