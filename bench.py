@@ -548,6 +548,43 @@ def run_ours(args, rank, world):
                  "cpu_eigh_ms": eigh_ms, "cpu_power_method_ms": cpu_pm_ms, "cpu_power_steps": kc,
                  "cpu_threads": os.cpu_count()}
 
+    # ---- the eigenfaces-sized configuration, 4096 x 16384 FP32 (64x64 synthetic images: the
+    # LFW data is not available), c = 1024, 300 steps of each method without variance
+    # reduction: steps/s and the λ error against LAPACK ----
+    faces = None
+    if rank == 0 and not args.no_small:
+        sys.path.insert(0, str(ROOT / "tests"))
+        from helpers import eigenfaces_like
+        from eigenvaluecomputation_by_amm_b200 import column_major
+        F = eigenfaces_like(16384, seed=3)
+        Fd = column_major(torch.from_numpy(F).to(dev))
+        F64 = Fd.double()
+        lam_f = float(torch.linalg.eigvalsh(F64 @ F64.t())[-1])
+        del F64
+        xf = torch.from_numpy(np.random.default_rng(4).standard_normal(4096).astype(np.float32)).to(dev)
+        faces = {"workload": "A 4096x16384 FP32 (64x64 synthetic faces), c = 1024, 300 steps, no VR"}
+        for meth in ("exact", "previous", "proposed"):
+            cf = AMMContext(4096, 16384, c=1024, step=300, dtype="f32")
+            tf_ = []
+            for r in range(3):
+                if meth != "exact":
+                    cf.seed_rng(11 + r)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                cf.set_matrix(Fd)
+                cf.power_method(meth, xf)
+                e1.record(stream)
+                e1.synchronize()
+                if r:
+                    tf_.append(e0.elapsed_time(e1))
+            lam_m = float(cf.trace()["eigs"][-1])
+            cf.close()
+            faces[meth] = {"ms": statistics.median(tf_), "steps_per_s": 300e3 / statistics.median(tf_),
+                           "rel_err_vs_eigh": abs(lam_m - lam_f) / lam_f}
+        del Fd
+
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -616,6 +653,7 @@ def run_ours(args, rank, world):
         "cublas_sgemv_fp32": blas,
         "c_large": c_big,
         "small_exact_1024x4096": small,
+        "faces_4096x16384": faces,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "traffic": traffic, "peak_source": src,
                      "kernel": f"panel_kernel<bf16> step kernel, step mix of one solve "
