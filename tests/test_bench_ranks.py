@@ -66,3 +66,27 @@ def test_trace_bytes():
     import bench
     # state + 7 steps of (λ, err, cos, kind, distinct) + 8 clock stamps + status
     assert bench.trace_d2h_bytes(7) == 56 + 7 * 32 + 64 + 4
+
+
+def test_reference_arm_json_line():
+    """`bench.py --impl reference` (the host-core arm) prints one JSON line with the contract's
+    keys, on a small matrix so that it runs in seconds on the CPU."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--m", "256",
+                        "--n", "1024", "--steps", "2", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=str(root))
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
