@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--no-small", action="store_true", help="skip the 1024x4096 exact report")
     p.add_argument("--trace-out", default=None, help="write the calibration λ traces (JSON)")
     p.add_argument("--seeds", type=int, default=5, help="sampling-state seeds for calibration")
+    p.add_argument("--heldout", type=int, default=16,
+                   help="sampling-state seeds, disjoint from the calibration ones, that the "
+                        "chosen schedule is checked and timed on")
     return p.parse_args()
 
 
@@ -177,18 +180,6 @@ def peaks():
 # ------------------------------------------------------------------------------------------
 # CPU exact power method (the oracle port of powerMethod_by_exact)
 # ------------------------------------------------------------------------------------------
-def cpu_exact_iter_time(At, x, iters=3):
-    """Seconds per x -> A(Aᵀx) on the host cores (numpy/BLAS, all threads), FP32."""
-    A = At.T                                # (m, n) column-major view
-    x = x / np.linalg.norm(x)
-    t0 = time.perf_counter()
-    for _ in range(iters):
-        t = A.T @ x
-        y = A @ t
-        x = y / np.linalg.norm(y)
-    return (time.perf_counter() - t0) / iters, x
-
-
 def cpu_exact_solve(At, x0, k):
     A = At.T
     x = x0 / np.linalg.norm(x0)
@@ -244,11 +235,14 @@ def run_reference(args, rank, world):
         t0 = time.perf_counter()
         cpu_exact_solve(At, x0, k)
         times.append(time.perf_counter() - t0)
-    ms = 1000.0 * max(times)
+    # a step's time is the mean of the K timed solves, as in our arm (the slowest beside it)
+    ms = 1000.0 * statistics.mean(times)
+    ms_max = 1000.0 * max(times)
     v = 1000.0 / ms
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "ms_per_step_max": ms_max,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"exact FP32 power method to 1e-3 on A {args.m}x{args.n} "
                                f"(N(0,1) x lognormal(0,1) columns + 30·u·wᵀ), {k} iterations, host cores",
@@ -276,10 +270,14 @@ def run_ours(args, rank, world):
     A32 = At_d.t()                                   # (m, n) column-major FP32
     A16 = At_d.to(torch.bfloat16).t()               # (m, n) column-major BF16
     x0 = torch.from_numpy(x0_h).to(dev)
-    # independent sampling-state seeds: the step count to 1e-3 must hold for every one of them
-    state_sets = [torch.from_numpy(np.random.default_rng(args.seed + 7 + k).integers(
-        1, 2**32, size=c, dtype=np.uint64).astype(np.uint32).view(np.int32)).to(dev)
-        for k in range(args.seeds)]
+    # independent sampling-state seeds: the schedule and its step count are chosen on the
+    # calibration seeds; the held-out seeds (a disjoint range) check it and are the ones timed
+    def seed_states(seed, count):
+        return torch.from_numpy(np.random.default_rng(seed).integers(
+            1, 2**32, size=count, dtype=np.uint64).astype(np.uint32).view(np.int32)).to(dev)
+
+    state_sets = [seed_states(args.seed + 7 + k, c) for k in range(args.seeds)]
+    heldout_sets = [seed_states(args.seed + 100_003 + k, c) for k in range(args.heldout)]
 
     # FP64 truth (torch, test infrastructure): power method on the FP32 matrix in FP64
     A64 = A32.double()
@@ -313,11 +311,12 @@ def run_ours(args, rank, world):
 
     stream = torch.cuda.current_stream()
 
-    def timed_solve(ctx, A, method, reps, warm, errs=None):
+    def timed_solve(ctx, A, method, reps, warm, errs=None, sets=None, clocks=None):
+        sets = state_sets if sets is None else sets
         ts = []
         for r in range(warm + reps):
             if method != "exact":
-                ctx.set_rng_state(state_sets[r % len(state_sets)])
+                ctx.set_rng_state(sets[r % len(sets)])
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
@@ -328,8 +327,13 @@ def run_ours(args, rank, world):
             e1.synchronize()
             if r >= warm:
                 ts.append(e0.elapsed_time(e1))
+                if errs is not None or clocks is not None:
+                    tr_ = ctx.trace()
                 if errs is not None:
-                    errs.append(abs(float(ctx.trace()["eigs"][-1]) - lam_true) / abs(lam_true))
+                    errs.append(abs(float(tr_["eigs"][-1]) - lam_true) / abs(lam_true))
+                if clocks is not None:
+                    clocks.append((tr_["kinds"], tr_["distinct"].tolist(),
+                                   ctx.step_clocks().astype(np.float64)))
         return ts
 
     # ---- exact FP32: steps to 1e-3 ----
@@ -384,19 +388,49 @@ def run_ours(args, rank, world):
     for z in cands[1:]:
         z[4].close()
 
+    # ---- the chosen schedule on the held-out seeds: its calibrated step count must reach 1e-3
+    # on seeds it was not chosen on; if one needs more steps, the solve takes that many ----
+    steps_calibrated = amm_steps
+    cal = AMMContext(m, n, c=c, step=args.max_amm_steps, dtype="bf16", **sched)
+    cal.set_matrix(A16)
+    held_ks, held_errs = [], []
+    for st_set in heldout_sets:
+        cal.set_rng_state(st_set)
+        cal.power_method("proposed", x0)
+        eigs = cal.trace()["eigs"]
+        held_ks.append(steps_to_tol(eigs, lam_true))
+        held_errs.append(abs(float(eigs[steps_calibrated - 1]) - lam_true) / abs(lam_true))
+    cal.close()
+    heldout = {"seeds": len(heldout_sets), "steps_calibrated": steps_calibrated,
+               "reached_1e-3_at_calibrated_steps": sum(e < TOL for e in held_errs) / len(held_errs),
+               "rel_err_max_at_calibrated_steps": max(held_errs),
+               "steps_needed_max": (None if any(k is None for k in held_ks)
+                                    else max(held_ks) + 1)}
+    if heldout["steps_needed_max"] is None:
+        raise RuntimeError("the chosen schedule did not reach 1e-3 on every held-out seed")
+    if heldout["steps_needed_max"] > amm_steps:
+        amm_steps = heldout["steps_needed_max"]
+        ctx.close()
+        ctx = AMMContext(m, n, c=c, step=amm_steps, dtype="bf16", **sched)
+        timed_solve(ctx, A16, "proposed", 1, 1, sets=heldout_sets)
+        n_vr = ctx.trace()["kinds"].count("exact")
+    heldout["steps_used"] = amm_steps
+
     # ---- timed region ----
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
     launches0 = _lib.launch_count()
     timed_errs = []
+    step_clocks = []
     with ClockSampler(dev.index) as clk:
-        ts = timed_solve(ctx, A16, "proposed", args.steps, args.warmup, timed_errs)
+        ts = timed_solve(ctx, A16, "proposed", args.steps, args.warmup, timed_errs,
+                         sets=heldout_sets, clocks=step_clocks)
         launches = (_lib.launch_count() - launches0) // (args.steps + args.warmup)
         # keep the GPU busy for the clock sampler (not timed)
         t_end = time.time() + 1.5
         while time.time() < t_end:
-            timed_solve(ctx, A16, "proposed", 1, 0)
+            timed_solve(ctx, A16, "proposed", 1, 0, sets=heldout_sets)
     tr = ctx.trace()
     lam_amm = float(tr["eigs"][-1])
     # a step is one solve: the K timed solves' mean device time (each solve is bracketed by a
@@ -405,11 +439,35 @@ def run_ours(args, rank, world):
     ms_max = max_over_ranks(max(ts), world, dev)
     value = world * 1000.0 / ms
 
-    # ---- roofline of the step kernel (live CUDA-event timing) ----
-    # The dominant kernel of a solve is the step kernel (product, grid-wide reduction and
-    # Rayleigh quotient in one launch): n_vr exact launches and amm_steps - n_vr AMM launches.
-    # Its achieved rate is the algorithmic bytes of that launch mix over its summed time.
+    # ---- roofline of the step kernel as it runs inside the timed solves ----
+    # The dominant kernel of a solve is the persistent step kernel: one launch runs every step
+    # of the solve (product, grid-wide reduction, Rayleigh quotient).  Its device clock stamps
+    # the end of each step, so steps 1 .. k-1 of every timed solve give the kernel's in-solve
+    # time (step 0's interval also holds the sampling launches before the step kernel).  Bytes
+    # are algorithmic: an exact step m·n·2 + 16·m, an AMM step m·c_d·2 + 8·c + 16·m with c_d its
+    # distinct columns.
     hbm, src = peaks()
+    ins_bytes = {"exact": 0.0, "amm": 0.0}
+    ins_ns = {"exact": 0.0, "amm": 0.0}
+    ins_steps = {"exact": 0, "amm": 0}
+    for kinds_, dist_, stamps_ in step_clocks:
+        for i in range(1, len(kinds_)):
+            dt = float(stamps_[i + 1] - stamps_[i])
+            if kinds_[i] == "exact":
+                key, b = "exact", m * n * 2 + 16 * m
+            else:
+                key, b = "amm", m * int(dist_[i]) * 2 + 8 * c + 16 * m
+            ins_bytes[key] += b
+            ins_ns[key] += dt
+            ins_steps[key] += 1
+    tot_b = ins_bytes["exact"] + ins_bytes["amm"]
+    tot_ns = ins_ns["exact"] + ins_ns["amm"]
+    ach = tot_b / tot_ns  # bytes per ns = GB/s
+    in_solve = {k: ({"steps": ins_steps[k], "ms_per_step": ins_ns[k] / ins_steps[k] / 1e6,
+                     "bytes_per_step": ins_bytes[k] / ins_steps[k],
+                     "achieved": ins_bytes[k] / ins_ns[k],
+                     "frac": ins_bytes[k] / ins_ns[k] / hbm} if ins_steps[k] else None)
+                for k in ("exact", "amm")}
     ctx.set_rng_state(state_sets[0])
     t_amm, cd = ctx.benchmark_product("proposed", reps=50)
     bytes_amm = m * cd * 2 + 8 * c + 16 * m
@@ -441,17 +499,17 @@ def run_ours(args, rank, world):
             "how": "y = A·(Aᵀx) as two torch.mv calls (cuBLAS) per iteration, 10 timed after 3 "
                    "warm-up; the fused exact kernel reads A once per iteration"}
     n_amm = amm_steps - n_vr
-    launches_mix = amm_steps
-    bytes_mix = (n_vr * bytes_ex16 + n_amm * bytes_amm) / launches_mix
-    t_mix = (n_vr * t_ex16 + n_amm * t_amm) / launches_mix
-    ach = bytes_mix / (t_mix * 1e-3) / 1e9
+    n_in = ins_steps["exact"] + ins_steps["amm"]
+    bytes_mix = tot_b / max(n_in, 1)
+    t_mix = tot_ns / max(n_in, 1) / 1e6
+    # DRAM traffic per step of the same mix, from the ncu capture of single-step launches
     traffic = None
     tf = ROOT / "profiles" / "step_kernel_bf16_16384x65536_traffic.json"
     if tf.exists():
         try:
             tj = json.loads(tf.read_text())
-            traffic = (n_vr * tj["exact_bf16_bytes_per_launch"]
-                       + n_amm * tj["proposed_bf16_c4096_bytes_per_launch"]) / launches_mix
+            traffic = (ins_steps["exact"] * tj["exact_bf16_bytes_per_launch"]
+                       + ins_steps["amm"] * tj["proposed_bf16_c4096_bytes_per_launch"]) / max(n_in, 1)
         except Exception:
             traffic = None
 
@@ -526,10 +584,24 @@ def run_ours(args, rank, world):
                 t1.append(e0.elapsed_time(e1))
         tr1 = c1x.trace()
         c1x.close()
-        t0 = time.perf_counter()
-        A64 = A1.astype(np.float64)
-        lam_eigh = float(np.linalg.eigvalsh(A64 @ A64.T)[-1])
-        eigh_ms = 1000.0 * (time.perf_counter() - t0)
+        # the reference's CPU script, calculate_largest_eigenvalue.py:1-13, restated step by
+        # step: C = A·Aᵀ written as square float32 matrix.dat (no header), read back with
+        # np.fromfile, widened to FP64 and diagonalised by LAPACK eigh (all eigenpairs), the
+        # largest and smallest eigenvalue taken; timed from the file read, and end to end from
+        # forming C
+        import tempfile
+        t_e2e = time.perf_counter()
+        C1 = (A1.astype(np.float64) @ A1.astype(np.float64).T).astype(np.float32)
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "matrix.dat")
+            C1.tofile(path)
+            t0 = time.perf_counter()
+            data = np.fromfile(path, dtype=np.float32)
+            size = int(np.sqrt(len(data)))
+            w_all, _ = np.linalg.eigh(data.reshape((size, size)).astype(np.float64))
+            lam_eigh = float(max(w_all))
+            eigh_ms = 1000.0 * (time.perf_counter() - t0)
+        eigh_e2e_ms = 1000.0 * (time.perf_counter() - t_e2e)
         t0 = time.perf_counter()
         xc = x1 / np.linalg.norm(x1)
         lam_prev, lam_c, kc = 0.0, 0.0, 0
@@ -545,7 +617,10 @@ def run_ours(args, rank, world):
         small = {"workload": "exact FP32, A 1024x4096, |Δλ|/λ <= 1e-6 or 200 steps",
                  "gpu_ms": statistics.median(t1), "gpu_steps": int(tr1["steps_run"]),
                  "gpu_rel_err_vs_eigh": abs(lam_gpu - lam_eigh) / lam_eigh,
-                 "cpu_eigh_ms": eigh_ms, "cpu_power_method_ms": cpu_pm_ms, "cpu_power_steps": kc,
+                 "cpu_eigh_ms": eigh_ms, "cpu_eigh_end_to_end_ms": eigh_e2e_ms,
+                 "cpu_eigh_how": "calculate_largest_eigenvalue.py's steps: matrix.dat (float32 C = "
+                                 "A·Aᵀ) read with np.fromfile, LAPACK eigh in FP64",
+                 "cpu_power_method_ms": cpu_pm_ms, "cpu_power_steps": kc,
                  "cpu_threads": os.cpu_count()}
 
     # ---- the eigenfaces-sized configuration, 4096 x 16384 FP32 (64x64 synthetic images: the
@@ -600,7 +675,7 @@ def run_ours(args, rank, world):
             e0.record(stream)
             A16_buf.copy_(A16_h, non_blocking=True)
             x0_buf.copy_(x0_pin, non_blocking=True)
-            ctx.set_rng_state(state_sets[r % len(state_sets)])
+            ctx.set_rng_state(heldout_sets[r % len(heldout_sets)])
             ctx.set_matrix(A16_buf.t())
             ctx.power_method("proposed", x0_buf)
             eig = ctx.trace()["eigs"][-1]          # D2H of the λ trace (synchronises)
@@ -618,12 +693,16 @@ def run_ours(args, rank, world):
     # ---- CPU baseline (oracle port of the exact power method, bounded sample) ----
     cpu = None
     if rank == 0 and not args.no_cpu:
-        t_it, _ = cpu_exact_iter_time(At, x0_h, iters=3)
-        cpu_ms = t_it * 1000.0 * exact_steps
+        cpu_exact_solve(At, x0_h, 1)  # warm the BLAS threads
+        tcs = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            cpu_exact_solve(At, x0_h, exact_steps)
+            tcs.append(1000.0 * (time.perf_counter() - t0))
+        cpu_ms = statistics.mean(tcs)
         cpu = {"value": 1000.0 / cpu_ms, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"3 iterations of x -> A(Aᵀx) on the full {m}x{n} FP32 matrix "
-                         f"(numpy, all host threads), scaled to the {exact_steps} iterations the exact "
-                         "method needs for 1e-3"}
+               "sample": f"3 full solves of the {exact_steps} iterations x -> A(Aᵀx) the exact method "
+                         f"needs for 1e-3, full {m}x{n} FP32 matrix (numpy, all host threads), mean"}
 
     if rank != 0:
         return
@@ -644,6 +723,7 @@ def run_ours(args, rank, world):
                                     else abs(lam_eigsh - lam_true) / abs(lam_true)),
         "rel_err": abs(lam_amm - lam_true) / abs(lam_true),
         "rel_err_max_timed": max(timed_errs), "calibration_seeds": len(state_sets),
+        "heldout": heldout,
         "iters_per_s": 1000.0 * amm_steps / ms,
         "exact_fp32": {"time_to_lambda_ms": ms_exact, "steps": exact_steps,
                        "iters_per_s": 1000.0 * exact_steps / ms_exact,
@@ -656,13 +736,17 @@ def run_ours(args, rank, world):
         "faces_4096x16384": faces,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "traffic": traffic, "peak_source": src,
-                     "kernel": f"panel_kernel<bf16> step kernel, step mix of one solve "
-                               f"({n_vr} exact + {n_amm} proposed AMM); each kind timed as "
-                               "single-step launches (in a solve the steps run back to back "
-                               "inside one persistent launch)",
-                     "bytes_per_launch": bytes_mix, "ms_per_launch": t_mix},
+                     "kernel": f"panel_kernel<bf16> persistent step kernel inside the timed "
+                               f"solves: steps 1..{amm_steps - 1} of each of the {len(step_clocks)} "
+                               f"solves ({ins_steps['exact']} exact + {ins_steps['amm']} proposed "
+                               "AMM steps), timed by the kernel's own device clock stamp at the "
+                               "end of every step",
+                     "bytes_per_launch": bytes_mix, "ms_per_launch": t_mix,
+                     "unit_of_work": "one step of the persistent launch",
+                     "in_solve": in_solve},
         "roofline_amm_step": {"achieved": ach_amm, "frac": ach_amm / hbm, "ms_per_launch": t_amm,
-                              "bytes_per_launch": bytes_amm, "distinct_columns": cd},
+                              "bytes_per_launch": bytes_amm, "distinct_columns": cd,
+                              "how": "single-step launches of the AMM step (benchmark_product)"},
         "roofline_exact_bf16": {"achieved": ach_ex16, "frac": ach_ex16 / hbm, "ms_per_launch": t_ex16},
         "roofline_setup_bf16": {"achieved": ach_setup, "frac": ach_setup / hbm,
                                 "ms_per_launch": t_setup},

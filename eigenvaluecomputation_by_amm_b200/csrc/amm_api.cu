@@ -407,7 +407,8 @@ int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   if (ctx->nsm < 1) ctx->nsm = 1;
   ctx->sanity_active = (cfg.sanity && cfg.c == cfg.n) ? 1 : 0;
-  if (!amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm, &ctx->geom)) {
+  if (!amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm, &ctx->geom) ||
+      !amm::panel_coresident(ctx->geom)) {
     delete ctx;
     cudaGetLastError();
     return AMM_ERR_UNSUPPORTED;

@@ -140,6 +140,9 @@ struct PanelGeom {
 };
 
 bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g);
+// One CTA of the step kernel and of the set-up pass fits on an SM with the geometry's
+// shared-memory carve (the persistent grids need every CTA resident at once).
+bool panel_coresident(const PanelGeom& g);
 
 // ---- launchers (amm_kernels.cu); each returns the cudaError_t of the launch ----
 // Set-up pass over A (amm_panel.cu): column statistics (α, ‖A_j‖, ‖A_j − α_j‖), z = A·α,

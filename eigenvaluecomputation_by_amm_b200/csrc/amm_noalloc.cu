@@ -17,14 +17,16 @@
 // device, two calls that overlap in time (different streams, or different host threads without
 // ordering) race on it and return garbage: serialise them.
 //
-// Launch sequence (stream-ordered on the caller's stream): clear -> draw -> tile sums ->
-// expand.  One set-up per device resolves the array's address with cudaGetSymbolAddress; that
-// first call on each device should come before any stream capture begins.
+// Launch sequence (stream-ordered on the caller's stream): clear -> draw -> tile prefix ->
+// expand.  The expansion is parallel over the c output positions (each finds its tile and then
+// its column by binary search), so a CDF that puts every pick on one column costs no more than
+// a spread one.  Every call resolves the array's device address with cudaGetSymbolAddress for
+// the current device (a lookup once the module is loaded; the first call on a device loads it,
+// so that first call should come before any stream capture begins).
 
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 
 #include "amm.h"
 #include "amm_device.cuh"
@@ -38,7 +40,6 @@ constexpr int kTileThreads = 256;
 constexpr int kTilePer = 4;                           // columns per thread
 constexpr int kTile = kTileThreads * kTilePer;        // columns per tile (one CTA)
 constexpr int kMaxTiles = kMaxColumns / kTile;        // 256
-constexpr int kMaxDevices = 64;
 
 struct NoAllocScratch {
   uint32_t count[kMaxColumns];  // multiplicity of each column among the c picks
@@ -87,75 +88,97 @@ __global__ void __launch_bounds__(kTileThreads) draw_kernel(NoAllocScratch* s,
   }
 }
 
-// Per tile: number of picks and number of distinct picked columns.
+// Per tile: number of picks and number of distinct picked columns; the multiplicities of the
+// tile become their inclusive prefix within the tile (in place), the expansion's search table.
 __global__ void __launch_bounds__(kTileThreads) tile_kernel(NoAllocScratch* s, int n) {
   __shared__ uint32_t scan[40];
   const int j0 = blockIdx.x * kTile + threadIdx.x * kTilePer;
+  uint32_t cnt[kTilePer];
   uint32_t sum = 0, nz = 0;
 #pragma unroll
   for (int e = 0; e < kTilePer; ++e) {
-    const uint32_t v = j0 + e < n ? s->count[j0 + e] : 0u;
-    sum += v;
-    nz += v ? 1u : 0u;
+    cnt[e] = j0 + e < n ? s->count[j0 + e] : 0u;
+    sum += cnt[e];
+    nz += cnt[e] ? 1u : 0u;
   }
   uint32_t tot_sum, tot_nz;
-  block_exclusive_scan(sum, scan, &tot_sum);
+  uint32_t run = block_exclusive_scan(sum, scan, &tot_sum);
   block_exclusive_scan(nz, scan, &tot_nz);
+#pragma unroll
+  for (int e = 0; e < kTilePer; ++e) {
+    run += cnt[e];
+    if (j0 + e < n) s->count[j0 + e] = run;
+  }
   if (threadIdx.x == 0) {
     s->tile_sum[blockIdx.x] = tot_sum;
     s->tile_nz[blockIdx.x] = tot_nz;
   }
 }
 
-// Per tile: its offset in the sorted output (picks of the tiles before it), then each picked
-// column j written count[j] times at its rank.  Tile 0 also writes the distinct count.
-__global__ void __launch_bounds__(kTileThreads) expand_kernel(NoAllocScratch* s, int n,
-                                                               uint32_t* out, int32_t* distinct) {
+// Output position p of the sorted picks (0 <= p < c) holds the column j whose picks cover it:
+// its tile is the last one whose first position is <= p (the exclusive prefix of the tile
+// totals, in shared memory), and within the tile the first column whose inclusive prefix
+// exceeds p's rank in the tile.  Block 0 also writes the number of distinct columns.
+__global__ void __launch_bounds__(kTileThreads) expand_kernel(NoAllocScratch* s, int n, int tiles,
+                                                               int c, uint32_t* out,
+                                                               int32_t* distinct) {
+  __shared__ uint32_t first[kMaxTiles + 1];
   __shared__ uint32_t scan[40];
   const int t = threadIdx.x;
-  uint32_t before = 0;
-  for (int k = t; k < (int)blockIdx.x; k += kTileThreads) before += s->tile_sum[k];
-  uint32_t base;
-  block_exclusive_scan(before, scan, &base);
-  if (blockIdx.x == 0) {
-    uint32_t nz = 0;
-    for (int k = t; k < (int)gridDim.x; k += kTileThreads) nz += s->tile_nz[k];
-    uint32_t total;
-    block_exclusive_scan(nz, scan, &total);
-    if (t == 0) *distinct = (int32_t)total;
-  }
-  const int j0 = blockIdx.x * kTile + t * kTilePer;
-  uint32_t cnt[kTilePer];
-  uint32_t sum = 0;
+  // exclusive prefix of the tile totals: kMaxTiles / kTileThreads tiles per thread, in order
+  constexpr int kPer = kMaxTiles / kTileThreads;
+  uint32_t v[kPer];
+  uint32_t sum = 0, nz = 0;
 #pragma unroll
-  for (int e = 0; e < kTilePer; ++e) {
-    cnt[e] = j0 + e < n ? s->count[j0 + e] : 0u;
-    sum += cnt[e];
+  for (int e = 0; e < kPer; ++e) {
+    const int k = t * kPer + e;
+    v[e] = k < tiles ? s->tile_sum[k] : 0u;
+    sum += v[e];
+    nz += k < tiles ? s->tile_nz[k] : 0u;
   }
-  uint32_t unused;
-  uint32_t pos = base + block_exclusive_scan(sum, scan, &unused);
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(sum, scan, &total);
 #pragma unroll
-  for (int e = 0; e < kTilePer; ++e)
-    for (uint32_t r = 0; r < cnt[e]; ++r) out[pos++] = (uint32_t)(j0 + e);
+  for (int e = 0; e < kPer; ++e) {
+    first[t * kPer + e] = run;
+    run += v[e];
+  }
+  if (t == 0) first[tiles] = total;
+  uint32_t dtot;
+  block_exclusive_scan(nz, scan, &dtot);  // ends with a barrier: `first` is complete
+  if (blockIdx.x == 0 && t == 0) *distinct = (int32_t)dtot;
+  for (int p = blockIdx.x * kTileThreads + t; p < c; p += gridDim.x * kTileThreads) {
+    int lo = 0, hi = tiles - 1;  // last tile with first[tile] <= p
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (first[mid] <= (uint32_t)p)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const uint32_t r = (uint32_t)p - first[lo];
+    const int c0 = lo * kTile;
+    const int cn = min(kTile, n - c0);
+    const uint32_t* pre = s->count + c0;
+    int a = 0, b = cn - 1;  // first column of the tile whose inclusive prefix exceeds r
+    while (a < b) {
+      const int mid = (a + b) >> 1;
+      if (pre[mid] <= r)
+        a = mid + 1;
+      else
+        b = mid;
+    }
+    out[p] = (uint32_t)(c0 + a);
+  }
 }
 
-std::mutex g_setup_mutex;
-NoAllocScratch* g_scratch_ptr[kMaxDevices] = {};
-
-// Address of g_scratch on the current device, resolved once per device.
+// Address of g_scratch on the current device (resolved on every call, so that a context torn
+// down and recreated, which reloads the module, never leaves a stale address behind).
 int scratch_for_current_device(NoAllocScratch** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return record_cuda_failure(e, "cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices) return AMM_ERR_UNSUPPORTED;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) return record_cuda_failure(e, "cudaGetSymbolAddress(g_scratch)");
-    g_scratch_ptr[dev] = static_cast<NoAllocScratch*>(p);
-  }
-  *out = g_scratch_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess) return record_cuda_failure(e, "cudaGetSymbolAddress(g_scratch)");
+  *out = static_cast<NoAllocScratch*>(p);
   return AMM_OK;
 }
 
@@ -188,7 +211,10 @@ extern "C" int amm_pick_sorted_noalloc(const uint32_t* d_states_in, uint32_t* d_
     draw_kernel<float><<<draw_blocks, kTileThreads, 0, st>>>(
         s, d_states_in, d_states_out, ci, static_cast<const float*>(d_cdf), ni);
   tile_kernel<<<tiles, kTileThreads, 0, st>>>(s, ni);
-  expand_kernel<<<tiles, kTileThreads, 0, st>>>(s, ni, d_idx_sorted, d_distinct);
+  int expand_blocks = (ci + kTileThreads - 1) / kTileThreads;
+  if (expand_blocks > 1024) expand_blocks = 1024;
+  expand_kernel<<<expand_blocks, kTileThreads, 0, st>>>(s, ni, tiles, ci, d_idx_sorted,
+                                                        d_distinct);
   count_launch(4);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return record_cuda_failure(e, "amm_pick_sorted_noalloc launch");

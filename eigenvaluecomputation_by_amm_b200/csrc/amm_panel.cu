@@ -1162,6 +1162,67 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   return b.smem_bytes <= 227 * 1024;
 }
 
+// ---- co-residency of the persistent grids ----
+// The step kernel and the set-up pass synchronise all their CTAs with grid barriers, so every
+// CTA of the grid (one per SM) must be resident at once.  panel_coresident checks at context
+// creation that one CTA of each variant fits on an SM with its shared-memory carve; at launch
+// the grids also carry the cooperative attribute, with which the runtime refuses a grid that
+// cannot be co-resident (fewer SMs available to this process, e.g. under an MPS thread limit)
+// instead of letting the barriers run into their time limit.  Whether the runtime accepts the
+// cooperative attribute beside programmatic stream serialization is probed once per device
+// with an empty kernel; where it does not, the step grids keep programmatic dependent launch
+// and rely on the creation-time check.
+__global__ void coop_probe_kernel() {}
+
+static int g_coop_pdl[64] = {};  // per device: 0 unknown, 1 accepted, 2 refused
+
+static bool coop_with_pdl() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  if (g_coop_pdl[dev] == 0) {
+    cudaStream_t ps = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) {
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(1);
+      cfg.blockDim = dim3(32);
+      cfg.stream = ps;
+      cudaLaunchAttribute at[2];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      at[1].id = cudaLaunchAttributeCooperative;
+      at[1].val.cooperative = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 2;
+      ok = cudaLaunchKernelEx(&cfg, coop_probe_kernel) == cudaSuccess;
+      ok = (cudaStreamSynchronize(ps) == cudaSuccess) && ok;
+      cudaStreamDestroy(ps);
+    }
+    cudaGetLastError();  // a refused launch leaves a (non-sticky) error behind
+    g_coop_pdl[dev] = ok ? 1 : 2;
+  }
+  return g_coop_pdl[dev] == 1;
+}
+
+bool panel_coresident(const PanelGeom& g) {
+  for (int setup = 0; setup < 2; ++setup) {
+    KernelFn fn;
+    int smem = 0;
+    if (configure(g, setup != 0, &fn, &smem) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, g.threads, (size_t)smem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (per_sm < 1) return false;
+  }
+  return true;
+}
+
 static cudaError_t launch_panel(const PanelArgs& a, bool setup, cudaStream_t s) {
   KernelFn fn;
   int smem = 0;
@@ -1169,16 +1230,26 @@ static cudaError_t launch_panel(const PanelArgs& a, bool setup, cudaStream_t s) 
   if (e != cudaSuccess) return e;
   // step grids: programmatic dependent launch (AMM_PDL=0 turns it off, for comparison)
   static const bool pdl = env_int("AMM_PDL", 1) != 0;
+  const bool dep = !setup && pdl;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(a.g.nclusters);
   cfg.blockDim = dim3(a.g.threads);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute at[2];
+  int na = 0;
+  if (dep) {
+    at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
+  }
+  if (!dep || coop_with_pdl()) {
+    at[na].id = cudaLaunchAttributeCooperative;
+    at[na].val.cooperative = 1;
+    ++na;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = (!setup && pdl) ? 1 : 0;
+  cfg.numAttrs = na;
   e = cudaLaunchKernelEx(&cfg, fn, a);
   count_launch();
   return e != cudaSuccess ? e : cudaGetLastError();

@@ -6,6 +6,10 @@
 Builds a context on a seeded N(0,1) x lognormal(0,1) matrix, runs one warm-up call (which also
 runs the set-up pass), then times `reps` launches of the product kernel per kind with CUDA
 events and prints the mean time and the algorithmic HBM rate per launch.
+
+This is the driver that the ncu captures summarised under profiles/ were taken with (each
+summary gives its exact command line); it ships with the package so that those commands run
+on any install, and the library itself never imports it.
 """
 from __future__ import annotations
 

@@ -24,7 +24,7 @@ def load():
     global _lib
     if _lib is None:
         if not LIB.exists():
-            raise FileNotFoundError(f"{LIB} not built (make -C oracle)")
+            raise FileNotFoundError(f"{LIB} not built (make -C oracle REF=<reference checkout>)")
         _lib = C.CDLL(str(LIB))
         P = C.c_void_p
         _lib.ref_draw_x0.argtypes = [C.c_int64, C.c_uint64, P]
