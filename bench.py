@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-c-big", action="store_true", help="skip the 4c sample-count report")
     p.add_argument("--no-small", action="store_true", help="skip the 1024x4096 exact report")
+    p.add_argument("--no-batch", action="store_true",
+                   help="skip the batched (512 matrices) and differentiation (64 x 512x2048) reports")
     p.add_argument("--trace-out", default=None, help="write the calibration λ traces (JSON)")
     p.add_argument("--seeds", type=int, default=5, help="sampling-state seeds for calibration")
     p.add_argument("--heldout", type=int, default=16,
@@ -660,6 +662,24 @@ def run_ours(args, rank, world):
                            "rel_err_vs_eigh": abs(lam_m - lam_f) / lam_f}
         del Fd
 
+    # ---- the batched configuration (512 FP32 matrices, 8 vectors, exact / AMM c = n/8 / AMM
+    # with variance reduction) and the differentiation configuration (64 x 512x2048 forward +
+    # backward), beside the headline; comparators give each matrix the whole GPU ----
+    c4 = c5 = None
+    if rank == 0 and not args.no_batch:
+        from eigenvaluecomputation_by_amm_b200 import bench_batch as BB
+        torch.cuda.empty_cache()
+        try:
+            c4 = BB.batch_report()
+        except Exception as exc:  # a report beside the headline, not the headline
+            c4 = {"error": repr(exc)}
+        torch.cuda.empty_cache()
+        try:
+            c5 = BB.grad_report()
+        except Exception as exc:
+            c5 = {"error": repr(exc)}
+        torch.cuda.empty_cache()
+
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -734,6 +754,8 @@ def run_ours(args, rank, world):
         "c_large": c_big,
         "small_exact_1024x4096": small,
         "faces_4096x16384": faces,
+        "c4_batch_512": c4,
+        "c5_grad_64x512x2048": c5,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "traffic": traffic, "peak_source": src,
                      "kernel": f"panel_kernel<bf16> persistent step kernel inside the timed "

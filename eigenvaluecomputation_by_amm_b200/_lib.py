@@ -58,6 +58,7 @@ class amm_batch_config(C.Structure):
         ("c_divisor", C.c_int32),
         ("cluster", C.c_int32),
         ("wide", C.c_int32),
+        ("vr_period", C.c_int32),
     ]
 
 
@@ -118,6 +119,8 @@ _SIGS = {
     "amm_batch_run_each": [_P, _P, _P, _P, _P],
     "amm_batch_grad": [_P, _P, _P, _P, _P, _P],
     "amm_batch_tile_choice": [_P, _P, _P, _P],
+    "amm_batch_record": [_P, _P, _P, _I64],
+    "amm_batch_set_matrices": [_P, C.POINTER(amm_batch_matrix), _I64, _P],
     "amm_batch_wide_plan": [_P, _P, _P, _P, _P],
     "amm_probe_bounded_waits": [_P, _P, _P],
     "amm_benchmark_product": [_P, C.c_int, C.c_int, _P, _P, _P],

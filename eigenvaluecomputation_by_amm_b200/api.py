@@ -307,13 +307,15 @@ class BatchSolver:
     stride(1) % 4 == 0, m_b <= 2048).  ``nvec`` vectors per matrix (1, 4 or 8) with
     Rayleigh–Ritz every ``rr_period`` products; iteration stops when the residual of the top
     Ritz pair ‖C·v − λ·v‖ is at most ``tol``·λ, or after ``max_iter`` products.  ``c_divisor`` k > 0 replaces the exact
-    product by the previous-AMM estimate with c = n/k sampled columns per step.  The tensors are
-    borrowed: keep them alive.
+    product by the previous-AMM estimate with c = n/k sampled columns per step; ``vr_period``
+    P > 0 then makes every P-th product (and the last) exact and memoised, the others
+    estimating C·X = Y_memo·S + Ĉ·(X − X_memo·S) with S = X_memoᵀX (variance reduction), and
+    convergence is tested on exact products only.  The tensors are borrowed: keep them alive.
     """
 
     def __init__(self, mats, nvec: int = 8, max_iter: int = 500, tol: float = 1e-6,
                  rr_period: int = 1, seed: int = 1234, use_graph: bool = True, tile_gc: int = 0,
-                 c_divisor: int = 0, cluster: int = 0, wide: int = 0,
+                 c_divisor: int = 0, cluster: int = 0, wide: int = 0, vr_period: int = 0,
                  device: Optional[int] = None):
         self.lib = _lib.load()
         self.mats = list(mats)
@@ -321,13 +323,7 @@ class BatchSolver:
         self.nvec = int(nvec)
         self.device = torch.cuda.current_device() if device is None else int(device)
         self._dev = torch.device("cuda", self.device)
-        descs = (_lib.amm_batch_matrix * self.count)()
-        for i, A in enumerate(self.mats):
-            if A.dtype != torch.float32 or A.dim() != 2 or A.stride(0) != 1:
-                raise ValueError("batch matrices must be column-major FP32 CUDA tensors")
-            descs[i].A = A.data_ptr()
-            descs[i].ld = A.stride(1) if A.shape[1] > 1 else max(A.shape[0], 4)
-            descs[i].m, descs[i].n = A.shape
+        descs = self._descs(self.mats)
         cfg = _lib.amm_batch_config()
         self.lib.amm_batch_config_default(C.byref(cfg))
         cfg.nvec, cfg.max_iter, cfg.tol = int(nvec), int(max_iter), float(tol)
@@ -336,6 +332,10 @@ class BatchSolver:
         cfg.c_divisor = int(c_divisor)
         cfg.cluster = int(cluster)
         cfg.wide = int(wide)
+        cfg.vr_period = int(vr_period)
+        self.vr_period = int(vr_period)
+        self.c_divisor = int(c_divisor)
+        self.max_iter = int(max_iter)
         self._b = C.c_void_p()
         check(self.lib.amm_batch_create(C.byref(self._b), descs, self.count, C.byref(cfg),
                                         self.device), "amm_batch_create")
@@ -347,6 +347,25 @@ class BatchSolver:
         self.vectors = torch.empty(int(offs[-1]), dtype=torch.float32, device=self._dev)
         self.iters = torch.empty(self.count, dtype=torch.int32, device=self._dev)
 
+    def _descs(self, mats):
+        descs = (_lib.amm_batch_matrix * len(mats))()
+        for i, A in enumerate(mats):
+            if A.dtype != torch.float32 or A.dim() != 2 or A.stride(0) != 1:
+                raise ValueError("batch matrices must be column-major FP32 CUDA tensors")
+            descs[i].A = A.data_ptr()
+            descs[i].ld = A.stride(1) if A.shape[1] > 1 else max(A.shape[0], 4)
+            descs[i].m, descs[i].n = A.shape
+        return descs
+
+    def set_matrices(self, mats, stream=None):
+        """Rebind to new matrices of the same shapes (amm_batch_set_matrices; stream-ordered).
+        The tile choice, the launch plan and the captured graph are kept."""
+        mats = list(mats)
+        descs = self._descs(mats)
+        check(self.lib.amm_batch_set_matrices(self._b, descs, len(mats), _stream(stream)),
+              "amm_batch_set_matrices")
+        self.mats = mats
+
     def run(self, each: bool = False, stream=None):
         """One persistent launch (or one launch per matrix with ``each``); asynchronous."""
         fn = self.lib.amm_batch_run_each if each else self.lib.amm_batch_run
@@ -357,15 +376,34 @@ class BatchSolver:
     def vector(self, i: int) -> torch.Tensor:
         return self.vectors[int(self.offsets[i]):int(self.offsets[i + 1])]
 
-    def grad(self, grads, scale: Optional[torch.Tensor] = None, stream=None):
-        """grads[b] <- scale_b · 2·v_b(v_bᵀA_b) (column-major tensors shaped like A_b)."""
+    def grad(self, grads, scale: Optional[torch.Tensor] = None, vectors=None, stream=None):
+        """grads[b] <- scale_b · 2·v_b(v_bᵀA_b) (column-major tensors shaped like A_b), with the
+        top vectors of the last run, or ``vectors`` (a copy of them) if given."""
         ptrs = (C.c_void_p * self.count)(*[g.data_ptr() for g in grads])
         lds = np.array([g.stride(1) if g.shape[1] > 1 else max(g.shape[0], 1) for g in grads],
                        np.int64)
         sc = None if scale is None else scale.to(device=self._dev, dtype=torch.float32).contiguous()
-        check(self.lib.amm_batch_grad(self._b, _ptr(self.vectors), ptrs,
+        vec = self.vectors if vectors is None else vectors
+        check(self.lib.amm_batch_grad(self._b, _ptr(vec), ptrs,
                                       lds.ctypes.data_as(C.c_void_p), _ptr(sc), _stream(stream)),
               "amm_batch_grad")
+        self._grad_keep = sc
+
+    def record(self, products: int):
+        """Record, on every later run, each matrix's FP32 sampling CDF and the raw picks of its
+        first ``products`` AMM products (amm_batch_record).  Returns (cdf, picks, offsets):
+        matrix b's CDF is cdf[col_off[b]:col_off[b+1]] and its picks of product p are
+        picks[st_off[b]*products + p*c_b :][:c_b], with offsets = (col_off, st_off, c)."""
+        cols = [int(A.shape[1]) for A in self.mats]
+        cs = [max(1, n // self.c_divisor) for n in cols] if self.c_divisor else [0] * len(cols)
+        col_off = np.concatenate([[0], np.cumsum(cols)]).astype(np.int64)
+        st_off = np.concatenate([[0], np.cumsum(cs)]).astype(np.int64)
+        self._rec_cdf = torch.zeros(int(col_off[-1]), dtype=torch.float32, device=self._dev)
+        self._rec_picks = torch.full((int(st_off[-1]) * int(products),), -1, dtype=torch.int32,
+                                     device=self._dev)
+        check(self.lib.amm_batch_record(self._b, _ptr(self._rec_cdf), _ptr(self._rec_picks),
+                                        int(products)), "amm_batch_record")
+        return self._rec_cdf, self._rec_picks, (col_off, st_off, np.array(cs, np.int64))
 
     def tile_choice(self):
         """(vectors, columns per group, CTAs per matrix) picked by the autotuner."""

@@ -6,6 +6,17 @@
 backward pass is libamm's kernel for ∂λ/∂A = 2·v(vᵀA) (``amm_batch_grad``), v being the unit
 top eigenvector of A_b·A_bᵀ that the forward pass returns.  The gradient formula holds for a
 simple top eigenvalue (a gap between λ_1 and λ_2).
+
+No copy of A is made when its rows are contiguous (a contiguous (B, m, n) tensor) and n <= 2048:
+the memory of a row-major m x n matrix is the column-major n x m matrix Aᵀ, and
+λ_max(AᵀA) = λ_max(AAᵀ).  The solver then runs on Aᵀ (top eigenvector u of AᵀA), and the same
+gradient kernel applied to the transposed problem, 2·u·(uᵀAᵀ), is (∂λ/∂A)ᵀ — whose column-major
+n x m layout is exactly the row-major m x n gradient (indeed ∂λ/∂A = 2·(A·u)·uᵀ).  Other inputs
+are copied into a column-major buffer first.
+
+One solver (batch context, tile choice) is kept per input shape and rebound to each call's
+matrices (``amm_batch_set_matrices``, stream-ordered), so a call allocates no device context and
+runs no autotuning after the first call of its shape.
 """
 from __future__ import annotations
 
@@ -17,8 +28,15 @@ from .api import BatchSolver
 
 __all__ = ["lambda_max", "LambdaMax"]
 
-# tile shape (columns per group, CTAs per matrix) picked by the autotuner, per batch shape
-_TILES: Dict[Tuple, int] = {}
+# one solver per (device, B, m, n, nvec, max_iter, tol, route)
+_SOLVERS: Dict[Tuple, BatchSolver] = {}
+
+
+def _route(A: torch.Tensor, nvec: int) -> str:
+    B, m, n = A.shape
+    if (A.is_contiguous() and nvec <= n <= 2048 and n % 4 == 0 and A.data_ptr() % 16 == 0):
+        return "transposed"
+    return "copy"
 
 
 def _column_major_batch(A: torch.Tensor) -> torch.Tensor:
@@ -30,6 +48,26 @@ def _column_major_batch(A: torch.Tensor) -> torch.Tensor:
     return buf
 
 
+def _views(A: torch.Tensor, route: str):
+    """The column-major matrices the solver runs on, and the storage they live in."""
+    B, m, n = A.shape
+    if route == "transposed":
+        return [A[b].t() for b in range(B)], A           # (n, m), stride (1, n): Aᵀ_b
+    buf = _column_major_batch(A)
+    return [buf[b].t()[:m] for b in range(B)], buf       # (m, n), stride (1, ld)
+
+
+def _solver(key, mats, max_iter, tol, nvec):
+    s = _SOLVERS.get(key)
+    if s is None:
+        # the first call of a shape autotunes the tile shape on its own batch (untimed after)
+        s = BatchSolver(mats, nvec=nvec, max_iter=max_iter, tol=tol, use_graph=False)
+        _SOLVERS[key] = s
+    else:
+        s.set_matrices(mats)
+    return s
+
+
 class LambdaMax(torch.autograd.Function):
     @staticmethod
     def forward(ctx, A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-6,
@@ -37,30 +75,36 @@ class LambdaMax(torch.autograd.Function):
         if not A.is_cuda or A.dtype != torch.float32 or A.dim() != 3:
             raise ValueError("lambda_max expects an FP32 CUDA tensor of shape (B, m, n)")
         B, m, n = A.shape
-        buf = _column_major_batch(A)
-        mats = [buf[b].t()[:m] for b in range(B)]            # (m, n) views, stride (1, ld)
-        key = (B, m, n, nvec)
-        gc, cl = _TILES.get(key, (0, 0))
-        solver = BatchSolver(mats, nvec=nvec, max_iter=max_iter, tol=tol, tile_gc=gc,
-                             cluster=cl, use_graph=False)
-        lam, _, iters = solver.run()
-        if key not in _TILES:
-            _TILES[key] = solver.tile_choice()[1:]
-        lam = lam.clone()
-        ctx.solver = solver
-        ctx.buf = buf
+        route = _route(A, nvec)
+        mats, store = _views(A, route)
+        key = (A.device.index, B, m, n, nvec, int(max_iter), float(tol), route)
+        solver = _solver(key, mats, max_iter, tol, nvec)
+        lam, vec, iters = solver.run()
+        ctx.key = key
+        ctx.mats = mats
+        ctx.store = store
+        ctx.vectors = vec.clone()      # a later forward of the same shape reuses the solver
         ctx.shape = (B, m, n)
+        ctx.route = route
+        lam, iters = lam.clone(), iters.clone()
         ctx.mark_non_differentiable(iters)
         return lam, iters
 
     @staticmethod
     def backward(ctx, g_lam, g_iters):
         B, m, n = ctx.shape
-        solver = ctx.solver
-        gbuf = torch.empty(B, n, ctx.buf.shape[2], dtype=torch.float32, device=ctx.buf.device)
+        solver = _SOLVERS[ctx.key]
+        solver.set_matrices(ctx.mats)  # this call's matrices (stream-ordered)
+        if ctx.route == "transposed":
+            # ∂λ/∂Aᵀ_b column-major (n x m, ld = n) is ∂λ/∂A_b row-major (m x n)
+            out = torch.empty(B, m, n, dtype=torch.float32, device=ctx.store.device)
+            grads = [out[b].t() for b in range(B)]
+            solver.grad(grads, scale=g_lam.to(torch.float32), vectors=ctx.vectors)
+            return out, None, None, None
+        ld = ctx.store.shape[2]
+        gbuf = torch.empty(B, n, ld, dtype=torch.float32, device=ctx.store.device)
         grads = [gbuf[b].t()[:m] for b in range(B)]
-        solver.grad(grads, scale=g_lam.to(torch.float32))
-        solver.close()
+        solver.grad(grads, scale=g_lam.to(torch.float32), vectors=ctx.vectors)
         return gbuf[:, :, :m].transpose(1, 2), None, None, None
 
 

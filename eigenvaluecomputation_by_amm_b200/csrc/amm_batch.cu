@@ -69,6 +69,19 @@ struct Args {
   double* lam;      // count x K Ritz values, descending ([0] = λ_max)
   float* vec;       // Σ m: v of each matrix (top Ritz vector, unit)
   int32_t* iters;   // iterations run (-1: rank-deficient block, no result)
+  // AMM mode with variance reduction: product p is exact, and memoised, when
+  // (p + 1) % vr_period == 0 and for the last product; the others estimate
+  // C·X = Y_memo·S + Ĉ·(X − X_memo·S), S = X_memoᵀ·X (0: no variance reduction)
+  int32_t vr_period;
+  int32_t vr_base;   // first slot of this launch's CTAs in vr_mem (the second launch of a run
+                     // is offset past the first one's CTAs)
+  float* vr_mem;     // per CTA slot: X_memo then Y_memo, kMaxRows x K floats each ([row][v])
+  // optional record for parity checks (null: none): each matrix's FP32 CDF at col_start[mi]
+  // and the raw picks of its AMM product p < rec_products at st_off·rec_products + p·c + k
+  float* rec_cdf;
+  uint32_t* rec_picks;
+  int32_t rec_products;
+  const int64_t* col_start;
 };
 
 // A shared-memory float4 load the compiler keeps in place (X is re-read per column group
@@ -220,7 +233,8 @@ struct Smem {
   static constexpr int lcol = align16(hist + kMaxCols * 4);            // int32 [kMaxPicks]
   static constexpr int lw = align16(lcol + kMaxPicks * 4);             // float [kMaxPicks]
   static constexpr int scan = align16(lw + kMaxPicks * 4);             // uint32 [40], double[32]
-  static constexpr int total_amm = align16(scan + 40 * 4 + 32 * 8);
+  static constexpr int svr = align16(scan + 40 * 4 + 32 * 8);           // float S[K*K] (VR)
+  static constexpr int total_amm = align16(svr + K * K * 4);
   static_assert(gpart % 8 == 0 && cs % 8 == 0 && xs % 16 == 0, "shared-memory alignment");
 };
 
@@ -253,9 +267,10 @@ template <int K>
 __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm, double* Hm,
                                        double* Vm, double* cs, double* ritz, float* Rinv,
                                        float* qv, int* ctl, double* scratch, int lane,
-                                       bool writer) {
+                                       bool writer, bool force_rr) {
   const bool first = (it == 0);
-  const bool rr = !first && ((K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter));
+  const bool rr = !first && ((K == 1) || ((it % a.rr_period) == 0) || (it >= a.max_iter) ||
+                             force_rr);
   if (rr) jacobi_warp<K>(Hm, Vm, cs, lane);
   // the Ritz values (lane 0: K entries)
   int st = 0;
@@ -393,6 +408,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   float* lw = reinterpret_cast<float*>(smem + SL::lw);
   uint32_t* scan = reinterpret_cast<uint32_t*>(smem + SL::scan);
   double* dscan = reinterpret_cast<double*>(smem + SL::scan + 40 * 4);
+  float* Svr = reinterpret_cast<float*>(smem + SL::svr);
 
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   namespace cg = cooperative_groups;
@@ -503,9 +519,17 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         pre += (double)nj;
         cdf[j] = (float)pre;  // in place: this thread alone reads and writes cdf[j0, j1)
         hist[j] = 0u;
+        if (a.rec_cdf && writer) a.rec_cdf[a.col_start[mi] + j] = cdf[j];
       }
       __syncthreads();
     }
+    // AMM mode with variance reduction: this CTA's memo slot (CTA-private: every thread reads
+    // back only the rows it wrote) and whether it holds an exact product of this matrix
+    const bool vr = amm && a.vr_period > 0;
+    float* Xm = a.vr_mem + (size_t)(a.vr_base + blockIdx.x) * (2 * kMaxRows * K);
+    float* Ym = Xm + kMaxRows * K;
+    bool memo = false;
+    bool prev_exact = false;  // the product the Ritz step of this iteration uses was exact
 
     // ---- start block X0 (hash), orthonormalised below like every later Y ----
     float Y[4][K];
@@ -571,7 +595,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       }
       // (gpart, summed into Gm and Hm above, is the Ritz step's scratch)
       if (warp == 0)
-        ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, gpart, lane, writer);
+        ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, gpart, lane, writer,
+                     vr && prev_exact);
       __syncthreads();
       if (ctl[2] && ctl[1] == 0) {
         // residual of the top Ritz pair, r = C·v − λ·v = (Y − λ·X)·q, over team 0's rows (FP64)
@@ -596,7 +621,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         if (t == 0) {
           double s = 0.0;
           for (int w = 0; w < kWarps; ++w) s += gpart[w];
-          const bool done = sqrt(s) <= a.tol * fabs(lam) || it >= a.max_iter;
+          // with variance reduction only an exact product's residual is the true one
+          const bool done = (sqrt(s) <= a.tol * fabs(lam) && (!vr || prev_exact)) ||
+                            it >= a.max_iter;
           if (done) {
             if (writer) {
               for (int i = 0; i < K; ++i) a.lam[(int64_t)mi * K + i] = ritz[i];
@@ -639,10 +666,16 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         }
       }
       __syncthreads();
+      // kind of product `it`: exact in exact mode; in AMM mode with variance reduction exact
+      // (and memoised) when (it + 1) % vr_period == 0 (powerMethod_by_previous.cuh:135-157)
+      // and for the last product, so that the reported Ritz values come from an exact product
+      const bool exact_p =
+          !amm || (vr && ((it + 1) % a.vr_period == 0 || it + 1 >= a.max_iter));
+      const bool wamm = amm && !exact_p;  // this product is sampled
       // ---- AMM: draw c columns (get_rand + pick_index, device_memory.h:506-545) and list the
       // distinct ones in ascending order with weight multiplicity / (c·p_j) ----
       int ncols = n;
-      if (amm) {
+      if (wamm) {
         const float total_f = cdf[n - 1];
         uint32_t* st = a.states + M.st_off;
         // every CTA of the cluster draws the same picks from the same states; rank 0 stores the
@@ -669,7 +702,10 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             else
               hi = mid;
           }
-          atomicAdd(&hist[lo < n ? lo : n - 1], 1u);
+          const int pick = lo < n ? lo : n - 1;
+          atomicAdd(&hist[pick], 1u);
+          if (a.rec_picks && writer && it < a.rec_products)
+            a.rec_picks[M.st_off * a.rec_products + (int64_t)it * M.c + k] = (uint32_t)pick;
         }
         __syncthreads();
         const int per = (n + kThreads - 1) / kThreads;
@@ -692,6 +728,48 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         ncols = (int)cd;
         __syncthreads();
       }
+      // ---- variance reduction: S = X_memoᵀ·X (FP64 sums over team 0's rows) and the block
+      // the sampled product multiplies, D = X − X_memo·S, into yred (free until the team sums
+      // after the product); Y_memo·S is added once the product is summed ----
+      const bool use_d = wamm && memo;
+      if (use_d) {
+        const int tw = P / 32;  // warps of team 0
+        if (warp < tw) {
+          for (int ab = 0; ab < K * K; ++ab) {
+            const int va = ab / K, vb = ab % K;
+            double sv = 0.0;
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              sv = fma((double)Xm[(r0 + e) * K + va], (double)Xs[xs_idx<K>(vb, r0 + e)], sv);
+            sv = warp_sum(sv);
+            if (lane == 0) gpart[warp * K * K + ab] = sv;
+          }
+        }
+        __syncthreads();
+        if (t < K * K) {
+          double sv = 0.0;
+          for (int w = 0; w < tw; ++w) sv += gpart[w * K * K + t];
+          Svr[t] = (float)sv;
+        }
+        __syncthreads();
+        if (team == 0) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            float xm[K];
+#pragma unroll
+            for (int v = 0; v < K; ++v) xm[v] = Xm[(r0 + e) * K + v];
+#pragma unroll
+            for (int vb = 0; vb < K; ++vb) {
+              float d = Xs[xs_idx<K>(vb, r0 + e)];
+#pragma unroll
+              for (int va = 0; va < K; ++va) d = fmaf(-xm[va], Svr[va * K + vb], d);
+              yred[xs_idx<K>(vb, r0 + e)] = d;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      const float* Xsrc = use_d ? yred : Xs;  // the block the product multiplies
       // ---- Y = C·X (or its AMM estimate): the fused pass over the columns (team-local) ----
 #pragma unroll
       for (int e = 0; e < 4; ++e)
@@ -707,8 +785,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         for (int c = 0; c < GC; ++c) {
           av[c] = make_float4(0.f, 0.f, 0.f, 0.f);
           wt[c] = 1.f;
-          const int col = (g0 + c < ncols) ? (amm ? lcol[g0 + c] : g0 + c) : -1;
-          if (amm && col >= 0) wt[c] = lw[g0 + c];
+          const int col = (g0 + c < ncols) ? (wamm ? lcol[g0 + c] : g0 + c) : -1;
+          if (wamm && col >= 0) wt[c] = lw[g0 + c];
           if (rows && col >= 0)
             av[c] = __ldcs(reinterpret_cast<const float4*>(Ab + (int64_t)col * M.ld));
           if (r0 + 1 >= m) av[c].y = 0.f;
@@ -730,8 +808,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           // packed FP32x2: a vector pair per instruction (X pairs interleaved in shared memory)
 #pragma unroll
           for (int vp = 0; vp < K / 2; ++vp) {
-            const float4 x01 = lds_f4(Xs + vp * 2 * kMaxRows + 2 * r0);      // rows 0, 1
-            const float4 x23 = lds_f4(Xs + vp * 2 * kMaxRows + 2 * r0 + 4);  // rows 2, 3
+            const float4 x01 = lds_f4(Xsrc + vp * 2 * kMaxRows + 2 * r0);      // rows 0, 1
+            const float4 x23 = lds_f4(Xsrc + vp * 2 * kMaxRows + 2 * r0 + 4);  // rows 2, 3
             const float2 xr[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
                                   make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
 #pragma unroll
@@ -747,7 +825,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         } else {
 #pragma unroll
           for (int v = 0; v < K; ++v) {
-            const float4 xv = lds_f4(Xs + v * kMaxRows + r0);
+            const float4 xv = lds_f4(Xsrc + v * kMaxRows + r0);
 #pragma unroll
             for (int c = 0; c < GC; ++c) {
               float s = av[c].x * xv.x;
@@ -771,7 +849,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
 #pragma unroll
             for (int vp = 0; vp < K / 2; ++vp) {
               float2 tc = *reinterpret_cast<const float2*>(bcw + c * K + 2 * vp);
-              if (amm) tc = __fmul2_rn(tc, make_float2(wt[c], wt[c]));
+              if (wamm) tc = __fmul2_rn(tc, make_float2(wt[c], wt[c]));
               const float ae[4] = {av[c].x, av[c].y, av[c].z, av[c].w};
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
@@ -846,6 +924,36 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         }
         cluster.sync();  // the buffers are rewritten by the next step
       }
+      // ---- variance reduction: Y = Y_memo·S + Ĉ·D for a sampled product; an exact product
+      // becomes the memo pair (team 0, its own rows, in every CTA of the cluster alike) ----
+      if (use_d && team == 0) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          float ym[K];
+#pragma unroll
+          for (int v = 0; v < K; ++v) ym[v] = Ym[(r0 + e) * K + v];
+#pragma unroll
+          for (int vb = 0; vb < K; ++vb) {
+            float acc = Y[e][vb];
+#pragma unroll
+            for (int va = 0; va < K; ++va) acc = fmaf(ym[va], Svr[va * K + vb], acc);
+            Y[e][vb] = acc;
+          }
+        }
+      }
+      if (vr && exact_p) {
+        if (team == 0) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int v = 0; v < K; ++v) {
+              Xm[(r0 + e) * K + v] = Xs[xs_idx<K>(v, r0 + e)];
+              Ym[(r0 + e) * K + v] = Y[e][v];
+            }
+        }
+        memo = true;
+      }
+      prev_exact = exact_p;
     }
     __syncthreads();
   }
@@ -940,6 +1048,11 @@ struct amm_batch {
   int64_t* d_grad_ld = nullptr;
   uint32_t* d_states0 = nullptr;  // seeded xorshift states (AMM mode), copied per run
   uint32_t* d_states = nullptr;
+  float* d_vr = nullptr;          // AMM mode with variance reduction: per-CTA memo pairs
+  // optional record of the CDFs and picks (amm_batch_record)
+  float* rec_cdf = nullptr;
+  uint32_t* rec_picks = nullptr;
+  int rec_products = 0;
   int variant = -1;  // chosen tile shape (index into kVariants)
   int cluster = 1;   // CTAs per matrix (cluster size)
   int grid = 0;      // CTAs of the persistent launch for that cluster size
@@ -1036,7 +1149,8 @@ int run_prologue(amm_batch* b, cudaStream_t s) {
 // stream, so that it starts on the SMs that launch leaves free.
 int launch_kernel(amm_batch* b, int variant, int cl, int grid, double* d_lam, float* d_vec,
                   int32_t* d_iters, int max_iter, const int32_t* order, int count,
-                  const int32_t* order0, int count0, bool dependent, cudaStream_t s) {
+                  const int32_t* order0, int count0, bool dependent, cudaStream_t s,
+                  int vr_base = 0) {
   const auto& V = amm::batch::kVariants[variant];
   const int sm = amm::batch::smem_bytes(V.K, b->amm);
   BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -1057,6 +1171,13 @@ int launch_kernel(amm_batch* b, int variant, int cl, int grid, double* d_lam, fl
   a.lam = d_lam;
   a.vec = d_vec;
   a.iters = d_iters;
+  a.vr_period = b->d_vr ? b->cfg.vr_period : 0;
+  a.vr_base = vr_base;
+  a.vr_mem = b->d_vr;
+  a.rec_cdf = b->rec_cdf;
+  a.rec_picks = b->rec_picks;
+  a.rec_products = b->rec_products;
+  a.col_start = b->d_col_start;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(amm::batch::kThreads, 1, 1);
@@ -1099,7 +1220,7 @@ int launch_wide(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, int
                      max_iter, rest, nrest, b->d_order, b->wide_count, false, s);
   if (rc) return rc;
   return launch_kernel(b, b->variant, b->cluster, b->narrow_grid, d_lam, d_vec, d_iters,
-                       max_iter, rest, nrest, nullptr, 0, true, s);
+                       max_iter, rest, nrest, nullptr, 0, true, s, b->wide_grid);
 }
 
 // The run of the chosen plan.
@@ -1261,6 +1382,8 @@ void amm_batch_config_default(amm_batch_config* c) {
   c->tile_gc = 0;
   c->c_divisor = 0;
   c->cluster = 0;
+  c->wide = 0;
+  c->vr_period = 0;
 }
 
 int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t count,
@@ -1269,7 +1392,7 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   *out = nullptr;
   if (cfg->nvec != 1 && cfg->nvec != 4 && cfg->nvec != 8) return AMM_ERR_UNSUPPORTED;
   if (cfg->max_iter < 1 || !(cfg->tol >= 0.0) || cfg->rr_period < 0 || cfg->c_divisor < 0 ||
-      cfg->wide < -1 || cfg->wide > 1)
+      cfg->wide < -1 || cfg->wide > 1 || cfg->vr_period < 0)
     return AMM_ERR_INVALID_ARGUMENT;
   const bool amm_mode = cfg->c_divisor > 0;
   int ndev = 0;
@@ -1333,6 +1456,11 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   const size_t o_gld = carve(sizeof(int64_t) * count, 256);
   const size_t o_st0 = carve(sizeof(uint32_t) * (nst > 0 ? nst : 1), 256);
   const size_t o_st = carve(sizeof(uint32_t) * (nst > 0 ? nst : 1), 256);
+  // memo pairs of the variance reduction: one slot per CTA that can be resident at once (the
+  // launches of a run hold at most one CTA per SM between them)
+  const bool with_vr = amm_mode && cfg->vr_period > 0;
+  const size_t vr_floats = (size_t)2 * amm::batch::kMaxRows * cfg->nvec;
+  const size_t o_vr = with_vr ? carve(sizeof(float) * vr_floats * b->nsm, 256) : 0;
   cudaError_t e = cudaMalloc(&b->mem, bytes);
   if (e != cudaSuccess) {
     delete b;
@@ -1347,6 +1475,7 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   b->d_grad_ld = reinterpret_cast<int64_t*>(base + o_gld);
   b->d_states0 = reinterpret_cast<uint32_t*>(base + o_st0);
   b->d_states = reinterpret_cast<uint32_t*>(base + o_st);
+  b->d_vr = with_vr ? reinterpret_cast<float*>(base + o_vr) : nullptr;
   std::vector<int64_t> cs((size_t)count + 1, 0);
   for (int64_t i = 0; i < count; ++i) cs[i + 1] = cs[i] + ms[i].n;
   e = cudaMemcpy(b->d_mats, ms.data(), sizeof(Mat) * count, cudaMemcpyHostToDevice);
@@ -1482,8 +1611,44 @@ int amm_batch_grad(amm_batch* b, const float* d_vectors, void* const* grad_ptrs,
   amm::batch::grad_kernel<<<(int)blocks, 256, 0, s>>>(a);
   amm::count_launch(1);
   BATCH_CUDA(cudaGetLastError());
-  // the pointer arrays are read by the kernel: keep the host copies alive until it has run
-  BATCH_CUDA(cudaStreamSynchronize(s));
+  // (the pointer arrays come from pageable host memory: the copies above were staged before
+  // they returned, so the caller's arrays may go at once)
+  return AMM_OK;
+}
+
+int amm_batch_set_matrices(amm_batch* b, const amm_batch_matrix* mats, int64_t count,
+                           void* stream) {
+  if (!b || !mats || count != b->count) return AMM_ERR_INVALID_ARGUMENT;
+  for (int64_t i = 0; i < count; ++i) {
+    const amm_batch_matrix& x = mats[i];
+    if (!x.A || x.m != b->mats[i].m || x.n != b->mats[i].n || x.ld < x.m)
+      return AMM_ERR_INVALID_ARGUMENT;
+    if ((reinterpret_cast<uintptr_t>(x.A) & 15) != 0 || (x.ld % 4) != 0) return AMM_ERR_ALIGNMENT;
+  }
+  for (int64_t i = 0; i < count; ++i) {
+    b->mats[i].A = static_cast<const float*>(mats[i].A);
+    b->mats[i].ld = mats[i].ld;
+  }
+  Guard g(b->device);
+  // pageable source: the copy is staged before the call returns, then stream-ordered
+  BATCH_CUDA(cudaMemcpyAsync(b->d_mats, b->mats.data(), sizeof(Mat) * count,
+                             cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)));
+  return AMM_OK;
+}
+
+int amm_batch_record(amm_batch* b, float* d_cdf, uint32_t* d_picks, int64_t products) {
+  if (!b || products < 0 || products > (1 << 20) || (d_picks && products == 0))
+    return AMM_ERR_INVALID_ARGUMENT;
+  if ((d_cdf || d_picks) && !b->amm) return AMM_ERR_INVALID_ARGUMENT;
+  b->rec_cdf = d_cdf;
+  b->rec_picks = d_picks;
+  b->rec_products = d_picks ? (int)products : 0;
+  // the captured graph holds the launch arguments by value
+  Guard g(b->device);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->gexec = nullptr;
+  b->graph = nullptr;
   return AMM_OK;
 }
 

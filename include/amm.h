@@ -250,6 +250,12 @@ typedef struct amm_batch_config {
   int32_t wide;       /* two-launch plan for uneven batches (amm_batch_wide_plan): 0 = with */
                       /* an autotuned cluster size, kept if it times faster; 1 = whenever   */
                       /* the batch is uneven enough, untimed; -1 = never                    */
+  int32_t vr_period;  /* AMM mode only: variance reduction as the reference's -vr            */
+                      /* (powerMethod_by_previous.cuh:135-157) over a block: product p is   */
+                      /* exact and memoised when (p + 1) % vr_period == 0, and so is the    */
+                      /* last product; the others estimate C·X = Y_memo·S + Ĉ·(X − X_memo·S) */
+                      /* with S = X_memoᵀX (for one vector, S = x_memo·x).  Convergence is  */
+                      /* tested on exact products only.  0 = off                            */
 } amm_batch_config;
 
 void amm_batch_config_default(amm_batch_config *cfg);
@@ -265,14 +271,25 @@ int amm_batch_vector_offsets(amm_batch *b, int64_t *offsets);
  * autotunes the tile shape (columns per group) on this batch. */
 int amm_batch_run(amm_batch *b, double *d_lambda, float *d_vectors, int32_t *d_iters,
                   void *stream);
+/* Rebind the batch to new matrices of the same shapes (same count, m and n per matrix; A and
+ * ld may change), stream-ordered: later runs and gradients use them, while the tile choice,
+ * the launch plan and any captured graph are kept.  No counterpart in the reference. */
+int amm_batch_set_matrices(amm_batch *b, const amm_batch_matrix *mats, int64_t count,
+                           void *stream);
 /* The same computation with one launch per matrix (the comparison arm). */
 int amm_batch_run_each(amm_batch *b, double *d_lambda, float *d_vectors, int32_t *d_iters,
                        void *stream);
 /* Backward of λ_max: grad_b = scale_b · 2·v_b·(v_bᵀA_b), column-major with leading dimension
- * grad_ld[b]; grad_ptrs and grad_ld are host arrays of count entries, d_scale a device array of
- * count factors or NULL.  Synchronises the stream. */
+ * grad_ld[b]; grad_ptrs and grad_ld are host arrays of count entries (read before the call
+ * returns), d_scale a device array of count factors or NULL.  Asynchronous on the stream. */
 int amm_batch_grad(amm_batch *b, const float *d_vectors, void *const *grad_ptrs,
                    const int64_t *grad_ld, const float *d_scale, void *stream);
+/* Parity record of the AMM mode (no counterpart in the reference; test aid): with d_cdf set,
+ * each run writes every matrix's FP32 sampling CDF (its n_b entries at the matrix's column
+ * offset, Σ n_b floats in all); with d_picks set, the raw picks of AMM product p < products of
+ * matrix b, in draw order, at (Σ_{a<b} c_a)·products + p·c_b + k (exact products leave their
+ * slots untouched).  NULL pointers stop recording.  The buffers must outlive the runs. */
+int amm_batch_record(amm_batch *b, float *d_cdf, uint32_t *d_picks, int64_t products);
 /* The tile shape the autotuner picked: block size, columns per group and CTAs per matrix
  * (cluster size; cluster_size may be NULL).  AMM_ERR_NOT_READY before the first run. */
 int amm_batch_tile_choice(amm_batch *b, int32_t *nvec, int32_t *cols_per_group,

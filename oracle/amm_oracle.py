@@ -39,6 +39,7 @@ __all__ = [
     "xorshift32", "pick_index", "sample_sorted", "previous_amm", "proposed_amm", "dots",
     "exact_product", "dot_product_and_generate_x", "normalize", "generate_zv",
     "PowerTrace", "power_method", "reported_eigenvalue", "grad_lambda", "lambda_max_f64",
+    "batch_seed_states", "batch_start_block", "batch_cdf", "batch_block_power", "BatchTrace",
 ]
 
 
@@ -427,6 +428,141 @@ def power_method(A, x0, *, method="exact", step=10, c=None, states=None, vr_peri
     return PowerTrace(np.array(eigs, dtype=F64), np.array(errs, dtype=F64),
                       np.array(coss, dtype=F64), modes, indices, x, y, states,
                       {k: v_[0] for k, v_ in cdfs.items()})
+
+
+# --------------------------------------------------------------------------------------------
+# Batched block power iteration (an extension: the reference solves one vector of one matrix per
+# run).  The products and sampling follow the reference's single-vector path column by column:
+# the exact product is powerMethod_by_exact.cuh:37-53, the sampled product is
+# previousAMM_kernel1+2 (core_previousAMM.cuh:163-174, 225-232) with pick_index
+# (device_memory.h:506-545), and variance reduction follows powerMethod_by_previous.cuh:135-157,
+# applied to a block of K vectors.
+# --------------------------------------------------------------------------------------------
+
+_M64 = (1 << 64) - 1
+
+
+def batch_seed_states(seed: int, total: int) -> np.ndarray:
+    """The batch's xorshift32 states: a splitmix64 stream from ``seed`` (the high 32 bits of
+    each output; a zero, xorshift32's fixed point, is replaced by 0x6A09E667).  Matrix b owns
+    the c_b states after those of the matrices before it."""
+    out = np.empty(total, dtype=U32)
+    z = int(seed) & _M64
+    for k in range(total):
+        z = (z + 0x9E3779B97F4A7C15) & _M64
+        x = z
+        x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+        x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & _M64
+        x ^= x >> 31
+        v = x >> 32
+        out[k] = v if v else 0x6A09E667
+    return out
+
+
+def batch_start_block(seed: int, mi: int, m: int, K: int) -> np.ndarray:
+    """The start block of matrix ``mi`` (m x K, FP32): a counter-based hash of (seed, matrix,
+    row, vector) mapped to [-1, 1)."""
+    rows = np.arange(m, dtype=np.uint64)[:, None]
+    vecs = np.arange(K, dtype=np.uint64)[None, :]
+    with np.errstate(over="ignore"):
+        z = (np.uint64(seed) ^ (np.uint64(0x9E3779B97F4A7C15) * np.uint64(mi + 1))
+             ^ (rows << np.uint64(20)) ^ (vecs << np.uint64(52)))
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    hi = (z >> np.uint64(32)).astype(np.uint32).view(np.int32)
+    return (hi.astype(F32) * F32(1.0 / 2147483648.0)).astype(F32)
+
+
+def batch_cdf(A) -> np.ndarray:
+    """The FP32 sampling CDF of previous AMM for one matrix: ‖A_j‖² (get_norms / set_weights,
+    device_memory.h:34-59, common.h:34-40), prefix-summed in FP64 and stored in FP32 (the
+    reference's CUB InclusiveSum, powerMethod_by_previous.cuh:26-32)."""
+    A64 = np.asarray(A, dtype=F64)
+    w = (A64 * A64).sum(axis=0).astype(F32)
+    return np.cumsum(w.astype(F64)).astype(F32)
+
+
+@dataclasses.dataclass
+class BatchTrace:
+    ritz: np.ndarray          # K Ritz values of the last Rayleigh–Ritz step, descending
+    vector: np.ndarray        # unit top Ritz vector (m)
+    picks: list               # per product: uint32[c] raw picks (None for an exact product)
+    kinds: list               # per product: "exact" or "amm"
+    states: np.ndarray        # the states after the run
+
+
+def _orth(Y):
+    """An orthonormal basis of span(Y) (any basis serves: every step below is invariant under
+    a rotation of the block)."""
+    q, _ = np.linalg.qr(Y)
+    return q
+
+
+def batch_block_power(A, *, K: int, max_iter: int, c: int = 0, states=None, cdf=None,
+                      vr_period: int = 0, seed: int = 1234, mi: int = 0) -> BatchTrace:
+    """Block power iteration with Rayleigh–Ritz on C = A·Aᵀ for one matrix of the batch, run
+    for exactly ``max_iter`` products (no early stop), in FP64.
+
+    X_0 is the orthonormalised start block.  Product p multiplies the current orthonormal
+    block X:
+      * exact (c == 0, or with variance reduction when (p + 1) % vr_period == 0 or p is the
+        last product): Y = A·(Aᵀ·X), and with variance reduction (X_memo, Y_memo) <- (X, Y);
+      * sampled: c draws by pick_index from ``cdf`` and ``states`` (advanced once per sampled
+        product), column j weighted mult_j·total/(c·(cdf[j] − cdf[j−1])) with the FP32 CDF
+        values (the realised probability of the draw), and
+        Y = Y_memo·S + Σ_j w_j·A_j·(A_jᵀ·D),  D = X − X_memo·S,  S = X_memoᵀ·X
+        (S = 0 before the first exact product: Y = Ĉ·X).
+    After each product the next block is an orthonormal basis of span(Y); the Ritz values are
+    the eigenvalues of sym(XᵀY) of the last product.
+    """
+    A64 = np.asarray(A, dtype=F64)
+    m, n = A64.shape
+    X = _orth(batch_start_block(seed, mi, m, K).astype(F64))
+    st = None if states is None else np.asarray(states, dtype=U32).copy()
+    cdf32 = None if cdf is None else np.asarray(cdf, dtype=F32)
+    Xm = Ym = None
+    picks, kinds = [], []
+    Y = None
+    for p in range(max_iter):
+        exact = c == 0 or (vr_period > 0 and ((p + 1) % vr_period == 0 or p + 1 >= max_iter))
+        if exact:
+            Y = A64 @ (A64.T @ X)
+            if vr_period > 0 and c > 0:
+                Xm, Ym = X.copy(), Y.copy()
+            picks.append(None)
+            kinds.append("exact")
+        else:
+            idx, st = pick_index(cdf32, st, c)
+            picks.append(idx)
+            kinds.append("amm")
+            cols, mult = np.unique(idx, return_counts=True)
+            total = F64(cdf32[-1])
+            prev = np.where(cols > 0, cdf32[np.maximum(cols.astype(np.int64) - 1, 0)].astype(F64), 0.0)
+            step = cdf32[cols].astype(F64) - prev
+            w = (mult.astype(F64) * total / (F64(c) * step)).astype(F32).astype(F64)
+            if Xm is not None:
+                S = Xm.T @ X
+                D = X - Xm @ S
+            else:
+                S, D = None, X
+            As = A64[:, cols]
+            Y = As @ (w[:, None] * (As.T @ D))
+            if S is not None:
+                Y = Y + Ym @ S
+        if p + 1 < max_iter:
+            Xn = _orth(Y)
+            X_last, Y_last = X, Y
+            X = Xn
+        else:
+            X_last, Y_last = X, Y
+    H = 0.5 * (X_last.T @ Y_last + Y_last.T @ X_last)
+    th, V = np.linalg.eigh(H)
+    order = np.argsort(th)[::-1]
+    v = X_last @ V[:, order[0]]
+    return BatchTrace(ritz=th[order], vector=v / np.linalg.norm(v), picks=picks, kinds=kinds,
+                      states=st)
 
 
 # --------------------------------------------------------------------------------------------
