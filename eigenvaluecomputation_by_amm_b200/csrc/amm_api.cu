@@ -407,8 +407,17 @@ int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
   if (ctx->nsm < 1) ctx->nsm = 1;
   ctx->sanity_active = (cfg.sanity && cfg.c == cfg.n) ? 1 : 0;
-  if (!amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm, &ctx->geom) ||
-      !amm::panel_coresident(ctx->geom)) {
+  // thread-block clusters of the step kernel (AMM_PANEL_CLUSTER: 1, 2, 4 or 8), falling back
+  // to none where the shape or the residency does not allow them
+  int want_cluster = amm::panel_cluster_request();
+  bool geo = amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm,
+                                 want_cluster, &ctx->geom) &&
+             amm::panel_coresident(&ctx->geom, ctx->nsm);
+  if (!geo && want_cluster > 1)
+    geo = amm::panel_geometry((int)cfg.m, cfg.dtype, (int)cfg.c, (int)cfg.n, ctx->nsm, 1,
+                              &ctx->geom) &&
+          amm::panel_coresident(&ctx->geom, ctx->nsm);
+  if (!geo) {
     delete ctx;
     cudaGetLastError();
     return AMM_ERR_UNSUPPORTED;
@@ -419,7 +428,7 @@ int amm_create(amm_ctx** out, const amm_config* cfg_in, int device) {
   b.c = (int32_t)cfg.c;
   b.dtype = cfg.dtype;
   b.cdf_f32 = cfg.cdf_precision == AMM_CDF_F32 ? 1 : 0;
-  b.nsm = ctx->geom.nclusters;
+  b.nsm = ctx->geom.grid;
   int seg = amm::kSeg;
   while (cfg.n / seg > amm::kCoarseMax) seg <<= 1;
   b.seg = seg;

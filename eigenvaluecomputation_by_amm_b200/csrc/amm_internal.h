@@ -124,9 +124,12 @@ struct Buffers {
 // Launch geometry of the panel kernel for a given (m, dtype).
 struct PanelGeom {
   int dtype;        // 0 FP32, 1 BF16
-  int cluster;      // CTAs per cluster (K); CTA rank r owns rows [r*rows, (r+1)*rows)
-  int rows;         // rows per CTA = m / cluster
-  int nclusters;    // clusters launched (= partial sums)
+  int cluster;      // CTAs per thread-block cluster (1: no clusters).  The CTAs of a cluster
+                    // pre-sum their partial y through distributed shared memory: rank r sums
+                    // rows [r*m/cluster, (r+1)*m/cluster) of the cluster's partials
+  int rows;         // rows each CTA streams (all m)
+  int nclusters;    // clusters launched (= partial y vectors written per step)
+  int grid;         // CTAs launched = nclusters * cluster (one per SM, all resident)
   int threads;      // consumer threads (a producer warp is added)
   int slots;        // 16-byte vector slots per consumer thread (R)
   int elems;        // elements per 16-byte vector (E)
@@ -139,10 +142,15 @@ struct PanelGeom {
   int wl_cap;       // work-list capacity per cluster
 };
 
-bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g);
+// cluster: requested CTAs per cluster (1, 2, 4 or 8; falls back to 1 where the shape or the
+// residency does not allow it).
+bool panel_geometry(int m, int dtype, int c, int n, int nsm, int cluster, PanelGeom* g);
+// CTAs per cluster the step kernel is asked to use (AMM_PANEL_CLUSTER, default 1).
+int panel_cluster_request();
 // One CTA of the step kernel and of the set-up pass fits on an SM with the geometry's
-// shared-memory carve (the persistent grids need every CTA resident at once).
-bool panel_coresident(const PanelGeom& g);
+// shared-memory carve (the persistent grids need every CTA resident at once); with clusters,
+// fixes the grid to the clusters that fit at once (false if fewer than half the SMs).
+bool panel_coresident(PanelGeom* g, int nsm);
 
 // ---- launchers (amm_kernels.cu); each returns the cudaError_t of the launch ----
 // Set-up pass over A (amm_panel.cu): column statistics (α, ‖A_j‖, ‖A_j − α_j‖), z = A·α,

@@ -16,11 +16,14 @@
 //   4. warp-reduce and publish the dots of g+1, then meet at one named barrier,
 // so the reduction latency of a group hides behind the next group's math and there is one
 // barrier per group.  Each column is read from HBM once (the reference's kernel1/kernel2 read
-// it twice).  Each CTA writes one partial y; after a grid barrier every CTA sums its rows of
-// the partials in a fixed order, and the last CTA to finish forms λ and the next step's state.
+// it twice).  Each CTA writes one partial y (with thread-block clusters, the cluster's CTAs first
+// sum theirs through distributed shared memory and write one partial per cluster); after a grid
+// barrier every CTA sums its rows of the partials in a fixed order, and every CTA forms λ and
+// the next step's state from the same per-CTA sums.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 
@@ -282,6 +285,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   __shared__ uint32_t iss_s;    // groups issued so far (thread 0)
   __shared__ IterState nxs_s;   // the next state, formed by warp 0
   __shared__ int32_t wlkey_s;   // slot of the coefficient slice copied ahead into wl_* (-2: none)
+  __shared__ uint32_t xstage_s; // clusters: the stage holding this CTA's partial y (read by peers)
 
   // A launch of the step kernel is a programmatic dependent of the grid before it: its CTAs
   // start on the SMs that the previous grid leaves, initialise their barriers, and wait for
@@ -289,11 +293,26 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   // by the time it lets the next grid be scheduled (one CTA per SM), so the grid barriers
   // below are unaffected.
   if (!SETUP) griddep_launch_dependents();
+  // Clusters (CL > 1): the partial-y exchange of each step runs on two mbarriers per CTA, each
+  // completing when all CL CTAs of the cluster have arrived (remote arrives): xbar[0] when every
+  // CTA has published its partial in shared memory, xbar[1] when every CTA is done reading its
+  // peers'.  A CTA refills the stage holding its partial, or leaves the kernel, only after
+  // xbar[1] of its last exchange (bounded waits throughout: no hardware cluster barrier after
+  // the prologue, so no CTA can be held by a peer that gave up).
+  const int CL = g.cluster;
+  uint64_t* xbar = full + 8;
   if (t == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+    if (CL > 1) {
+      mbar_init(&xbar[0], (uint32_t)CL);
+      mbar_init(&xbar[1], (uint32_t)CL);
+    }
     fence_barrier_init();
   }
   __syncthreads();  // barrier initialisation visible to every thread
+  // every CTA of the cluster has initialised its barriers before any peer arrives on them (no
+  // CTA can have left the kernel yet)
+  if (CL > 1) cluster_sync_all();
   if (!SETUP) griddep_wait();
 
   // work-list lengths of every slot (fixed for the launch: the window is refilled between
@@ -380,6 +399,27 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       for (uint32_t p = issued > (uint32_t)NS ? issued - (uint32_t)NS : 0u; p < issued; ++p)
         wait_pos(p);
     }
+  };
+  // partial-y exchanges of the cluster completed by this CTA (uniform over its threads)
+  uint32_t npub = 0;
+  auto xarrive = [&](int which) {  // thread r < CL arrives on rank r's barrier
+    if (t < CL) mbar_arrive_remote(map_to_rank(smem_addr(&xbar[which]), (uint32_t)t));
+  };
+  // before leaving the kernel: the peers are done with this CTA's shared memory
+  auto xsettle = [&]() {
+    if (CL > 1 && npub > 0) mbar_wait_cluster_bounded(&xbar[1], (npub - 1) & 1u);
+  };
+  // this step's exchange without data, on a failure path: the peers waiting on this CTA are
+  // released, and it leaves only once they are done with its shared memory
+  auto xabandon = [&]() {
+    if (CL <= 1) return;
+    named_barrier_or(1, T, false);
+    xarrive(0);
+    mbar_wait_cluster_bounded(&xbar[0], npub & 1u);
+    named_barrier_or(1, T, false);
+    xarrive(1);
+    ++npub;
+    xsettle();
   };
 
   // ---- everything step j needs that does not depend on the product of the step before ----
@@ -537,7 +577,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       }
     }
 
-    if (t == 0 && ngroups > pre) {  // the first NS groups not already in flight
+    // the stage that held this CTA's partial of the last exchange is refilled below: the
+    // peers must be done reading it (already so in practice: two grid barriers lie between)
+    if (CL > 1 && npub > 0 && t == 0) {
+      if (!mbar_wait_cluster_bounded(&xbar[1], (npub - 1) & 1u)) ok = false;
+      fence_proxy_async_smem();  // generic writes of the partial before the async refill
+    }
+    if (t == 0 && ok && ngroups > pre) {  // the first NS groups not already in flight
       uint32_t first[kGcMax * 8];
       const int nf = min(NS * GC, nb);
       if (sampled)
@@ -800,6 +846,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       ph_cur = ph_nxt;
     }
     if (!ok) {
+      xabandon();
       drain();
       if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
       return;
@@ -833,7 +880,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         chk[col >> cs] = 0u;
       }
     }
-    float* part = b.partials + (size_t)q * m;
+    // this CTA's partial y: to the partial-sum buffer, or (clusters) to a stage that no copy
+    // uses (at most kPrefetchGroups of the NS >= 3 stages hold the next step's first groups;
+    // which one depends on this CTA's ring position, so it is published for the peers)
+    const uint32_t xstage = (gbase + kPrefetchGroups) % (uint32_t)NS;
+    if (CL > 1 && t == 0) xstage_s = xstage;
+    float* part = CL > 1 ? reinterpret_cast<float*>(stages + (size_t)xstage * stage_bytes)
+                         : b.partials + (size_t)q * m;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int vi = t + r * T;
@@ -849,6 +902,52 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       b.spart[q] = sacc;
       b.spart64[q] = a2acc;
     }
+    if (CL > 1) {
+      // The cluster's partial: CTA rank r sums float4 row groups [r·m/(4·CL), (r+1)·m/(4·CL))
+      // of the CL partials in rank order (FP32) from the peers' shared memory, and writes them
+      // to the cluster's partial-sum row.
+      fence_acq_rel_cluster();
+      named_barrier_or(1, T, false);  // the whole partial is in shared memory
+      xarrive(0);
+      const bool got = mbar_wait_cluster_bounded(&xbar[0], npub & 1u);
+      const bool bad = named_barrier_or(1, T, !got);
+      if (!bad) {
+        const int per = (m >> 2) / CL;
+        const int r0 = (int)cluster_ctarank() * per;
+        // each peer's partial: its stage index, then the stage's address in its shared memory
+        uint32_t fa[8];
+        const uint32_t sbase = smem_addr(stages), xs_addr = smem_addr(&xstage_s);
+        for (int k = 0; k < CL; ++k) {
+          uint32_t ks;
+          asm volatile("ld.shared::cluster.u32 %0, [%1];"
+                       : "=r"(ks)
+                       : "r"(map_to_rank(xs_addr, (uint32_t)k))
+                       : "memory");
+          fa[k] = map_to_rank(sbase + ks * stage_bytes, (uint32_t)k);
+        }
+        float4* cpart = reinterpret_cast<float4*>(b.partials + (size_t)(q / CL) * m);
+        for (int gi = r0 + t; gi < r0 + per; gi += T) {
+          float4 acc = ld_cluster_f4(fa[0] + 16u * (uint32_t)gi);
+          for (int k = 1; k < CL; ++k) {
+            const float4 v = ld_cluster_f4(fa[k] + 16u * (uint32_t)gi);
+            acc.x += v.x;
+            acc.y += v.y;
+            acc.z += v.z;
+            acc.w += v.w;
+          }
+          cpart[gi] = acc;
+        }
+      }
+      named_barrier_or(1, T, false);  // this CTA is done reading its peers
+      xarrive(1);
+      ++npub;
+      if (bad) {
+        xsettle();
+        drain();
+        if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
+        return;
+      }
+    }
 
     // ====================== the step's epilogue, fused (grid-wide) ======================
     // Every CTA is resident (one per SM), so after a grid barrier the G partials are summed
@@ -862,12 +961,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     bool bar_ok = true;
     if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
     if (named_barrier_or(1, T, !bar_ok)) {
+      xsettle();
       drain();
       if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
       return;
     }
     double S = 0.0;  // Σ over the CTAs of the per-CTA scalar (fixed order, the same everywhere)
     double xy = 0.0, yy = 0.0, yv = 0.0;
+    const int NPART = G / CL;  // partial-sum rows: one per CTA, or one per cluster
     constexpr int kU = 10;
     for (int c0 = g0; c0 < g1; c0 += 32) {
       const int gi = c0 + lane;
@@ -875,13 +976,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
       if (gi < g1) {
         const float* P = b.partials + 4 * (size_t)gi;
-        for (int k0 = warp; k0 < G; k0 += ncw * kU) {
+        for (int k0 = warp; k0 < NPART; k0 += ncw * kU) {
           float4 v[kU];
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
             const int k = k0 + u * ncw;
-            v[u] = k < G ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * m))
-                         : make_float4(0.f, 0.f, 0.f, 0.f);
+            v[u] = k < NPART ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * m))
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
           }
           if (first && k0 == warp && warp == 0 && (SETUP || centred)) {
             zdx = 0.0;
@@ -998,6 +1099,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         }
         if (lane == 0) *b.alpha2 = S;
       }
+      xsettle();
       return;
     } else {
       if (warp == 0) {
@@ -1027,6 +1129,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       named_barrier_or(1, T, false);  // this CTA's Rayleigh shares are written
       if (t == 0) bar_ok = grid_barrier(b.ticket + 2, (uint32_t)G);
       if (named_barrier_or(1, T, !bar_ok)) {
+        xsettle();
         drain();
         if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
         return;
@@ -1060,6 +1163,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   // past the last step of the launch (or the early stop): the state the next launch (or the
   // call's end) reads, and no copy still in flight
   if (!SETUP) {
+    xsettle();
     drain();
     if (q == 0 && t == 0) b.st[a.iter_end & 1] = st_s;
   }
@@ -1108,9 +1212,13 @@ static int env_int(const char* name, int dflt) {
   return (v && *v) ? atoi(v) : dflt;
 }
 
-// Rows per thread, columns per group and stages for (m, dtype): one persistent CTA per SM
-// (grid = number of SMs).  Tuning overrides: AMM_PANEL_GC, AMM_PANEL_STAGES (0 = automatic).
-bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
+int panel_cluster_request() { return env_int("AMM_PANEL_CLUSTER", 1); }
+
+// Rows per thread, columns per group and stages for (m, dtype): one persistent CTA per SM.
+// Tuning overrides: AMM_PANEL_GC, AMM_PANEL_STAGES (0 = automatic).  With cluster > 1 the grid
+// is fixed by panel_coresident (the clusters that fit at once, at least half the SMs); the
+// work-list capacity is sized for that lower bound.
+bool panel_geometry(int m, int dtype, int c, int n, int nsm, int cluster, PanelGeom* g) {
   const int es = dtype == 1 ? 2 : 4;
   const int E = 16 / es;
   if (m <= 0 || m % E != 0) return false;
@@ -1133,10 +1241,16 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   if (fgc > 0) gc = fgc;
   const int stage = gc * colb;
   const int maxlist = c < n ? c : n;
+  // clusters: the partial y (m floats) must fit one stage, and the ranks' row slices be whole
+  // float4 groups
+  if (cluster != 2 && cluster != 4 && cluster != 8) cluster = 1;
+  if (cluster > 1 && (stage < 4 * m || (m / 4) % cluster != 0 || nsm < 2 * cluster))
+    cluster = 1;
+  const int grid_min = cluster > 1 ? nsm / 2 : nsm;
   // the stages take what the rest of the carve leaves of 227 KB (at most 8)
   PanelGeom probe{};
   probe.gc = gc;
-  probe.wl_cap = (maxlist + nsm - 1) / nsm + 1;
+  probe.wl_cap = (maxlist + grid_min - 1) / grid_min + 1;
   const int rest = smem_layout(probe, true).total;
   int ns = (227 * 1024 - rest) / stage;
   if (ns > 8) ns = 8;
@@ -1145,9 +1259,10 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, PanelGeom* g) {
   if (ns < 3 || !pick_kernel(dtype, R, gc, false)) return false;
   PanelGeom b{};
   b.dtype = dtype;
-  b.cluster = 1;
+  b.cluster = cluster;
   b.rows = m;
-  b.nclusters = nsm;
+  b.nclusters = nsm / cluster;
+  b.grid = b.nclusters * cluster;
   b.threads = T;
   b.slots = R;
   b.elems = E;
@@ -1204,21 +1319,46 @@ static bool coop_with_pdl() {
   return g_coop_pdl[dev] == 1;
 }
 
-bool panel_coresident(const PanelGeom& g) {
+bool panel_coresident(PanelGeom* g, int nsm) {
+  int fit = nsm / g->cluster;  // clusters resident at once, over both variants
   for (int setup = 0; setup < 2; ++setup) {
     KernelFn fn;
     int smem = 0;
-    if (configure(g, setup != 0, &fn, &smem) != cudaSuccess) {
+    if (configure(*g, setup != 0, &fn, &smem) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, g.threads, (size_t)smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, g->threads, (size_t)smem) !=
         cudaSuccess) {
       cudaGetLastError();
       return false;
     }
     if (per_sm < 1) return false;
+    if (g->cluster > 1) {
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(g->cluster * (nsm / g->cluster));
+      cfg.blockDim = dim3(g->threads);
+      cfg.dynamicSmemBytes = (size_t)smem;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = g->cluster;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, (void*)fn, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      fit = std::min(fit, nc);
+    }
+  }
+  if (g->cluster > 1) {
+    if (fit * g->cluster < nsm / 2) return false;  // the work lists are sized for >= nsm/2 CTAs
+    g->nclusters = fit;
+    g->grid = fit * g->cluster;
   }
   return true;
 }
@@ -1232,18 +1372,25 @@ static cudaError_t launch_panel(const PanelArgs& a, bool setup, cudaStream_t s) 
   static const bool pdl = env_int("AMM_PDL", 1) != 0;
   const bool dep = !setup && pdl;
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(a.g.nclusters);
+  cfg.gridDim = dim3(a.g.grid);
   cfg.blockDim = dim3(a.g.threads);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = s;
-  cudaLaunchAttribute at[2];
+  cudaLaunchAttribute at[3];
   int na = 0;
   if (dep) {
     at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[na].val.programmaticStreamSerializationAllowed = 1;
     ++na;
   }
-  if (!dep || coop_with_pdl()) {
+  if (a.g.cluster > 1) {
+    // clusters: the grid is the clusters that fit at once (panel_coresident)
+    at[na].id = cudaLaunchAttributeClusterDimension;
+    at[na].val.clusterDim.x = a.g.cluster;
+    at[na].val.clusterDim.y = 1;
+    at[na].val.clusterDim.z = 1;
+    ++na;
+  } else if (!dep || coop_with_pdl()) {
     at[na].id = cudaLaunchAttributeCooperative;
     at[na].val.cooperative = 1;
     ++na;

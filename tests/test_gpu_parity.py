@@ -425,10 +425,13 @@ print(json.dumps({"eigs": tr["eigs"].tolist(), "kinds": tr["kinds"],
 
 
 @pytest.mark.parametrize("env", [{}, {"AMM_PDL": "0"}, {"AMM_PANEL_GC": "4"},
-                                 {"AMM_PANEL_STAGES": "4", "AMM_PDL": "0"}])
+                                 {"AMM_PANEL_STAGES": "4", "AMM_PDL": "0"},
+                                 {"AMM_PANEL_CLUSTER": "2"}, {"AMM_PANEL_CLUSTER": "4"},
+                                 {"AMM_PANEL_CLUSTER": "4", "AMM_PDL": "0"}])
 def test_launch_knobs_agree(env):
     """The environment knobs (no programmatic dependent launch, 4 instead of 8 columns per stage,
-    a shallower ring) change only the launch shape: the same picks and step kinds, λ within the
+    a shallower ring, thread-block clusters that pre-sum their partial y through distributed
+    shared memory) change only the launch shape: the same picks and step kinds, λ within the
     FP32 tolerance of the default configuration (run in separate processes: the knobs are read
     once per process)."""
     import json
@@ -440,7 +443,7 @@ def test_launch_knobs_agree(env):
 
     def run(extra):
         e = dict(os.environ)
-        for k in ("AMM_PDL", "AMM_PANEL_GC", "AMM_PANEL_STAGES"):
+        for k in ("AMM_PDL", "AMM_PANEL_GC", "AMM_PANEL_STAGES", "AMM_PANEL_CLUSTER"):
             e.pop(k, None)
         e.update(extra)
         r = subprocess.run([sys.executable, "-c", _KNOB_SCRIPT, root], env=e, capture_output=True,
@@ -456,3 +459,6 @@ def test_launch_knobs_agree(env):
         assert got["geometry"]["cols_per_stage"] == int(env["AMM_PANEL_GC"])
     if "AMM_PANEL_STAGES" in env:
         assert got["geometry"]["stages"] == int(env["AMM_PANEL_STAGES"])
+    if "AMM_PANEL_CLUSTER" in env:
+        assert got["geometry"]["cluster"] == int(env["AMM_PANEL_CLUSTER"])
+        assert got["geometry"]["clusters"] * got["geometry"]["cluster"] >= 74
