@@ -102,6 +102,8 @@ _SIGS = {
     "amm_core_previousAMM": [_P, _P, _P, _P, _P, _P, _P],
     "amm_core_proposedAMM": [_P, _P, _P, _P, _P, _P, _P],
     "amm_exact_product": [_P, _P, _P, _P],
+    "amm_core_list_product": [_P, C.c_int, _P, _P, _I64, _P, _P, _P, _P, _P],
+    "amm_shard_product": [_P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P],
     "amm_rayleigh_normalize": [_P, _P, _P, _P, _P],
     "amm_normalize": [_P, _P, _P],
     "amm_get_column_stats": [_P, _P, _P, _P, _P, _P, _P, _P],

@@ -231,6 +231,33 @@ class AMMContext:
                                             _stream(stream)), "amm_core_proposedAMM")
         return y, idx
 
+    def core_list_product(self, method: str, cols: torch.Tensor, wm: torch.Tensor, x,
+                          x_memo=None, y_memo=None, stream=None):
+        """The sampled product over a given work list (amm_core_list_product): distinct column
+        indices ``cols`` (int32) with weights ``wm`` = w_j·multiplicity (FP32)."""
+        cols = _u32(cols.to(self._dev).contiguous())
+        wm = wm.to(device=self._dev, dtype=torch.float32).contiguous()
+        x, xm, ym = self._vec(x), self._vec(x_memo), self._vec(y_memo)
+        y = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        check(self.lib.amm_core_list_product(self._ctx, _lib.METHODS[method], _ptr(cols), _ptr(wm),
+                                             cols.numel(), _ptr(x), _ptr(xm), _ptr(ym), _ptr(y),
+                                             _stream(stream)), "amm_core_list_product")
+        return y
+
+    def shard_product(self, cdf_global: torch.Tensor, col0: int, states: torch.Tensor, x,
+                      x_memo=None, y_memo=None, stream=None):
+        """This rank's part of a previous-AMM product over a column-sharded matrix
+        (amm_shard_product): the context holds global columns [col0, col0 + n); ``cdf_global``
+        (FP64, all columns) and the c ``states`` (advanced in place) are the same on every
+        rank."""
+        st = _u32(states)
+        x, xm, ym = self._vec(x), self._vec(x_memo), self._vec(y_memo)
+        y = torch.empty(self.m, dtype=torch.float32, device=self._dev)
+        check(self.lib.amm_shard_product(self._ctx, _ptr(cdf_global), cdf_global.numel(),
+                                         int(col0), _ptr(st), _ptr(st), _ptr(x), _ptr(xm),
+                                         _ptr(ym), _ptr(y), _stream(stream)), "amm_shard_product")
+        return y
+
     def exact_product(self, x, stream=None):
         x = self._vec(x)
         y = torch.empty(self.m, dtype=torch.float32, device=self._dev)

@@ -79,6 +79,7 @@ struct amm_ctx {
   int last_step = 0;
   bool has_run = false;
   CallCfg last_cc{};
+  uint32_t ext_count = 0;  // length of a caller-supplied work list (host copy read by a memcpy)
 };
 
 namespace {
@@ -185,7 +186,7 @@ int ensure_setup(amm_ctx* ctx, cudaStream_t s);
 int enqueue_call(amm_ctx* ctx, const CallCfg& cc, const float* x0, int no_normalize,
                  cudaStream_t s) {
   const Buffers& b = ctx->b;
-  const bool draws = cc.uses_amm && !cc.sanity;
+  const bool draws = cc.uses_amm && !cc.sanity && !cc.ext_list;
   AMM_CUDA(amm::launch_init(b, cc, x0, no_normalize, s));
   // One persistent step launch per window of kListWindow steps (the whole call when nothing
   // is sampled), each preceded by the draw and compaction of the work lists of its AMM steps
@@ -277,13 +278,26 @@ int read_status(amm_ctx* ctx, cudaStream_t s) {
       AMM_CUDA(cudaMemsetAsync(ctx->b.ticket, 0, sizeof(uint32_t) * 4, s));
       return AMM_ERR_DEVICE_TIMEOUT;
     }
+    if (st & amm::kDevBadIndex) return AMM_ERR_INVALID_ARGUMENT;
     return AMM_ERR_DEGENERATE;
   }
   return AMM_OK;
 }
 
+// A draw over a column-sharded matrix (amm_shard_product) in place of the context's own.
+struct ShardDraw {
+  const double* cdf;
+  int64_t n_global, col0;
+  const uint32_t* st_in;
+  uint32_t* st_out;
+};
+
+// One product of `method`; the AMM step's work list is the context's own draw, or the caller's
+// (ext_cols/ext_wm, ext_count entries), or this rank's share of a sharded draw (shard).
 int single_product(amm_ctx* ctx, int method, const float* x, const float* x_memo,
-                   const float* y_memo, float* y, uint32_t* idx_out, cudaStream_t s) {
+                   const float* y_memo, float* y, uint32_t* idx_out, cudaStream_t s,
+                   const uint32_t* ext_cols = nullptr, const float* ext_wm = nullptr,
+                   int64_t ext_count = 0, const ShardDraw* shard = nullptr) {
   int rc = check_ready(ctx);
   if (rc) return rc;
   if (!x || !y) return AMM_ERR_INVALID_ARGUMENT;
@@ -307,6 +321,23 @@ int single_product(amm_ctx* ctx, int method, const float* x, const float* x_memo
     rc = ensure_setup(ctx, s);
     if (rc) return rc;
   }
+  if (ext_cols) {
+    // the caller's work list goes to slot 0, the slot of the call's first AMM step
+    cc.ext_list = 1;
+    ctx->ext_count = (uint32_t)ext_count;
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.wl_col[0], ext_cols, sizeof(uint32_t) * ext_count,
+                             cudaMemcpyDeviceToDevice, s));
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.wl_wm[0], ext_wm, sizeof(float) * ext_count,
+                             cudaMemcpyDeviceToDevice, s));
+    AMM_CUDA(amm::launch_gather_alpha(ctx->b, ext_count, s));
+    AMM_CUDA(cudaMemcpyAsync(ctx->b.wl_count, &ctx->ext_count, sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, s));
+  } else if (shard) {
+    cc.ext_list = 1;
+    AMM_CUDA(amm::launch_shard_worklist(ctx->b, shard->cdf, (int)shard->n_global,
+                                        (int)shard->col0, shard->st_in, shard->st_out,
+                                        (int)ctx->cfg.c, s));
+  }
   AMM_CUDA(cudaMemcpyAsync(ctx->x0_buf, x, vb, cudaMemcpyDeviceToDevice, s));
   ctx->last_cc = cc;
   ctx->last_step = 1;
@@ -314,7 +345,7 @@ int single_product(amm_ctx* ctx, int method, const float* x, const float* x_memo
   rc = enqueue_call(ctx, cc, ctx->x0_buf, /*no_normalize=*/1, s);
   if (rc) return rc;
   AMM_CUDA(cudaMemcpyAsync(y, ctx->y_final, vb, cudaMemcpyDeviceToDevice, s));
-  if (idx_out && method != amm::kMethodExact) {
+  if (idx_out && method != amm::kMethodExact && !ext_cols && !shard) {
     if (ctx->sanity_active) {
       std::vector<uint32_t> seq(ctx->cfg.n);
       for (int64_t k = 0; k < ctx->cfg.n; ++k) seq[k] = (uint32_t)k;
@@ -713,6 +744,29 @@ int amm_core_proposedAMM(amm_ctx* ctx, const float* d_x, const float* d_x_memo,
                          const float* d_y_memo, float* d_y, uint32_t* d_idx_out, void* stream) {
   return single_product(ctx, amm::kMethodProposed, d_x, d_x_memo, d_y_memo, d_y, d_idx_out,
                         as_stream(stream));
+}
+
+int amm_core_list_product(amm_ctx* ctx, int method, const uint32_t* d_cols, const float* d_wm,
+                          int64_t count, const float* d_x, const float* d_x_memo,
+                          const float* d_y_memo, float* d_y, void* stream) {
+  if (!ctx || !d_cols || !d_wm) return AMM_ERR_INVALID_ARGUMENT;
+  if (method != amm::kMethodPrevious && method != amm::kMethodProposed)
+    return AMM_ERR_INVALID_ARGUMENT;
+  if (count < 1 || count > ctx->cfg.c || ctx->sanity_active) return AMM_ERR_INVALID_ARGUMENT;
+  return single_product(ctx, method, d_x, d_x_memo, d_y_memo, d_y, nullptr, as_stream(stream),
+                        d_cols, d_wm, count);
+}
+
+int amm_shard_product(amm_ctx* ctx, const double* d_cdf_global, int64_t n_global, int64_t col0,
+                      const uint32_t* d_states_in, uint32_t* d_states_out, const float* d_x,
+                      const float* d_x_memo, const float* d_y_memo, float* d_y, void* stream) {
+  if (!ctx || !d_cdf_global || !d_states_in || !d_states_out) return AMM_ERR_INVALID_ARGUMENT;
+  if (n_global < ctx->cfg.n || n_global > INT32_MAX || col0 < 0 || col0 + ctx->cfg.n > n_global ||
+      ctx->sanity_active)
+    return AMM_ERR_INVALID_ARGUMENT;
+  const ShardDraw sd{d_cdf_global, n_global, col0, d_states_in, d_states_out};
+  return single_product(ctx, amm::kMethodPrevious, d_x, d_x_memo, d_y_memo, d_y, nullptr,
+                        as_stream(stream), nullptr, nullptr, 0, &sd);
 }
 
 int amm_exact_product(amm_ctx* ctx, const float* d_x, float* d_y, void* stream) {

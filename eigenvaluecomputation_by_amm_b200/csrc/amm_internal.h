@@ -11,7 +11,7 @@ enum StepKind : int32_t { kExactMemo = 0, kExact = 1, kPrevious = 2, kProposed =
 enum Method : int32_t { kMethodExact = 0, kMethodPrevious = 1, kMethodProposed = 2, kMethodProposedV2 = 3 };
 
 // Device status bits (ORed into Buffers::status).
-enum DevStatus : uint32_t { kDevTimeout = 1u, kDevNonFinite = 2u };
+enum DevStatus : uint32_t { kDevTimeout = 1u, kDevNonFinite = 2u, kDevBadIndex = 4u };
 
 constexpr int kMaxThreads = 512;   // panel kernel block size limit
 constexpr int kGcMax = 8;          // columns per pipeline stage, upper bound
@@ -53,6 +53,8 @@ struct CallCfg {
   int32_t sanity;      // sanity mode active (sanity && c == n)
   int32_t uses_amm;    // the call draws samples at all
   int32_t step;
+  int32_t ext_list;    // the (single) AMM step's work list in slot 0 comes from the caller or
+                       // from a sharded draw: the context draws nothing and keeps its states
 };
 
 // Every device buffer of a context.
@@ -194,6 +196,14 @@ cudaError_t launch_expand_sorted(const Buffers& b, const int32_t* d_cd, uint32_t
                                  cudaStream_t s);
 cudaError_t launch_grad(const Buffers& b, const float* v, float* grad, int64_t ldg,
                         cudaStream_t s);
+// Caller-supplied work list in slot 0 (count entries of wl_col[0], wl_wm[0]): α of each listed
+// column into wl_al[0]; an index outside [0, n) becomes column 0 with weight 0 and sets
+// kDevBadIndex.
+cudaError_t launch_gather_alpha(const Buffers& b, int64_t count, cudaStream_t s);
+// One rank's work list (slot 0) from a draw over a column-sharded matrix's global CDF: picks in
+// [col0, col0 + n) of the c picks drawn from st_in (advanced into st_out, may alias).
+cudaError_t launch_shard_worklist(const Buffers& b, const double* cdf, int n_global, int col0,
+                                  const uint32_t* st_in, uint32_t* st_out, int c, cudaStream_t s);
 
 // Count of this library's launches (for the bench's gpu_launches field).
 void count_launch(int k = 1);

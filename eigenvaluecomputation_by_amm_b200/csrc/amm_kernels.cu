@@ -247,6 +247,97 @@ __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_c
   }
 }
 
+// A caller-supplied work list (amm_core_list_product): α_j of each listed column, and no index
+// outside the matrix reaches the product kernel.
+__global__ void __launch_bounds__(256) gather_alpha_kernel(const __grid_constant__ Buffers b,
+                                                           int count) {
+  griddep_wait();
+  griddep_launch_dependents();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    uint32_t col = b.wl_col[0][k];
+    if (col >= (uint32_t)b.n) {
+      b.wl_col[0][k] = 0u;
+      b.wl_wm[0][k] = 0.0f;
+      col = 0u;
+      atomicOr(b.status, (uint32_t)kDevBadIndex);
+    }
+    b.wl_al[0][k] = __ldg(b.alpha + col);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// One rank's share of a draw over a column-sharded matrix (amm_shard_product): the c picks
+// are drawn from the GLOBAL inclusive CDF (every rank draws the same picks from the same
+// states), and the picks that fall in this rank's columns [col0, col0 + n) become its work list
+// in slot 0, with w = multiplicity·total/(c·(cdf[j] − cdf[j−1])) (the realised probability of
+// the draw) and the column's α.
+// ------------------------------------------------------------------------------------------
+struct ShardArgs {
+  Buffers b;
+  const double* cdf;   // global inclusive CDF, n_global entries
+  int n_global;
+  int col0;            // first global column of this rank
+  const uint32_t* st_in;
+  uint32_t* st_out;
+  int c;
+};
+
+__global__ void __launch_bounds__(256) shard_draw_kernel(const __grid_constant__ ShardArgs a) {
+  griddep_wait();
+  griddep_launch_dependents();
+  const double total = __ldg(a.cdf + a.n_global - 1);
+  uint32_t* cnt = a.b.count[0];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.c; k += gridDim.x * blockDim.x) {
+    const uint32_t y = xorshift32(a.st_in[k]);  // get_rand (device_memory.h:506-514)
+    a.st_out[k] = y;
+    const double target = __dmul_rn(total, (double)uniform_from(y));
+    int lo = 0, hi = a.n_global;  // first i with cdf[i] > target, else n - 1 (:529-543)
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(a.cdf + mid) <= target)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int j = (lo < a.n_global ? lo : a.n_global - 1) - a.col0;
+    if (j >= 0 && j < a.b.n) atomicAdd(cnt + j, 1u);
+  }
+}
+
+constexpr int kShardThreads = 1024;
+
+// One block: the picked local columns in ascending order (a block scan of the per-thread
+// counts of non-zero multiplicities over contiguous column runs), their weights and α; the
+// multiplicities are cleared for the next draw.
+__global__ void __launch_bounds__(kShardThreads) shard_compact_kernel(
+    const __grid_constant__ ShardArgs a) {
+  griddep_wait();
+  griddep_launch_dependents();
+  __shared__ uint32_t scan[40];
+  const Buffers& b = a.b;
+  const int t = threadIdx.x;
+  const int per = (b.n + kShardThreads - 1) / kShardThreads;
+  const int j0 = t * per, j1 = min(b.n, j0 + per);
+  uint32_t* cnt = b.count[0];
+  uint32_t nz = 0;
+  for (int j = j0; j < j1; ++j) nz += cnt[j] ? 1u : 0u;
+  uint32_t total_nz;
+  uint32_t r = block_exclusive_scan(nz, scan, &total_nz);
+  const double total = __ldg(a.cdf + a.n_global - 1);
+  for (int j = j0; j < j1; ++j) {
+    const uint32_t mult = cnt[j];
+    if (!mult) continue;
+    const int jg = j + a.col0;
+    const double step = __ldg(a.cdf + jg) - (jg > 0 ? __ldg(a.cdf + jg - 1) : 0.0);
+    b.wl_col[0][r] = (uint32_t)j;
+    b.wl_wm[0][r] = (float)((double)mult * total / ((double)a.c * step));
+    b.wl_al[0][r] = __ldg(b.alpha + j);
+    cnt[j] = 0u;
+    ++r;
+  }
+  if (t == 0) b.wl_count[0] = total_nz;
+}
+
 // ------------------------------------------------------------------------------------------
 // Call start / end
 // ------------------------------------------------------------------------------------------
@@ -334,7 +425,7 @@ __global__ void __launch_bounds__(kFinalThreads) finalize_kernel(const __grid_co
     if (a.xdst) a.xdst[k] = __fmul_rn(st.scale, yv);
     if (a.ydst) a.ydst[k] = yv;
   }
-  if (a.cc.uses_amm && !a.cc.sanity) {
+  if (a.cc.uses_amm && !a.cc.sanity && !a.cc.ext_list) {
     // commit: each state advanced once per AMM step that ran
     if (st.used > 0)
       for (int k = gt; k < b.c; k += gs) {
@@ -674,6 +765,30 @@ cudaError_t launch_build_cdf(const Buffers& b, int which, int keep_cdf, int sani
     if (e != cudaSuccess) return e;
   }
   return launch_pdl(cdf_scan_kernel, grid, dim3(kCdfThreads), s, b, w0, keep_cdf, sanity);
+}
+
+cudaError_t launch_shard_worklist(const Buffers& b, const double* cdf, int n_global, int col0,
+                                  const uint32_t* st_in, uint32_t* st_out, int c, cudaStream_t s) {
+  ShardArgs a{};
+  a.b = b;
+  a.cdf = cdf;
+  a.n_global = n_global;
+  a.col0 = col0;
+  a.st_in = st_in;
+  a.st_out = st_out;
+  a.c = c;
+  int blocks = (c + 255) / 256;
+  if (blocks > 1024) blocks = 1024;
+  cudaError_t e = launch_pdl(shard_draw_kernel, dim3(blocks), dim3(256), s, a);
+  if (e != cudaSuccess) return e;
+  return launch_pdl(shard_compact_kernel, dim3(1), dim3(kShardThreads), s, a);
+}
+
+cudaError_t launch_gather_alpha(const Buffers& b, int64_t count, cudaStream_t s) {
+  int blocks = (int)((count + 255) / 256);
+  if (blocks > 1024) blocks = 1024;
+  if (blocks < 1) blocks = 1;
+  return launch_pdl(gather_alpha_kernel, dim3(blocks), dim3(256), s, b, (int)count);
 }
 
 cudaError_t launch_init(const Buffers& b, const CallCfg& cc, const float* x0, int no_normalize,

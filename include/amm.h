@@ -166,6 +166,31 @@ int amm_core_previousAMM(amm_ctx *ctx, const float *d_x, const float *d_x_memo,
  *   y = y_memo + Σdx·v + (z·dx)·1 + Σ_k w_{s_k}·(A_{s_k} − α_{s_k})·((A_{s_k} − α_{s_k})ᵀdx). */
 int amm_core_proposedAMM(amm_ctx *ctx, const float *d_x, const float *d_x_memo,
                          const float *d_y_memo, float *d_y, uint32_t *d_idx_out, void *stream);
+/* The sampled product over a caller-supplied work list instead of the context's own draw:
+ *   y = y_memo + Σ_k wm_k·A_{cols_k}·(A_{cols_k}ᵀ(x − x_memo))            (method previous)
+ * and the proposed form with the rank-one terms (method proposed), where cols (count distinct
+ * column indices, 1 <= count <= c) and wm (w_j times the multiplicity of column j) are device
+ * arrays — the previousAMM_kernel1+2 / proposedAMM_kernel1+2 product
+ * (core_previousAMM.cuh:163-174,225-232, core_proposedAMM.cuh:195-277) for picks made
+ * elsewhere.  The sampling states are not touched.  An index outside [0, n) contributes
+ * nothing and makes the next status read (amm_get_trace) return AMM_ERR_INVALID_ARGUMENT. */
+int amm_core_list_product(amm_ctx *ctx, int method, const uint32_t *d_cols, const float *d_wm,
+                          int64_t count, const float *d_x, const float *d_x_memo,
+                          const float *d_y_memo, float *d_y, void *stream);
+/* One rank's part of a previous-AMM product over a column-sharded matrix (the reference runs
+ * on one GPU; its sampling and product are pick_index (device_memory.h:506-545) and
+ * previousAMM_kernel1+2 (core_previousAMM.cuh:163-174,225-232)).  The context holds this
+ * rank's n columns, which are global columns [col0, col0 + n) of a matrix with n_global
+ * columns; d_cdf_global is the inclusive FP64 CDF of ‖A_j‖² over all n_global columns (the
+ * same on every rank).  The c states d_states_in are advanced once into d_states_out (may
+ * alias) and c picks drawn from the global CDF; of those that fall in this rank's columns,
+ * column j enters with weight mult_j·total/(c·(cdf[j] − cdf[j−1])), and
+ *   d_y = y_memo + Σ_j w_j·A_j·(A_jᵀ(x − x_memo))
+ * over them.  Summing d_y over the ranks (all but one passing y_memo = NULL) gives the product
+ * of the whole matrix: one all-reduce of m floats per step. */
+int amm_shard_product(amm_ctx *ctx, const double *d_cdf_global, int64_t n_global, int64_t col0,
+                      const uint32_t *d_states_in, uint32_t *d_states_out, const float *d_x,
+                      const float *d_x_memo, const float *d_y_memo, float *d_y, void *stream);
 /* Exact product y = A·(Aᵀ·x) (the two cublasSgemv of powerMethod_by_exact.cuh:37-53). */
 int amm_exact_product(amm_ctx *ctx, const float *d_x, float *d_y, void *stream);
 

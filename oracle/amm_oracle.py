@@ -40,6 +40,7 @@ __all__ = [
     "exact_product", "dot_product_and_generate_x", "normalize", "generate_zv",
     "PowerTrace", "power_method", "reported_eigenvalue", "grad_lambda", "lambda_max_f64",
     "batch_seed_states", "batch_start_block", "batch_cdf", "batch_block_power", "BatchTrace",
+    "shard_cdf", "sharded_weights", "sharded_previous",
 ]
 
 
@@ -563,6 +564,84 @@ def batch_block_power(A, *, K: int, max_iter: int, c: int = 0, states=None, cdf=
     v = X_last @ V[:, order[0]]
     return BatchTrace(ritz=th[order], vector=v / np.linalg.norm(v), picks=picks, kinds=kinds,
                       states=st)
+
+
+# --------------------------------------------------------------------------------------------
+# Column-sharded previous AMM (an extension: the reference runs on one GPU).  Each shard builds
+# the FP64 CDF of ‖A_j‖² over its columns (set_weights and the CDF scan, common.h:34-40 and
+# powerMethod_by_previous.cuh:26-32); the global CDF shifts each shard's by the totals of the
+# shards before it.  Every rank draws the same picks from it (pick_index,
+# device_memory.h:506-545) and multiplies by its own picked columns (previousAMM_kernel1+2,
+# core_previousAMM.cuh:163-174, 225-232); the partial products are summed (one all-reduce).
+# --------------------------------------------------------------------------------------------
+
+def shard_cdf(A_shard) -> np.ndarray:
+    """One shard's FP64 CDF: the prefix of (double)norm_j² with norm_j the FP32 column norm."""
+    _, norm, _ = get_norms(A_shard)
+    n64 = norm.astype(F64)
+    return np.cumsum(n64 * n64, dtype=F64)
+
+
+def sharded_weights(cdf, idx):
+    """The distinct picked columns, and w_j = fl32(mult_j·total/(c·(cdf[j] − cdf[j−1]))) (the
+    realised probability of the draw), for the c picks idx."""
+    cdf = np.asarray(cdf, dtype=F64)
+    cols, mult = np.unique(np.asarray(idx), return_counts=True)
+    c = len(idx)
+    prev = np.where(cols > 0, cdf[np.maximum(cols.astype(np.int64) - 1, 0)], 0.0)
+    step = cdf[cols] - prev
+    w = (mult.astype(F64) * cdf[-1] / (F64(c) * step)).astype(F32)
+    return cols, w
+
+
+def sharded_previous(A, bounds, *, c, states, step, vr_period=0, x0, cdf=None):
+    """The column-sharded previous-AMM power method in one process, shard by shard.
+
+    ``bounds``: the shards' [col0, col1) in rank order.  ``cdf``: the global CDF to draw from
+    (default: the shards' FP64 CDFs shifted by the preceding shards' totals, summed in rank
+    order).  Step i is an exact, memoised step when vr_period > 0 and (i + 1) % vr_period == 0
+    (powerMethod_by_previous.cuh:135-157).  Each shard's partial product is rounded to FP32,
+    and the partials are summed in rank order (y_memo added by the first shard).
+    Returns (eigs, kinds, states, global cdf, the picks of every AMM step).
+    """
+    A = np.asarray(A)
+    if cdf is None:
+        parts, offset = [], 0.0
+        for a, b in bounds:
+            cg = shard_cdf(A[:, a:b])
+            parts.append(cg + offset)
+            offset = offset + float(cg[-1])
+        cdf = np.concatenate(parts)
+    cdf = np.asarray(cdf, dtype=F64)
+    st = np.asarray(states, dtype=U32).copy()
+    m = A.shape[0]
+    x = normalize(x0)
+    x_memo = np.zeros(m, F32)
+    y_memo = np.zeros(m, F32)
+    eigs, kinds, picks = [], [], []
+    for i in range(step):
+        if vr_period > 0 and (i + 1) % vr_period == 0:
+            y = np.zeros(m, F32)
+            for a, b in bounds:
+                y = (y + exact_product(A[:, a:b], x)).astype(F32)
+            x_memo, y_memo = x.copy(), y.copy()
+            kinds.append("exact")
+        else:
+            idx, st = pick_index(cdf, st, c)
+            picks.append(idx)
+            cols, w = sharded_weights(cdf, idx)
+            dx = (np.asarray(x, F32) - x_memo).astype(F64)
+            y = np.zeros(m, F32)
+            for r, (a, b) in enumerate(bounds):
+                sel = (cols >= a) & (cols < b)
+                As = A[:, cols[sel]].astype(F64)
+                tmp = ((As.T @ dx).astype(F32) * w[sel]).astype(F32)
+                part = (y_memo.astype(F64) if r == 0 else 0.0) + As @ tmp.astype(F64)
+                y = (y + part.astype(F32)).astype(F32)
+            kinds.append("previous")
+        lam, _, _, x = dot_product_and_generate_x(x, y)
+        eigs.append(lam)
+    return np.array(eigs), kinds, st, cdf, picks
 
 
 # --------------------------------------------------------------------------------------------
