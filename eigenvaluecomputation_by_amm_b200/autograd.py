@@ -71,11 +71,15 @@ def _solver(key, mats, max_iter, tol, nvec):
 class LambdaMax(torch.autograd.Function):
     @staticmethod
     def forward(ctx, A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-6,
-                nvec: int = 8):
+                nvec: int = 8, route: str = "auto"):
         if not A.is_cuda or A.dtype != torch.float32 or A.dim() != 3:
             raise ValueError("lambda_max expects an FP32 CUDA tensor of shape (B, m, n)")
         B, m, n = A.shape
-        route = _route(A, nvec)
+        if route == "auto":
+            route = _route(A, nvec)
+        elif route not in ("copy", "transposed") or (route == "transposed" and
+                                                     _route(A, nvec) != "transposed"):
+            raise ValueError(f"lambda_max: route {route!r} is not available for this input")
         mats, store = _views(A, route)
         key = (A.device.index, B, m, n, nvec, int(max_iter), float(tol), route)
         solver = _solver(key, mats, max_iter, tol, nvec)
@@ -100,19 +104,21 @@ class LambdaMax(torch.autograd.Function):
             out = torch.empty(B, m, n, dtype=torch.float32, device=ctx.store.device)
             grads = [out[b].t() for b in range(B)]
             solver.grad(grads, scale=g_lam.to(torch.float32), vectors=ctx.vectors)
-            return out, None, None, None
+            return out, None, None, None, None
         ld = ctx.store.shape[2]
         gbuf = torch.empty(B, n, ld, dtype=torch.float32, device=ctx.store.device)
         grads = [gbuf[b].t()[:m] for b in range(B)]
         solver.grad(grads, scale=g_lam.to(torch.float32), vectors=ctx.vectors)
-        return gbuf[:, :, :m].transpose(1, 2), None, None, None
+        return gbuf[:, :, :m].transpose(1, 2), None, None, None, None
 
 
-def lambda_max(A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-6, nvec: int = 8):
+def lambda_max(A: torch.Tensor, max_iter: int = 1000, tol: float = 1e-6, nvec: int = 8,
+               route: str = "auto"):
     """λ_max(A_b·A_bᵀ) (FP64, shape (B,) or scalar) with a libamm backward for A.
 
     Iteration stops at ‖C·v − λ·v‖ <= tol·λ (or max_iter products); the eigenvector, and so the
-    gradient, is then accurate to about tol·λ_1/(λ_1 − λ_2)."""
+    gradient, is then accurate to about tol·λ_1/(λ_1 − λ_2).  ``route``: "auto" (in place as
+    the transposed problem when the input allows it), "copy" or "transposed"."""
     single = A.dim() == 2
-    lam, _ = LambdaMax.apply(A.unsqueeze(0) if single else A, max_iter, tol, nvec)
+    lam, _ = LambdaMax.apply(A.unsqueeze(0) if single else A, max_iter, tol, nvec, route)
     return lam[0] if single else lam

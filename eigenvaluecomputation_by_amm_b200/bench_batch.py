@@ -199,20 +199,25 @@ def grad_report(reps=5, fd_entries=32):
     g = torch.Generator(device="cuda").manual_seed(7)
     A = torch.randn(B, m, n, device="cuda", generator=g)
     A *= torch.exp(0.5 * torch.randn(B, 1, n, device="cuda", generator=g))
-    ts = []
-    for r in range(reps + 1):
-        X = A.clone().requires_grad_(True)
-        torch.cuda.synchronize()
-        e0, e1 = _events()
-        e0.record()
-        lam, iters = LambdaMax.apply(X, 2000, 1e-6, 8)
-        lam.sum().backward()
-        e1.record()
-        e1.synchronize()
-        if r:
-            ts.append(e0.elapsed_time(e1))
+    def timed(route):
+        out = []
+        for r in range(reps + 1):
+            X = A.clone().requires_grad_(True)
+            torch.cuda.synchronize()
+            e0, e1 = _events()
+            e0.record()
+            lam, iters = LambdaMax.apply(X, 2000, 1e-6, 8, route)
+            lam.sum().backward()
+            e1.record()
+            e1.synchronize()
+            if r:
+                out.append(e0.elapsed_time(e1))
+        return out, X, lam, iters
+
+    t_copy, _, _, _ = timed("copy")
+    ts, X, lam, iters = timed("transposed")
     # the backward kernel alone (grad_kernel: reads A, writes ∂λ/∂A; m·n·(4 + 4) bytes each)
-    solver = next(s for k, s in _SOLVERS.items() if k[1:4] == (B, m, n))
+    solver = next(s for k, s in _SOLVERS.items() if k[1:4] == (B, m, n) and k[-1] == "transposed")
     vec = solver.vectors.clone()
     out = torch.empty(B, m, n, device="cuda")
     views = [out[b].t() for b in range(B)]  # the transposed route's layout (rows of A contiguous)
@@ -251,6 +256,8 @@ def grad_report(reps=5, fd_entries=32):
             "config": {"workload": "64 FP32 matrices 512 x 2048, N(0,1) x lognormal(0,0.5) "
                                    "columns, 8-vector block power iteration to ‖Cv − λv‖ <= 1e-6·λ",
                        "timed": f"mean of {reps} calls after a first (solver creation, autotune)"},
+            "route": "transposed (A read in place as Aᵀ: no copy in either pass)",
+            "ms_copy_route": statistics.mean(t_copy),
             "products_per_matrix_max": int(iters.max()),
             "products_per_matrix_min": int(iters.min()),
             "grad_kernel": {"ms": t_grad, "bytes": grad_bytes,

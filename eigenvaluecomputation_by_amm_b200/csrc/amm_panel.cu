@@ -34,6 +34,12 @@ namespace amm {
 
 // column groups of the next step issued at the end of a step's last group
 constexpr int kPrefetchGroups = 2;
+// CTAs of a persistent grid at most (one per SM): the per-CTA scalars of a step are staged
+// in shared memory, 2 per CTA
+constexpr int kMaxGrid = 256;
+// dynamic shared memory a CTA may use: the opt-in maximum less room for the kernel's static
+// shared variables
+constexpr int kSmemBudget = 227 * 1024 - 1024;
 
 struct PanelArgs {
   Buffers b;
@@ -65,7 +71,7 @@ __device__ __forceinline__ double2 warp_red(double2 v) {
 
 // Shared memory carve (byte offsets), identical on host and device.
 struct SmemLayout {
-  int stages, bars, redw, wl_idx, wl_w, wl_al, nxt, red, epi, total;
+  int stages, bars, redw, wl_idx, wl_w, wl_al, nxt, red, epi, scal, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup) {
@@ -93,6 +99,8 @@ __host__ __device__ inline SmemLayout smem_layout(const PanelGeom& g, bool setup
   o += 16 * 32 * 32;
   L.epi = o;  // this CTA's first 32 row groups of y_{i-1}, y_memo, v, x_memo, z (float4)
   o += 5 * 32 * 16 + 32 * 32;  // and v* (4 doubles)
+  L.scal = o;  // the per-CTA scalars of the step (Σ α_k t_k or Σ α_j², z·dx): [2][kMaxGrid]
+  o += 2 * kMaxGrid * 8;
   L.total = (o + 127) & ~127;
   return L;
 }
@@ -970,10 +978,24 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     double xy = 0.0, yy = 0.0, yv = 0.0;
     const int NPART = G / CL;  // partial-sum rows: one per CTA, or one per cluster
     constexpr int kU = 10;
+    // The per-CTA scalars (Σ α_k t_k and z·dx of the proposed step, Σ α_j² of the set-up pass)
+    // reach shared memory with one load per thread, issued together with the partial-sum loads
+    // (one L2 round trip); warp 0 then sums them from shared memory in a fixed order.
+    const bool want_s = SETUP || centred;
+    double* scal = reinterpret_cast<double*>(smem + L.scal);
+    auto sval = [&](int k) -> double {  // entry k of [per-CTA scalar | z·dx]
+      if constexpr (SETUP) {
+        return k < G ? __ldcg(b.spart64 + k) : 0.0;
+      } else {
+        return k < G ? (double)__ldcg(b.spart + k) : __ldcg(b.rpart + 4 * (k - G) + 3);
+      }
+    };
     for (int c0 = g0; c0 < g1; c0 += 32) {
       const int gi = c0 + lane;
       const bool first = (c0 == g0);
       double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+      const bool sload = first && want_s && t < 2 * G;
+      const double sreg = sload ? sval(t) : 0.0;
       if (gi < g1) {
         const float* P = b.partials + 4 * (size_t)gi;
         for (int k0 = warp; k0 < NPART; k0 += ncw * kU) {
@@ -984,13 +1006,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
             v[u] = k < NPART ? __ldcg(reinterpret_cast<const float4*>(P + (size_t)k * m))
                              : make_float4(0.f, 0.f, 0.f, 0.f);
           }
-          if (first && k0 == warp && warp == 0 && (SETUP || centred)) {
-            zdx = 0.0;
-            for (int k = lane; k < G; k += 32) {
-              S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
-              if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
-            }
-          }
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
             acc.x += v[u].x;
@@ -999,19 +1014,21 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
             acc.w += v[u].w;
           }
         }
-      } else if (first && warp == 0 && (SETUP || centred)) {
+      }
+      if (sload) scal[t] = sreg;
+      if (first && want_s)  // CTAs of fewer than 2·G threads (small m)
+        for (int k = t + T; k < 2 * G; k += T) scal[k] = sval(k);
+      red[warp * 32 + lane] = acc;
+      named_barrier_or(1, T, false);
+      if (first && warp == 0 && want_s) {  // lane-strided, then a butterfly: the same everywhere
         zdx = 0.0;
         for (int k = lane; k < G; k += 32) {
-          S += SETUP ? __ldcg(b.spart64 + k) : (double)__ldcg(b.spart + k);
-          if (!SETUP) zdx += __ldcg(b.rpart + 4 * k + 3);
+          S += scal[k];
+          if (!SETUP) zdx += scal[G + k];
         }
-      }
-      if (first && warp == 0) {
         S = warp_sum(S);
         zdx = warp_sum(zdx);
       }
-      red[warp * 32 + lane] = acc;
-      named_barrier_or(1, T, false);
       if (warp == 0 && gi < g1) {
         double4 tot = red[lane];
         for (int w = 1; w < ncw; ++w) {
@@ -1135,15 +1152,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         return;
       }
       // λ and the next step, formed by warp 0 from the CTA shares (summed lane-strided and then
-      // by an xor butterfly: the same order in every CTA)
+      // by an xor butterfly: the same order in every CTA); the shares reach shared memory (the
+      // row-reduction scratch, free now) with one load per thread, one L2 round trip
+      double* shares = reinterpret_cast<double*>(red);
+      for (int k = t; k < 3 * G; k += T) shares[k] = __ldcg(b.rpart + 4 * (k / 3) + k % 3);
+      named_barrier_or(1, T, false);
       if (warp == 0) {
         xy = 0.0;
         yy = 0.0;
         yv = 0.0;
         for (int k = lane; k < G; k += 32) {
-          xy += __ldcg(b.rpart + 4 * k + 0);
-          yy += __ldcg(b.rpart + 4 * k + 1);
-          yv += __ldcg(b.rpart + 4 * k + 2);
+          xy += shares[3 * k + 0];
+          yy += shares[3 * k + 1];
+          yv += shares[3 * k + 2];
         }
         xy = warp_sum(xy);
         yy = warp_sum(yy);
@@ -1241,18 +1262,19 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, int cluster, PanelG
   if (fgc > 0) gc = fgc;
   const int stage = gc * colb;
   const int maxlist = c < n ? c : n;
+  if (nsm > kMaxGrid) nsm = kMaxGrid;
   // clusters: the partial y (m floats) must fit one stage, and the ranks' row slices be whole
   // float4 groups
   if (cluster != 2 && cluster != 4 && cluster != 8) cluster = 1;
   if (cluster > 1 && (stage < 4 * m || (m / 4) % cluster != 0 || nsm < 2 * cluster))
     cluster = 1;
   const int grid_min = cluster > 1 ? nsm / 2 : nsm;
-  // the stages take what the rest of the carve leaves of 227 KB (at most 8)
+  // the stages take what the rest of the carve leaves of the budget (at most 8)
   PanelGeom probe{};
   probe.gc = gc;
   probe.wl_cap = (maxlist + grid_min - 1) / grid_min + 1;
   const int rest = smem_layout(probe, true).total;
-  int ns = (227 * 1024 - rest) / stage;
+  int ns = (kSmemBudget - rest) / stage;
   if (ns > 8) ns = 8;
   const int fns = env_int("AMM_PANEL_STAGES", 0);
   if (fns > 0 && fns < ns) ns = fns;
@@ -1274,7 +1296,7 @@ bool panel_geometry(int m, int dtype, int c, int n, int nsm, int cluster, PanelG
   b.wl_cap = probe.wl_cap;
   b.smem_bytes = smem_layout(b, true).total;
   *g = b;
-  return b.smem_bytes <= 227 * 1024;
+  return b.smem_bytes <= kSmemBudget;
 }
 
 // ---- co-residency of the persistent grids ----
@@ -1320,6 +1342,7 @@ static bool coop_with_pdl() {
 }
 
 bool panel_coresident(PanelGeom* g, int nsm) {
+  if (nsm > kMaxGrid) nsm = kMaxGrid;
   int fit = nsm / g->cluster;  // clusters resident at once, over both variants
   for (int setup = 0; setup < 2; ++setup) {
     KernelFn fn;
