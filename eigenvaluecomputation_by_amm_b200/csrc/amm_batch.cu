@@ -383,6 +383,80 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
   __syncwarp();
 }
 
+// ---- variance reduction helpers, out of line so that their registers do not compete with the
+// product loop's ----
+// S = X_memoᵀ·X (FP64 sums over team 0's rows, into Svr) and D = X − X_memo·S into dst, in the
+// layout of X; called by every thread of the CTA.
+template <int K>
+__device__ __noinline__ void vr_difference(const float* Xm, const float* Xs, float* dst,
+                                           double* gpart, float* Svr, int P, int r0, int t,
+                                           int warp, int lane, int team) {
+  const int tw = P / 32;  // warps of team 0
+  if (warp < tw) {
+    for (int ab = 0; ab < K * K; ++ab) {
+      const int va = ab / K, vb = ab % K;
+      double sv = 0.0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        sv = fma((double)Xm[(r0 + e) * K + va], (double)Xs[xs_idx<K>(vb, r0 + e)], sv);
+      sv = warp_sum(sv);
+      if (lane == 0) gpart[warp * K * K + ab] = sv;
+    }
+  }
+  __syncthreads();
+  if (t < K * K) {
+    double sv = 0.0;
+    for (int w = 0; w < tw; ++w) sv += gpart[w * K * K + t];
+    Svr[t] = (float)sv;
+  }
+  __syncthreads();
+  if (team == 0) {
+    for (int e = 0; e < 4; ++e) {
+      float xm[K];
+#pragma unroll
+      for (int v = 0; v < K; ++v) xm[v] = Xm[(r0 + e) * K + v];
+#pragma unroll
+      for (int vb = 0; vb < K; ++vb) {
+        float d = Xs[xs_idx<K>(vb, r0 + e)];
+#pragma unroll
+        for (int va = 0; va < K; ++va) d = fmaf(-xm[va], Svr[va * K + vb], d);
+        dst[xs_idx<K>(vb, r0 + e)] = d;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Y += Y_memo·S over this thread's rows (team 0).
+template <int K>
+__device__ __noinline__ void vr_add_memo(float (&Y)[4][K], const float* Ym, const float* Svr,
+                                         int r0) {
+  for (int e = 0; e < 4; ++e) {
+    float ym[K];
+#pragma unroll
+    for (int v = 0; v < K; ++v) ym[v] = Ym[(r0 + e) * K + v];
+#pragma unroll
+    for (int vb = 0; vb < K; ++vb) {
+      float acc = Y[e][vb];
+#pragma unroll
+      for (int va = 0; va < K; ++va) acc = fmaf(ym[va], Svr[va * K + vb], acc);
+      Y[e][vb] = acc;
+    }
+  }
+}
+
+// The memo pair (X_memo, Y_memo) <- (X, Y) over this thread's rows (team 0).
+template <int K>
+__device__ __noinline__ void vr_store_memo(const float (&Y)[4][K], float* Xm, float* Ym,
+                                           const float* Xs, int r0) {
+  for (int e = 0; e < 4; ++e)
+#pragma unroll
+    for (int v = 0; v < K; ++v) {
+      Xm[(r0 + e) * K + v] = Xs[xs_idx<K>(v, r0 + e)];
+      Ym[(r0 + e) * K + v] = Y[e][v];
+    }
+}
+
 template <int K, int GC>
 __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ Args a) {
   constexpr int NV = K * GC;
@@ -732,43 +806,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       // the sampled product multiplies, D = X − X_memo·S, into yred (free until the team sums
       // after the product); Y_memo·S is added once the product is summed ----
       const bool use_d = wamm && memo;
-      if (use_d) {
-        const int tw = P / 32;  // warps of team 0
-        if (warp < tw) {
-          for (int ab = 0; ab < K * K; ++ab) {
-            const int va = ab / K, vb = ab % K;
-            double sv = 0.0;
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-              sv = fma((double)Xm[(r0 + e) * K + va], (double)Xs[xs_idx<K>(vb, r0 + e)], sv);
-            sv = warp_sum(sv);
-            if (lane == 0) gpart[warp * K * K + ab] = sv;
-          }
-        }
-        __syncthreads();
-        if (t < K * K) {
-          double sv = 0.0;
-          for (int w = 0; w < tw; ++w) sv += gpart[w * K * K + t];
-          Svr[t] = (float)sv;
-        }
-        __syncthreads();
-        if (team == 0) {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            float xm[K];
-#pragma unroll
-            for (int v = 0; v < K; ++v) xm[v] = Xm[(r0 + e) * K + v];
-#pragma unroll
-            for (int vb = 0; vb < K; ++vb) {
-              float d = Xs[xs_idx<K>(vb, r0 + e)];
-#pragma unroll
-              for (int va = 0; va < K; ++va) d = fmaf(-xm[va], Svr[va * K + vb], d);
-              yred[xs_idx<K>(vb, r0 + e)] = d;
-            }
-          }
-        }
-        __syncthreads();
-      }
+      if (use_d) vr_difference<K>(Xm, Xs, yred, gpart, Svr, P, r0, t, warp, lane, team);
       const float* Xsrc = use_d ? yred : Xs;  // the block the product multiplies
       // ---- Y = C·X (or its AMM estimate): the fused pass over the columns (team-local) ----
 #pragma unroll
@@ -926,31 +964,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       }
       // ---- variance reduction: Y = Y_memo·S + Ĉ·D for a sampled product; an exact product
       // becomes the memo pair (team 0, its own rows, in every CTA of the cluster alike) ----
-      if (use_d && team == 0) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          float ym[K];
-#pragma unroll
-          for (int v = 0; v < K; ++v) ym[v] = Ym[(r0 + e) * K + v];
-#pragma unroll
-          for (int vb = 0; vb < K; ++vb) {
-            float acc = Y[e][vb];
-#pragma unroll
-            for (int va = 0; va < K; ++va) acc = fmaf(ym[va], Svr[va * K + vb], acc);
-            Y[e][vb] = acc;
-          }
-        }
-      }
+      if (use_d && team == 0) vr_add_memo<K>(Y, Ym, Svr, r0);
       if (vr && exact_p) {
-        if (team == 0) {
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-#pragma unroll
-            for (int v = 0; v < K; ++v) {
-              Xm[(r0 + e) * K + v] = Xs[xs_idx<K>(v, r0 + e)];
-              Ym[(r0 + e) * K + v] = Y[e][v];
-            }
-        }
+        if (team == 0) vr_store_memo<K>(Y, Xm, Ym, Xs, r0);
         memo = true;
       }
       prev_exact = exact_p;
