@@ -53,7 +53,10 @@ def parse():
     p.add_argument("--no-batch", action="store_true",
                    help="skip the batched (512 matrices) and differentiation (64 x 512x2048) reports")
     p.add_argument("--trace-out", default=None, help="write the calibration λ traces (JSON)")
-    p.add_argument("--seeds", type=int, default=16, help="sampling-state seeds for calibration")
+    p.add_argument("--seeds", type=int, default=32, help="sampling-state seeds for calibration")
+    p.add_argument("--cal-margin", type=float, default=0.5,
+                   help="the schedule and step count are calibrated to end within "
+                        "cal_margin x 1e-3 on every calibration seed")
     p.add_argument("--heldout", type=int, default=16,
                    help="sampling-state seeds, disjoint from the calibration ones, that the "
                         "chosen schedule is checked and timed on")
@@ -370,7 +373,10 @@ def run_ours(args, rank, world):
 
     # ---- proposed AMM BF16: pick the variance-reduction schedule (the reference's periodic
     # -vr period or its -vr_adaptive threshold) and step count S with the shortest measured
-    # time among those whose S-step solve ends within 1e-3 on every calibration seed ----
+    # time among those whose S-step solve ends within cal_margin x 1e-3 on every calibration
+    # seed (the margin keeps a step count that only just passes on the calibration seeds from
+    # being chosen) ----
+    tol_cal = TOL * args.cal_margin
     schedules = [dict(vr_period=P) for P in (2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 24)]
     schedules += [dict(vr_adaptive_threshold=thr) for thr in (3e-2, 1e-2, 3e-3, 1e-3)]
     cands = []
@@ -392,7 +398,7 @@ def run_ours(args, rank, world):
                  else f"adaptive{sched['vr_adaptive_threshold']:g}")
         tr_cal = sched_traces(sched, state_sets)
         traces[f"proposed_{label}"] = {"eigs": tr_cal[0].tolist()}
-        steps = steps_for_final(final_errors(tr_cal, lam_true))
+        steps = steps_for_final(final_errors(tr_cal, lam_true), tol=tol_cal)
         if steps is None:
             continue
         ctx = AMMContext(m, n, c=c, step=steps, dtype="bf16", **sched)
@@ -416,7 +422,7 @@ def run_ours(args, rank, world):
     err_held = final_errors(sched_traces(sched, heldout_sets), lam_true)
     held_at = err_held[:, steps_calibrated - 1]
     heldout = {"seeds": len(heldout_sets), "calibration_seeds": len(state_sets),
-               "steps_calibrated": steps_calibrated,
+               "steps_calibrated": steps_calibrated, "calibration_tol": tol_cal,
                "reached_1e-3_at_calibrated_steps": float(np.mean(held_at < TOL)),
                "rel_err_max_at_calibrated_steps": float(held_at.max()),
                "criterion": "the S-step solve's final λ within 1e-3 of the FP64 λ on every seed"}
@@ -530,15 +536,21 @@ def run_ours(args, rank, world):
             traffic = None
 
     # ---- the configuration's other sample count, 4c (16384 by default; same schedule,
-    # reported beside the headline): steps to 1e-3 over the same state seeds, 3 timed solves ----
+    # reported beside the headline): the step count calibrated as above (margin included), then
+    # checked and timed on held-out seeds like the headline, 3 timed solves ----
     c_big = None
     if not args.no_c_big and c * 4 <= n:
         cb = 4 * c
-        big_sets = [torch.from_numpy(np.random.default_rng(args.seed + 7 + k).integers(
-            1, 2**32, size=cb, dtype=np.uint64).astype(np.uint32).view(np.int32)).to(dev)
-            for k in range(args.seeds)]
-        sb = steps_for_final(final_errors(sched_traces(sched, big_sets, cc=cb), lam_true))
+        big_sets = [seed_states(args.seed + 7 + k, cb) for k in range(args.seeds)]
+        big_held = [seed_states(args.seed + 100_003 + k, cb) for k in range(args.heldout)]
+        err_bc = final_errors(sched_traces(sched, big_sets, cc=cb), lam_true)
+        sb_cal = steps_for_final(err_bc, tol=tol_cal)
+        sb = None
+        if sb_cal is not None:
+            err_bh = final_errors(sched_traces(sched, big_held, cc=cb), lam_true)
+            sb = steps_for_final(np.vstack([err_bc, err_bh]), start=sb_cal)
         if sb is not None:
+            big_sets = big_held  # the timed solves run on the held-out seeds
             cbx = AMMContext(m, n, c=cb, step=sb, dtype="bf16", **sched)
             berrs = []
             tb = []
@@ -557,7 +569,10 @@ def run_ours(args, rank, world):
                     tb.append(e0.elapsed_time(e1))
                     berrs.append(abs(float(trb["eigs"][-1]) - lam_true) / abs(lam_true))
             dist_amm = [int(d) for d, k in zip(trb["distinct"], trb["kinds"]) if k == "proposed"]
-            c_big = {"c": cb, "steps": sb, "exact_vr_steps": trb["kinds"].count("exact"),
+            c_big = {"c": cb, "steps": sb, "steps_calibrated": sb_cal,
+                     "heldout_reached_1e-3_at_calibrated_steps":
+                         float(np.mean(err_bh[:, sb_cal - 1] < TOL)),
+                     "exact_vr_steps": trb["kinds"].count("exact"),
                      "time_to_lambda_ms": statistics.mean(tb), "rel_err_max": max(berrs),
                      "speedup_vs_exact_fp32": ms_exact / statistics.mean(tb),
                      "distinct_columns_per_amm_step": (statistics.mean(dist_amm) if dist_amm

@@ -10,7 +10,8 @@
 // atomic queue.  A matrix of m rows is held by "teams" of P threads (P = smallest power of two
 // >= m/4, at least 32), each thread owning 4 consecutive rows of the K vectors X and of the
 // product Y in registers; the 512/P teams split the columns.  Per group of GC columns a team
-// loads the columns once (coalesced 16-byte loads), forms the K·GC partial dots A_jᵀX over its
+// reads the columns once (coalesced 16-byte cp.async copies into a per-thread shared-memory
+// ring that keeps two or more groups in flight), forms the K·GC partial dots A_jᵀX over its
 // rows, reduces them across the team (warp butterfly, then shared memory for teams wider than a
 // warp) and accumulates Y += A_j·(A_jᵀX): the fused single-pass product of the main kernel.
 // After the pass the team partials of Y are summed in a fixed order, the Gram matrices
@@ -42,6 +43,7 @@ constexpr int kMaxK = 8;
 constexpr int kJacobiSweeps = 16;
 
 constexpr int kMaxCols = 8192;   // AMM mode: the CDF lives in shared memory
+constexpr int kVrSlot = 3;       // VR scratch per CTA: X_memo, Y_memo, saved X
 constexpr int kMaxPicks = 1024;  // AMM mode: c <= n / 8
 
 struct Mat {
@@ -75,7 +77,8 @@ struct Args {
   int32_t vr_period;
   int32_t vr_base;   // first slot of this launch's CTAs in vr_mem (the second launch of a run
                      // is offset past the first one's CTAs)
-  float* vr_mem;     // per CTA slot: X_memo then Y_memo, kMaxRows x K floats each ([row][v])
+  float* vr_mem;     // per CTA slot: X_memo, Y_memo, then X saved while a sampled product
+                     // multiplies D in its place; kMaxRows x K floats each ([row][v])
   // optional record for parity checks (null: none): each matrix's FP32 CDF at col_start[mi]
   // and the raw picks of its AMM product p < rec_products at st_off·rec_products + p·c + k
   float* rec_cdf;
@@ -211,12 +214,21 @@ __device__ void jacobi_warp(double* H, double* V, double* cs, int lane) {
 }
 
 constexpr int align16(int x) { return (x + 15) & ~15; }
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// The column ring of the product pass: every thread copies its own 16 bytes of each column of
+// a group (cp.async, no register staging) RingStages<GC> groups ahead and reads back only what it
+// copied, so the ring needs no barrier.  96 KB: 64 KB in flight per SM at NST = 3.
+constexpr int kRingBytes = 96 * 1024;
+template <int GC>
+struct Ring {
+  static constexpr int stages = kRingBytes / (kThreads * GC * 16);
+};
 
 template <int K>
 struct Smem {
   // byte offsets into dynamic shared memory, each 16-byte aligned
-  static constexpr int yred = 0;                                         // float [4*kThreads][K]
-  static constexpr int part = align16(yred + 4 * kThreads * K * 4);      // float [2][kWarps][32]
+  static constexpr int part = 0;                                         // float [2][kWarps][32]
   static constexpr int bcast = align16(part + 2 * kWarps * 32 * 4);      // float [kWarps][32]
   static constexpr int gpart = align16(bcast + kWarps * 32 * 4);         // double [kWarps][2*K*K]
   static constexpr int gram = align16(gpart + kWarps * 2 * K * K * 8);   // double G[K*K], H[K*K]
@@ -227,15 +239,23 @@ struct Smem {
   static constexpr int ritz = align16(cs + kMaxK * 8);                   // double θ[K], λ
   static constexpr int ctl = align16(ritz + (kMaxK + 1) * 8);            // int [4]
   static constexpr int xs = align16(ctl + 16);                           // float X[K][kMaxRows]
-  static constexpr int total = align16(xs + K * kMaxRows * 4);      // exact mode ends here
-  static constexpr int cdf = total;                                    // float [kMaxCols]
-  static constexpr int hist = align16(cdf + kMaxCols * 4);             // uint32 [kMaxCols]
-  static constexpr int lcol = align16(hist + kMaxCols * 4);            // int32 [kMaxPicks]
+  // one region used in turn by: the column ring during a product pass; the team partials of Y
+  // after it (yred); the block D of a sampled product with variance reduction (yred, during
+  // that product, which then keeps its columns in registers); the pick histogram of an AMM draw
+  // (hist, zeroed at the start of every draw)
+  static constexpr int region = align16(xs + K * kMaxRows * 4);
+  static constexpr int yred = region;                                    // float [4*kThreads][K]
+  static constexpr int hist = align16(yred + 4 * kThreads * K * 4);      // uint32 [kMaxCols]
+  static constexpr int region_bytes = cmax(hist + kMaxCols * 4 - region, kRingBytes);
+  static constexpr int total = align16(region + region_bytes);           // exact mode ends here
+  static constexpr int cdf = total;                                      // float [kMaxCols]
+  static constexpr int lcol = align16(cdf + kMaxCols * 4);               // int32 [kMaxPicks]
   static constexpr int lw = align16(lcol + kMaxPicks * 4);             // float [kMaxPicks]
   static constexpr int scan = align16(lw + kMaxPicks * 4);             // uint32 [40], double[32]
   static constexpr int svr = align16(scan + 40 * 4 + 32 * 8);           // float S[K*K] (VR)
   static constexpr int total_amm = align16(svr + K * K * 4);
-  static_assert(gpart % 8 == 0 && cs % 8 == 0 && xs % 16 == 0, "shared-memory alignment");
+  static_assert(gpart % 8 == 0 && cs % 8 == 0 && xs % 16 == 0 && region % 16 == 0,
+                "shared-memory alignment");
 };
 
 // Sum of the NV values d over the team (P threads).  Returns, in every lane, the total of value
@@ -385,10 +405,11 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
 
 // ---- variance reduction helpers, out of line so that their registers do not compete with the
 // product loop's ----
-// S = X_memoᵀ·X (FP64 sums over team 0's rows, into Svr) and D = X − X_memo·S into dst, in the
-// layout of X; called by every thread of the CTA.
+// S = X_memoᵀ·X (FP64 sums over team 0's rows, into Svr) and D = X − X_memo·S in place of X
+// (X saved to Xsave, [row][v], restored by vr_add_memo after the product); called by every
+// thread of the CTA.
 template <int K>
-__device__ __noinline__ void vr_difference(const float* Xm, const float* Xs, float* dst,
+__device__ __noinline__ void vr_difference(const float* Xm, float* Xs, float* Xsave,
                                            double* gpart, float* Svr, int P, int r0, int t,
                                            int warp, int lane, int team) {
   const int tw = P / 32;  // warps of team 0
@@ -418,20 +439,24 @@ __device__ __noinline__ void vr_difference(const float* Xm, const float* Xs, flo
 #pragma unroll
       for (int vb = 0; vb < K; ++vb) {
         float d = Xs[xs_idx<K>(vb, r0 + e)];
+        Xsave[(r0 + e) * K + vb] = d;
 #pragma unroll
         for (int va = 0; va < K; ++va) d = fmaf(-xm[va], Svr[va * K + vb], d);
-        dst[xs_idx<K>(vb, r0 + e)] = d;
+        Xs[xs_idx<K>(vb, r0 + e)] = d;  // this thread alone reads and writes its rows here
       }
     }
   }
   __syncthreads();
 }
 
-// Y += Y_memo·S over this thread's rows (team 0).
+// Y += Y_memo·S over this thread's rows, and X back in place of D (team 0, once no team
+// multiplies any more).
 template <int K>
 __device__ __noinline__ void vr_add_memo(float (&Y)[4][K], const float* Ym, const float* Svr,
-                                         int r0) {
+                                         const float* Xsave, float* Xs, int r0) {
   for (int e = 0; e < 4; ++e) {
+#pragma unroll
+    for (int v = 0; v < K; ++v) Xs[xs_idx<K>(v, r0 + e)] = Xsave[(r0 + e) * K + v];
     float ym[K];
 #pragma unroll
     for (int v = 0; v < K; ++v) ym[v] = Ym[(r0 + e) * K + v];
@@ -600,8 +625,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     // AMM mode with variance reduction: this CTA's memo slot (CTA-private: every thread reads
     // back only the rows it wrote) and whether it holds an exact product of this matrix
     const bool vr = amm && a.vr_period > 0;
-    float* Xm = a.vr_mem + (size_t)(a.vr_base + blockIdx.x) * (2 * kMaxRows * K);
+    float* Xm = a.vr_mem + (size_t)(a.vr_base + blockIdx.x) * (kVrSlot * kMaxRows * K);
     float* Ym = Xm + kMaxRows * K;
+    float* Xsave = Ym + kMaxRows * K;
     bool memo = false;
     bool prev_exact = false;  // the product the Ritz step of this iteration uses was exact
 
@@ -750,6 +776,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       // distinct ones in ascending order with weight multiplicity / (c·p_j) ----
       int ncols = n;
       if (wamm) {
+        // the histogram shares its memory with the column ring of the last product pass
+        for (int j = t; j < n; j += kThreads) hist[j] = 0u;
+        __syncthreads();
         const float total_f = cdf[n - 1];
         uint32_t* st = a.states + M.st_off;
         // every CTA of the cluster draws the same picks from the same states; rank 0 stores the
@@ -803,11 +832,11 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         __syncthreads();
       }
       // ---- variance reduction: S = X_memoᵀ·X (FP64 sums over team 0's rows) and the block
-      // the sampled product multiplies, D = X − X_memo·S, into yred (free until the team sums
-      // after the product); Y_memo·S is added once the product is summed ----
+      // the sampled product multiplies, D = X − X_memo·S, in place of X; Y_memo·S is added,
+      // and X put back, once the product is summed ----
       const bool use_d = wamm && memo;
-      if (use_d) vr_difference<K>(Xm, Xs, yred, gpart, Svr, P, r0, t, warp, lane, team);
-      const float* Xsrc = use_d ? yred : Xs;  // the block the product multiplies
+      if (use_d) vr_difference<K>(Xm, Xs, Xsave, gpart, Svr, P, r0, t, warp, lane, team);
+      const float* Xsrc = Xs;  // X, or D in its place
       // ---- Y = C·X (or its AMM estimate): the fused pass over the columns (team-local) ----
 #pragma unroll
       for (int e = 0; e < 4; ++e)
@@ -816,31 +845,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       const bool rows = r0 < m;
       const float* __restrict__ Ab = M.A + r0;
       int buf = 0;
-      // this team's columns of group g0 (weights in AMM mode); rows past m (the padding up to
-      // ld) count as zero
-      auto load_group = [&](int g0, float4 (&av)[GC], float (&wt)[GC]) {
-#pragma unroll
-        for (int c = 0; c < GC; ++c) {
-          av[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-          wt[c] = 1.f;
-          const int col = (g0 + c < ncols) ? (wamm ? lcol[g0 + c] : g0 + c) : -1;
-          if (wamm && col >= 0) wt[c] = lw[g0 + c];
-          if (rows && col >= 0)
-            av[c] = __ldcs(reinterpret_cast<const float4*>(Ab + (int64_t)col * M.ld));
-          if (r0 + 1 >= m) av[c].y = 0.f;
-          if (r0 + 2 >= m) av[c].z = 0.f;
-          if (r0 + 3 >= m) av[c].w = 0.f;
-        }
-      };
-      float4 av[GC];
-      float wt[GC];
-      if (gteam * GC < ncols) load_group(gteam * GC, av, wt);
-      for (int g0 = gteam * GC; g0 < ncols; g0 += NTG * GC, buf ^= 1) {
-        // the next group's loads are issued before this group's reduction (one group ahead)
-        float4 nav[GC];
-        float nwt[GC];
-        const bool more = g0 + NTG * GC < ncols;
-        if (more) load_group(g0 + NTG * GC, nav, nwt);
+      // one group of GC columns (weights in AMM mode): the team's dots A_jᵀX over its rows,
+      // their sums over the team, and Y += A_j·(A_jᵀX)·w_j
+      auto multiply = [&](const float4 (&av)[GC], const float (&wt)[GC]) {
         float d[NV];
         if constexpr (K % 2 == 0) {
           // packed FP32x2: a vector pair per instruction (X pairs interleaved in shared memory)
@@ -909,14 +916,48 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
               Y[3][v] = fmaf(av[c].w, tc, Y[3][v]);
             }
         }
-        if (more) {
+      };
+      // rows past m (the padding up to ld) are zero-filled, so are the slots past the list
+      const int gstep = NTG * GC;
+      constexpr int NST = Ring<GC>::stages;
+      static_assert(NST >= 3, "the column ring needs at least 3 stages");
+      // the ring: NST - 1 groups in flight while one is multiplied
+      float4* ring = reinterpret_cast<float4*>(smem + SL::region);
+      const int vbytes = rows ? 4 * min(4, m - r0) : 0;
+      auto issue = [&](int g0, int slot) {
 #pragma unroll
-          for (int c = 0; c < GC; ++c) {
-            av[c] = nav[c];
-            wt[c] = nwt[c];
-          }
+        for (int c = 0; c < GC; ++c) {
+          const int col = (g0 + c < ncols) ? (wamm ? lcol[g0 + c] : g0 + c) : -1;
+          const bool live = vbytes > 0 && col >= 0;
+          cp_async16_zfill(ring + (slot * GC + c) * kThreads + t,
+                           live ? Ab + (int64_t)col * M.ld : M.A, live ? vbytes : 0);
         }
+      };
+      int gi = gteam * GC;  // next group to copy
+#pragma unroll 1
+      for (int s = 0; s < NST - 1; ++s, gi += gstep) {
+        if (gi < ncols) issue(gi, s);
+        cp_async_commit();
       }
+      int slot = 0;
+#pragma unroll 1
+      for (int g0 = gteam * GC; g0 < ncols; g0 += gstep, buf ^= 1) {
+        cp_async_wait_group<NST - 2>();  // group g0 has landed (this thread's copies)
+        // refill the slot this thread emptied in the previous group
+        if (gi < ncols) issue(gi, slot == 0 ? NST - 1 : slot - 1);
+        cp_async_commit();
+        gi += gstep;
+        float4 av[GC];
+        float wt[GC];
+#pragma unroll
+        for (int c = 0; c < GC; ++c) {
+          av[c] = lds_f4(reinterpret_cast<const float*>(ring + (slot * GC + c) * kThreads + t));
+          wt[c] = (wamm && g0 + c < ncols) ? lw[g0 + c] : 1.f;
+        }
+        multiply(av, wt);
+        slot = (slot + 1 == NST) ? 0 : slot + 1;
+      }
+      cp_async_wait_all();  // only empty groups can still be open here
       // ---- sum the team partials of Y (fixed order), every team receives the total ----
       if (NT > 1) {
         __syncthreads();
@@ -964,7 +1005,11 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       }
       // ---- variance reduction: Y = Y_memo·S + Ĉ·D for a sampled product; an exact product
       // becomes the memo pair (team 0, its own rows, in every CTA of the cluster alike) ----
-      if (use_d && team == 0) vr_add_memo<K>(Y, Ym, Svr, r0);
+      if (use_d) {
+        // no team reads X or D any more: every team passed a barrier after its product pass
+        // (team sums, cluster sums) or team 0 is the only team
+        if (team == 0) vr_add_memo<K>(Y, Ym, Svr, Xsave, Xs, r0);
+      }
       if (vr && exact_p) {
         if (team == 0) vr_store_memo<K>(Y, Xm, Ym, Xs, r0);
         memo = true;
@@ -1022,7 +1067,7 @@ struct Variant {
 constexpr int kClusterSizes[] = {1, 2, 4, 8};
 
 static const Variant kVariants[] = {
-    {1, 4, batch_kernel<1, 4>}, {1, 8, batch_kernel<1, 8>}, {4, 2, batch_kernel<4, 2>},
+    {1, 2, batch_kernel<1, 2>}, {1, 4, batch_kernel<1, 4>}, {4, 2, batch_kernel<4, 2>},
     {4, 4, batch_kernel<4, 4>}, {8, 1, batch_kernel<8, 1>}, {8, 2, batch_kernel<8, 2>},
     {8, 4, batch_kernel<8, 4>},
 };
@@ -1475,7 +1520,7 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   // memo pairs of the variance reduction: one slot per CTA that can be resident at once (the
   // launches of a run hold at most one CTA per SM between them)
   const bool with_vr = amm_mode && cfg->vr_period > 0;
-  const size_t vr_floats = (size_t)2 * amm::batch::kMaxRows * cfg->nvec;
+  const size_t vr_floats = (size_t)amm::batch::kVrSlot * amm::batch::kMaxRows * cfg->nvec;
   const size_t o_vr = with_vr ? carve(sizeof(float) * vr_floats * b->nsm, 256) : 0;
   cudaError_t e = cudaMalloc(&b->mem, bytes);
   if (e != cudaSuccess) {

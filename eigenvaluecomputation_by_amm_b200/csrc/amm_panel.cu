@@ -353,9 +353,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   }
   // this thread's rows of y_{j-1} (and of x_memo when it is not known to be zero) for step j
   float4 ypv[R][E / 4], xmv[R][E / 4];
-  // staged: this thread's rows of y_{j-1} were copied ahead into `ystage` (shared memory)
-  auto load_vecs = [&](int j, bool memo, const float4* ystage) {
-    if (ystage) cp_async_wait_all();  // the thread waits only for its own copies
+  auto load_vecs = [&](int j, bool memo) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int vi = t + r * T;
@@ -365,8 +363,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         xmv[r][h4] = ypv[r][h4];
         if (!SETUP && vi < nvec) {
           const int o4 = vi * (E / 4) + h4;
-          ypv[r][h4] = ystage ? ystage[o4]
-                              : __ldcg(reinterpret_cast<const float4*>(b.y[(j + 1) & 1]) + o4);
+          ypv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.y[(j + 1) & 1]) + o4);
           if (memo) xmv[r][h4] = __ldcg(reinterpret_cast<const float4*>(b.x_memo) + o4);
         }
       }
@@ -443,7 +440,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   // first step of the launch, and for each later step right after the state is formed.
   float2 dx[R][H];
   double sum_dx = 0.0;
-  auto prepare = [&](int j, const IterState& sj, const float4* ystage) {
+  auto prepare = [&](int j, const IterState& sj) {
     const bool jamm = sj.mode == kPrevious || sj.mode == kProposed;
     const bool jcentred = sj.mode == kProposed;
     const bool jsampled = jamm && !cc.sanity;
@@ -453,7 +450,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     slice(jsampled, cd_s[jslot], jlo, jhi);
     const int jnb = (int)(jhi - jlo);
     const float* yprev = b.y[(j + 1) & 1];
-    load_vecs(j, jamm && !sj.memo_zero, ystage);
+    load_vecs(j, jamm && !sj.memo_zero);
     if (warp == (ncw > 2 ? 2 : 0)) {
       if (jcentred) {
         double zp = 0.0;
@@ -545,7 +542,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
   };
   if (!SETUP) {
     __syncthreads();  // st_s
-    if (a.iter < a.iter_end && !st_s.done) prepare(a.iter, st_s, nullptr);  // uniform over the grid
+    if (a.iter < a.iter_end && !st_s.done) prepare(a.iter, st_s);  // uniform over the grid
   }
 
   for (int i = a.iter;; ++i) {
@@ -592,10 +589,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
     // peers must be done reading it (already so in practice: two grid barriers lie between)
     if (CL > 1 && npub > 0 && t == 0) {
       if (!mbar_wait_cluster_bounded(&xbar[1], (npub - 1) & 1u)) ok = false;
+      fence_proxy_async_smem();  // generic writes of the partial before the async refill
     }
-    // the stages were last written by ordinary stores (a cluster's partial y, the staged rows
-    // of y) before the async refills below
-    if (!SETUP && t == 0) fence_proxy_async_smem();
     if (t == 0 && ok && ngroups > pre) {  // the first NS groups not already in flight
       uint32_t first[kGcMax * 8];
       const int nf = min(NS * GC, nb);
@@ -1156,26 +1151,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
         if (t == 0) atomicOr(b.status, (uint32_t)kDevTimeout);
         return;
       }
-      // This thread's rows of y_i, which the next step starts from, are copied now into a stage
-      // that no copy uses (at most kPrefetchGroups of the NS >= 3 hold the next step's first
-      // groups; y is m floats <= one stage), in the same round trip as the Rayleigh shares
-      // below instead of after the state is formed.
-      const bool next_here = i + 1 < a.iter_end;
-      float4* ystage = nullptr;
-      if (next_here && stage_bytes >= 4u * (uint32_t)m) {
-        ystage = reinterpret_cast<float4*>(
-            stages + (size_t)((gbase + kPrefetchGroups) % (uint32_t)NS) * stage_bytes);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int vi = t + r * T;
-          if (vi < nvec)
-#pragma unroll
-            for (int h4 = 0; h4 < E / 4; ++h4) {
-              const int o4 = vi * (E / 4) + h4;
-              cp_async16(ystage + o4, reinterpret_cast<const float4*>(ynew) + o4);
-            }
-        }
-      }
       // λ and the next step, formed by warp 0 from the CTA shares (summed lane-strided and then
       // by an xor butterfly: the same order in every CTA); the shares reach shared memory (the
       // row-reduction scratch, free now) with one load per thread, one L2 round trip
@@ -1202,8 +1177,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1)
       }
       named_barrier_or(1, T, false);  // nxs_s
       const IterState nx = nxs_s;
-      if (next_here && !nx.done) prepare(i + 1, nx, ystage);  // uniform over the grid
-      else if (next_here) cp_async_wait_all();  // no copy may land after the step
+      if (i + 1 < a.iter_end && !nx.done) prepare(i + 1, nx);  // uniform over the grid
       if (t == 0) st_s = nx;  // published by the barrier at the top of the next step
     }
   }
