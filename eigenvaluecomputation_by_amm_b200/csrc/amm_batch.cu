@@ -97,12 +97,19 @@ __device__ __forceinline__ float4 lds_f4(const float* p) {
   return v;
 }
 
+// Tensor-core product (exact mode, 8 vectors): X is stored [v][row] with a row stride of 2064
+// floats (516 16-byte chunks, 4 mod 8: the 16-byte fragment loads of vector pairs land on
+// disjoint banks).
+constexpr int kXsStrideTC = kMaxRows + 16;
+
 // Shared-memory position of X[row][v].  For an even block the vectors are interleaved in pairs
 // ([v/2][row][2]) so that a thread's 4 rows of a vector pair are two 16-byte loads holding the
-// float2 operands of the packed FMAs.
-template <int K>
+// float2 operands of the packed FMAs; the tensor-core kernel keeps [v][row].
+template <int K, bool TC = false>
 __device__ __forceinline__ int xs_idx(int v, int row) {
-  if constexpr (K % 2 == 0)
+  if constexpr (TC)
+    return v * kXsStrideTC + row;
+  else if constexpr (K % 2 == 0)
     return (v >> 1) * (2 * kMaxRows) + row * 2 + (v & 1);
   else
     return v * kMaxRows + row;
@@ -225,11 +232,17 @@ struct Ring {
   static constexpr int stages = kRingBytes / (kThreads * GC * 16);
 };
 
-template <int K>
+// Tensor-core product: per warp and stage, 8 columns x 128 rows (4 KB); two stages.
+constexpr int kTcCols = 8;
+constexpr int kTcWarpFloats = kTcCols * 128;
+constexpr int kTcStageFloats = kWarps * kTcWarpFloats;
+
+template <int K, bool TC = false>
 struct Smem {
   // byte offsets into dynamic shared memory, each 16-byte aligned
-  static constexpr int part = 0;                                         // float [2][kWarps][32]
-  static constexpr int bcast = align16(part + 2 * kWarps * 32 * 4);      // float [kWarps][32]
+  static constexpr int part = 0;                  // float [2][kWarps][32] (TC: float2 per lane)
+  static constexpr int bcast = align16(part + 2 * kWarps * 32 * 4 * (TC ? 2 : 1));
+                                                                         // float [kWarps][32]
   static constexpr int gpart = align16(bcast + kWarps * 32 * 4);         // double [kWarps][2*K*K]
   static constexpr int gram = align16(gpart + kWarps * 2 * K * K * 8);   // double G[K*K], H[K*K]
   static constexpr int vmat = align16(gram + 2 * K * K * 8);             // double V[K*K]
@@ -239,14 +252,17 @@ struct Smem {
   static constexpr int ritz = align16(cs + kMaxK * 8);                   // double θ[K], λ
   static constexpr int ctl = align16(ritz + (kMaxK + 1) * 8);            // int [4]
   static constexpr int xs = align16(ctl + 16);                           // float X[K][kMaxRows]
+  static constexpr int xs_bytes = K * (TC ? kXsStrideTC : kMaxRows) * 4;
   // one region used in turn by: the column ring during a product pass; the team partials of Y
   // after it (yred); the block D of a sampled product with variance reduction (yred, during
   // that product, which then keeps its columns in registers); the pick histogram of an AMM draw
   // (hist, zeroed at the start of every draw)
-  static constexpr int region = align16(xs + K * kMaxRows * 4);
+  static constexpr int region = align16(xs + xs_bytes);
   static constexpr int yred = region;                                    // float [4*kThreads][K]
   static constexpr int hist = align16(yred + 4 * kThreads * K * 4);      // uint32 [kMaxCols]
-  static constexpr int region_bytes = cmax(hist + kMaxCols * 4 - region, kRingBytes);
+  static constexpr int region_bytes =
+      TC ? cmax(2 * kTcStageFloats * 4, 4 * kThreads * K * 4)
+         : cmax(hist + kMaxCols * 4 - region, kRingBytes);
   static constexpr int total = align16(region + region_bytes);           // exact mode ends here
   static constexpr int cdf = total;                                      // float [kMaxCols]
   static constexpr int lcol = align16(cdf + kMaxCols * 4);               // int32 [kMaxPicks]
@@ -256,7 +272,33 @@ struct Smem {
   static constexpr int total_amm = align16(svr + K * K * 4);
   static_assert(gpart % 8 == 0 && cs % 8 == 0 && xs % 16 == 0 && region % 16 == 0,
                 "shared-memory alignment");
+  static_assert(!TC || total <= 227 * 1024, "the tensor-core layout exceeds a CTA's shared memory");
 };
+
+// One m16n8k8 TF32 tensor-core product D += A·B (FP32 accumulators), fragments as in the PTX
+// ISA: lane = 4·g + t holds A(g, t), A(g+8, t), A(g, t+4), A(g+8, t+4), B(t, g), B(t+4, g) and
+// D(g, 2t), D(g, 2t+1), D(g+8, 2t), D(g+8, 2t+1).
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, "
+      "{%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// x = hi + lo with hi x rounded to TF32 (11 significant bits, to nearest, ties away: add half
+// an ulp of TF32 to the bit pattern, then clear the 13 low bits) and lo = x - hi, exact in
+// FP32; the tensor core reads lo to 11 bits, so hi + lo carries x to about 2^-21 relative.
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+  const uint32_t h = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
+  hi = h;
+  lo = __float_as_uint(x - __uint_as_float(h));
+}
+
+// Swizzle of the 16-byte chunks of column c (0..7) in a warp's tile: chunk q of column c is
+// stored at q ^ tc_swz(c), so that both fragment loads of the tensor-core product (4 rows of
+// one column per lane; one row of columns 2t / 2t+1 per lane) hit 32 distinct banks.
+__device__ __forceinline__ int tc_swz(int c) { return ((c & 1) << 2) ^ (c & 6); }
 
 // Sum of the NV values d over the team (P threads).  Returns, in every lane, the total of value
 // lane / (32 / NV); the caller gathers value i from lane i·(32 / NV).  Fixed reduction order
@@ -482,11 +524,12 @@ __device__ __noinline__ void vr_store_memo(const float (&Y)[4][K], float* Xm, fl
     }
 }
 
-template <int K, int GC>
+template <int K, int GC, bool TC = false>
 __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ Args a) {
   constexpr int NV = K * GC;
-  static_assert(NV <= 32 && (32 % NV) == 0, "K*GC must divide 32");
-  using SL = Smem<K>;
+  static_assert(TC || (NV <= 32 && (32 % NV) == 0), "K*GC must divide 32");
+  static_assert(!TC || (K == 8 && GC == kTcCols), "the tensor-core product runs 8 vectors");
+  using SL = Smem<K, TC>;
   extern __shared__ __align__(16) unsigned char smem[];
   float* yred = reinterpret_cast<float*>(smem + SL::yred);
   float* part = reinterpret_cast<float*>(smem + SL::part);
@@ -551,7 +594,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     const int gteam = crank * NT + team;
     const int team_warp0 = team * (P / 32);
     const int r0 = 4 * tl;
-    const bool amm = M.c > 0;
+    const bool amm = !TC && M.c > 0;  // the tensor-core kernel runs exact batches only
     double total = 0.0;
     if (amm) {
       // ---- column norms² (get_norms, device_memory.h:34-59) into cdf[], then the CDF ----
@@ -642,7 +685,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
 #pragma unroll
       for (int v = 0; v < K; ++v)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) Xs[xs_idx<K>(v, r0 + e)] = 0.f;
+        for (int e = 0; e < 4; ++e) Xs[xs_idx<K, TC>(v, r0 + e)] = 0.f;
     __syncthreads();
 
     int it = 0, state = 0;  // state: 0 running, 1 converged / last, 2 degenerate
@@ -659,8 +702,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
               float xav[4], xbv[4];
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
-                xav[e] = Xs[xs_idx<K>(a0, r0 + e)];
-                xbv[e] = Xs[xs_idx<K>(b0, r0 + e)];
+                xav[e] = Xs[xs_idx<K, TC>(a0, r0 + e)];
+                xbv[e] = Xs[xs_idx<K, TC>(b0, r0 + e)];
               }
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
@@ -709,7 +752,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
 #pragma unroll
             for (int v = 0; v < K; ++v) {
               yq = fmaf(Y[e][v], qv[v], yq);
-              xq = fmaf(Xs[xs_idx<K>(v, r0 + e)], qv[v], xq);
+              xq = fmaf(Xs[xs_idx<K, TC>(v, r0 + e)], qv[v], xq);
             }
             const double r = (double)yq - lam * (double)xq;
             r2 = fma(r, r, r2);
@@ -742,7 +785,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             if (r0 + e < m) {
               float s = 0.f;
 #pragma unroll
-              for (int v = 0; v < K; ++v) s = fmaf(Xs[xs_idx<K>(v, r0 + e)], qv[v], s);
+              for (int v = 0; v < K; ++v) s = fmaf(Xs[xs_idx<K, TC>(v, r0 + e)], qv[v], s);
               a.vec[M.out_off + r0 + e] = s;
             }
           }
@@ -762,7 +805,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             xj[e] = s;
           }
 #pragma unroll
-          for (int e = 0; e < 4; ++e) Xs[xs_idx<K>(j, r0 + e)] = xj[e];
+          for (int e = 0; e < 4; ++e) Xs[xs_idx<K, TC>(j, r0 + e)] = xj[e];
         }
       }
       __syncthreads();
@@ -838,13 +881,144 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       if (use_d) vr_difference<K>(Xm, Xs, Xsave, gpart, Svr, P, r0, t, warp, lane, team);
       const float* Xsrc = Xs;  // X, or D in its place
       // ---- Y = C·X (or its AMM estimate): the fused pass over the columns (team-local) ----
+      const bool rows = r0 < m;
+      int buf = 0;
+      if constexpr (TC) {
+        // ---- tensor-core pass (exact mode, 8 vectors).  Warp wi of a team owns the team's
+        // rows [128·wi, 128·wi + 128) and copies, per group of 8 columns, only those rows
+        // (cp.async into its own swizzled 4 KB tile, two stages).  Phase 1, per 16-row block:
+        // Tᵀ(16 x 8) += [X_hi | X_lo]ᵀ·A_blk, rows 0-7 of the 16 holding X_hi, rows 8-15 X_lo,
+        // once with A_hi and once with A_lo (all four split terms in two products); the rows of
+        // the block are ordered so that a lane's operands are 4 consecutive rows (one 16-byte
+        // load each of A and X).  The team's warps sum their T (fixed order).  Phase 2, per
+        // 16-row tile: Y += A_tile·T with the 8 columns ordered 0,2,4,6 | 1,3,5,7 along k, so
+        // that the lane's T values are exactly its B operand; three products (A_hi·T_hi,
+        // A_hi·T_lo, A_lo·T_hi). ----
+        const int W = P / 32;               // warps of the team
+        const int wi = tl >> 5;             // this warp's place in the team
+        const int g = lane >> 2, tq = lane & 3;
+        const int rbase = 128 * wi;         // first row of this warp
+        const int nblk = max(0, min(8, (m - rbase + 15) >> 4));  // 16-row blocks below m
+        float* wtile = reinterpret_cast<float*>(smem + SL::region) + warp * kTcWarpFloats;
+        float yacc[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) yacc[i][j] = 0.f;
+        // chunk `lane` (rows rbase + 4·lane .. + 3) of the group's 8 columns; rows past m and
+        // columns past n are zero-filled; chunks of blocks past m are not copied (not read)
+        auto issue = [&](int g0, int st) {
+          float* dst = wtile + st * kTcStageFloats;
+          const int row = rbase + 4 * lane;
+          const int vb = lane < 4 * nblk ? 4 * max(0, min(4, m - row)) : -1;
+#pragma unroll
+          for (int c = 0; c < kTcCols; ++c) {
+            if (vb < 0) continue;
+            const int col = g0 + c;
+            const bool live = vb > 0 && col < ncols;
+            cp_async16_zfill(dst + c * 128 + 4 * (lane ^ tc_swz(c)),
+                             live ? M.A + (int64_t)col * M.ld + row : M.A, live ? vb : 0);
+          }
+        };
+        const int gstep = NTG * kTcCols;
+        int st = 0;
+        if (gteam * kTcCols < ncols) issue(gteam * kTcCols, 0);
+        cp_async_commit();
+#pragma unroll 1
+        for (int g0 = gteam * kTcCols; g0 < ncols; g0 += gstep, buf ^= 1) {
+          if (g0 + gstep < ncols) issue(g0 + gstep, st ^ 1);
+          cp_async_commit();
+          cp_async_wait_group<1>();  // this lane's copies of group g0 have landed
+          __syncwarp();              // ... and every lane's
+          const float* tile = wtile + st * kTcStageFloats;
+          // phase 1: T = AᵀX over this warp's rows
+          float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+          for (int sb = 0; sb < nblk; ++sb) {
+            const float4 av = lds_f4(tile + g * 128 + 4 * ((4 * sb + tq) ^ tc_swz(g)));
+            const float4 xv = lds_f4(Xs + g * kXsStrideTC + rbase + 16 * sb + 4 * tq);
+            uint32_t ah[4], al[4], xh[4], xl[4];
+            tf32_split(av.x, ah[0], al[0]);
+            tf32_split(av.y, ah[1], al[1]);
+            tf32_split(av.z, ah[2], al[2]);
+            tf32_split(av.w, ah[3], al[3]);
+            tf32_split(xv.x, xh[0], xl[0]);
+            tf32_split(xv.y, xh[1], xl[1]);
+            tf32_split(xv.z, xh[2], xl[2]);
+            tf32_split(xv.w, xh[3], xl[3]);
+            // k = tq <-> row 4·tq (+2), k = tq + 4 <-> row 4·tq + 1 (+2)
+            mma_tf32(d, xh[0], xl[0], xh[1], xl[1], ah[0], ah[1]);
+            mma_tf32(d, xh[0], xl[0], xh[1], xl[1], al[0], al[1]);
+            mma_tf32(d, xh[2], xl[2], xh[3], xl[3], ah[2], ah[3]);
+            mma_tf32(d, xh[2], xl[2], xh[3], xl[3], al[2], al[3]);
+          }
+          // lane (g, tq): T[col 2·tq][v g] and T[col 2·tq + 1][v g] (hi and lo rows summed)
+          float t0 = d[0] + d[2], t1 = d[1] + d[3];
+          if (W > 1) {
+            float2* pb = reinterpret_cast<float2*>(part) + buf * kWarps * 32;
+            pb[warp * 32 + lane] = make_float2(t0, t1);
+            named_barrier_or(1 + team, P, false);
+            t0 = 0.f;
+            t1 = 0.f;
+            for (int w = 0; w < W; ++w) {
+              const float2 q = pb[(team_warp0 + w) * 32 + lane];
+              t0 += q.x;
+              t1 += q.y;
+            }
+          }
+          uint32_t th0, tl0, th1, tl1;
+          tf32_split(t0, th0, tl0);
+          tf32_split(t1, th1, tl1);
+          // phase 2: Y += A·T over this warp's 16-row tiles
+          const float* ce = tile + (2 * tq) * 128 + (g & 3);      // column 2·tq
+          const float* co = tile + (2 * tq + 1) * 128 + (g & 3);  // column 2·tq + 1
+          const int se = tc_swz(2 * tq), so = tc_swz(2 * tq + 1);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            if (i >= nblk) break;
+            const int q0 = 4 * i + (g >> 2), q1 = q0 + 2;  // chunks of rows 16i + g, + 8
+            uint32_t ah[4], al[4];
+            tf32_split(ce[4 * (q0 ^ se)], ah[0], al[0]);
+            tf32_split(ce[4 * (q1 ^ se)], ah[1], al[1]);
+            tf32_split(co[4 * (q0 ^ so)], ah[2], al[2]);
+            tf32_split(co[4 * (q1 ^ so)], ah[3], al[3]);
+            mma_tf32(yacc[i], ah[0], ah[1], ah[2], ah[3], th0, th1);
+            mma_tf32(yacc[i], ah[0], ah[1], ah[2], ah[3], tl0, tl1);
+            mma_tf32(yacc[i], al[0], al[1], al[2], al[3], th0, th1);
+          }
+          __syncwarp();  // every lane is done with this stage before it is refilled
+          st ^= 1;
+        }
+        cp_async_wait_all();  // only empty groups can still be open here
+        // the team partials of Y through yred (which shares the tiles' memory), summed over the
+        // teams in a fixed order by team 0
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          if (i >= nblk) break;
+          const int row = team * 4 * P + rbase + 16 * i + g;
+          *reinterpret_cast<float2*>(yred + row * K + 2 * tq) = make_float2(yacc[i][0], yacc[i][1]);
+          *reinterpret_cast<float2*>(yred + (row + 8) * K + 2 * tq) =
+              make_float2(yacc[i][2], yacc[i][3]);
+        }
+        __syncthreads();
+        if (team == 0) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int v = 0; v < K; ++v) {
+              float s = 0.f;
+              if (rows)
+                for (int tm = 0; tm < NT; ++tm) s += yred[((tm * 4 * P) + r0 + e) * K + v];
+              Y[e][v] = s;
+            }
+        }
+      } else {
 #pragma unroll
       for (int e = 0; e < 4; ++e)
 #pragma unroll
         for (int v = 0; v < K; ++v) Y[e][v] = 0.f;
-      const bool rows = r0 < m;
       const float* __restrict__ Ab = M.A + r0;
-      int buf = 0;
       // one group of GC columns (weights in AMM mode): the team's dots A_jᵀX over its rows,
       // their sums over the team, and Y += A_j·(A_jᵀX)·w_j
       auto multiply = [&](const float4 (&av)[GC], const float (&wt)[GC]) {
@@ -958,8 +1132,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
         slot = (slot + 1 == NST) ? 0 : slot + 1;
       }
       cp_async_wait_all();  // only empty groups can still be open here
+      }
       // ---- sum the team partials of Y (fixed order), every team receives the total ----
-      if (NT > 1) {
+      if (!TC && NT > 1) {
         __syncthreads();
         if (rows) {
 #pragma unroll
@@ -1063,17 +1238,24 @@ using KernelFn = void (*)(Args);
 struct Variant {
   int K, GC;
   KernelFn fn;
+  bool tc;  // tensor-core product: exact batches only
 };
 constexpr int kClusterSizes[] = {1, 2, 4, 8};
 
 static const Variant kVariants[] = {
-    {1, 2, batch_kernel<1, 2>}, {1, 4, batch_kernel<1, 4>}, {4, 2, batch_kernel<4, 2>},
-    {4, 4, batch_kernel<4, 4>}, {8, 1, batch_kernel<8, 1>}, {8, 2, batch_kernel<8, 2>},
-    {8, 4, batch_kernel<8, 4>},
+    {1, 2, batch_kernel<1, 2>, false},
+    {1, 4, batch_kernel<1, 4>, false},
+    {4, 2, batch_kernel<4, 2>, false},
+    {4, 4, batch_kernel<4, 4>, false},
+    {8, 1, batch_kernel<8, 1>, false},
+    {8, 2, batch_kernel<8, 2>, false},
+    {8, 4, batch_kernel<8, 4>, false},
+    {8, kTcCols, batch_kernel<8, kTcCols, true>, true},
 };
 
-static int smem_bytes(int K, bool amm) {
-  switch (K) {
+static int smem_bytes(const Variant& V, bool amm) {
+  if (V.tc) return Smem<8, true>::total;
+  switch (V.K) {
     case 1: return amm ? Smem<1>::total_amm : Smem<1>::total;
     case 4: return amm ? Smem<4>::total_amm : Smem<4>::total;
     default: return amm ? Smem<8>::total_amm : Smem<8>::total;
@@ -1161,7 +1343,7 @@ struct Guard {
 // that cluster size cannot run.
 int max_clusters(amm_batch* b, int variant, int cl) {
   const auto& V = amm::batch::kVariants[variant];
-  const int sm = amm::batch::smem_bytes(V.K, b->amm);
+  const int sm = amm::batch::smem_bytes(V, b->amm);
   if (cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
     return 0;
   if (cl > 1 &&
@@ -1213,7 +1395,7 @@ int launch_kernel(amm_batch* b, int variant, int cl, int grid, double* d_lam, fl
                   const int32_t* order0, int count0, bool dependent, cudaStream_t s,
                   int vr_base = 0) {
   const auto& V = amm::batch::kVariants[variant];
-  const int sm = amm::batch::smem_bytes(V.K, b->amm);
+  const int sm = amm::batch::smem_bytes(V, b->amm);
   BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   if (cl > 1)
     BATCH_CUDA(cudaFuncSetAttribute(V.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -1349,6 +1531,7 @@ int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaSt
   std::vector<std::tuple<int, int, int>> cand;  // (variant, cluster size, grid)
   for (int v = 0; v < n_var; ++v) {
     if (amm::batch::kVariants[v].K != b->cfg.nvec) continue;
+    if (amm::batch::kVariants[v].tc && b->amm) continue;  // the tensor-core kernel is exact-only
     if (b->cfg.tile_gc > 0 && amm::batch::kVariants[v].GC != b->cfg.tile_gc) continue;
     for (int cl : amm::batch::kClusterSizes) {
       if (b->cfg.cluster > 0 && cl != b->cfg.cluster) continue;

@@ -267,7 +267,9 @@ typedef struct amm_batch_config {
   double tol;         /* stop when ‖C·v − λ_max·v‖ <= tol·λ_max (v: the top Ritz vector)  */
   uint64_t seed;      /* start block (counter-based hash of seed, matrix, row, vector)    */
   int32_t use_graph;  /* replay the launch from a CUDA graph                             */
-  int32_t tile_gc;    /* columns per group; 0 lets the autotuner choose                  */
+  int32_t tile_gc;    /* columns per group; 0 lets the autotuner choose; 8 (nvec = 8,     */
+                      /* exact products only) is the tensor-core product: TF32 mma.sync   */
+                      /* with a hi/lo split of A, X and AᵀX (about FP32 accuracy)          */
   int32_t c_divisor;  /* 0: exact products; k > 0: previous-AMM products with c = n/k      */
                       /* samples per step (n <= 8192, c <= 1024), drawn as pick_index does */
                       /* from a seeded xorshift32 state per sample, every run from the seed */

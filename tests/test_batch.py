@@ -109,8 +109,57 @@ def test_batch_ritz_values_and_one_launch_per_matrix(amm_lib):
         assert abs(got[0] - w[0]) <= 1e-5 * w[0]
         np.testing.assert_allclose(got[1:], w[1:], rtol=2e-3)
     k, gc, cl = bs.tile_choice()
-    assert k == 8 and gc in (1, 2, 4) and cl in (1, 2, 4, 8)
+    assert k == 8 and gc in (1, 2, 4, 8) and cl in (1, 2, 4, 8)
     assert int(bs.iters.max()) < 3000  # stopped on the residual, not on max_iter
+    bs.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cluster", [1, 2])
+def test_batch_tensor_core_product_vs_fp64(amm_lib, cluster):
+    """The tensor-core product (8 columns per group, TF32 mma.sync with A, X and AᵀX split into
+    hi + lo parts) reaches the accuracy of the CUDA-core product: λ within 1e-5 of FP64 at the
+    1e-6 residual, |v·v*| > 1 - 2e-5; at a fixed 20 products its Ritz values agree with the
+    CUDA-core product's within 1e-5 (relative to λ_max)."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver
+    host = _mats(SIZES, seed=5)
+    keep = [_device_col_major(A) for A in host]
+    mats = [v for _, v in keep]
+    tc = BatchSolver(mats, nvec=8, max_iter=3000, tol=1e-6, tile_gc=8, cluster=cluster)
+    lam, _, iters = tc.run()
+    torch.cuda.synchronize()
+    assert tc.tile_choice() == (8, 8, cluster)
+    lam = lam.cpu().numpy()
+    it = iters.cpu().numpy()
+    for i, A in enumerate(host):
+        w, V = _eigh_top(A)
+        assert 0 < it[i] < 3000
+        assert abs(lam[i] - w[0]) <= 1e-5 * w[0], (i, lam[i], w[0], it[i])
+        v = tc.vector(i).cpu().numpy().astype(np.float64)
+        assert abs(float(v @ V[:, 0])) > 1 - 2e-5, i
+    tc.close()
+    fixed = {}
+    for gc in (8, 4):
+        bs = BatchSolver(mats, nvec=8, max_iter=20, tol=0.0, tile_gc=gc, cluster=cluster)
+        bs.run()
+        torch.cuda.synchronize()
+        fixed[gc] = bs.lam.cpu().numpy()
+        assert (bs.iters.cpu().numpy() == 20).all()
+        bs.close()
+    scale = fixed[4][:, :1]
+    assert np.all(np.abs(fixed[8] - fixed[4]) <= 1e-5 * scale), np.abs(fixed[8] - fixed[4]).max()
+
+
+@pytest.mark.gpu
+def test_batch_tensor_core_product_is_exact_mode_only(amm_lib):
+    """AMM batches have no tensor-core product: asking for it is UNSUPPORTED at the first run."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver, _lib
+    host = _mats(SIZES[:2], seed=1)
+    keep = [_device_col_major(A) for A in host]
+    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=4, tol=0.0, c_divisor=8, tile_gc=8)
+    with pytest.raises(_lib.AmmError) as err:
+        bs.run()
+    assert err.value.status == _lib.AMM_ERR_UNSUPPORTED
     bs.close()
 
 
