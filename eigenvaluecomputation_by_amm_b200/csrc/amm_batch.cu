@@ -946,11 +946,17 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             tf32_split(xv.y, xh[1], xl[1]);
             tf32_split(xv.z, xh[2], xl[2]);
             tf32_split(xv.w, xh[3], xl[3]);
-            // k = tq <-> row 4·tq (+2), k = tq + 4 <-> row 4·tq + 1 (+2)
-            mma_tf32(d, xh[0], xl[0], xh[1], xl[1], ah[0], ah[1]);
-            mma_tf32(d, xh[0], xl[0], xh[1], xl[1], al[0], al[1]);
-            mma_tf32(d, xh[2], xl[2], xh[3], xl[3], ah[2], ah[3]);
-            mma_tf32(d, xh[2], xl[2], xh[3], xl[3], al[2], al[3]);
+            // k = tq <-> row 4·tq (+2), k = tq + 4 <-> row 4·tq + 1 (+2); the block's four
+            // products start from zero and the block sums are added in FP32 with rounding to
+            // nearest (the tensor core's own accumulation is not rounded to nearest, and a long
+            // chain of it drifts: 1e-5 relative over a 2048-row pass)
+            float db[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_tf32(db, xh[0], xl[0], xh[1], xl[1], ah[0], ah[1]);
+            mma_tf32(db, xh[0], xl[0], xh[1], xl[1], al[0], al[1]);
+            mma_tf32(db, xh[2], xl[2], xh[3], xl[3], ah[2], ah[3]);
+            mma_tf32(db, xh[2], xl[2], xh[3], xl[3], al[2], al[3]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) d[j] += db[j];
           }
           // lane (g, tq): T[col 2·tq][v g] and T[col 2·tq + 1][v g] (hi and lo rows summed)
           float t0 = d[0] + d[2], t1 = d[1] + d[3];
@@ -982,9 +988,14 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             tf32_split(ce[4 * (q1 ^ se)], ah[1], al[1]);
             tf32_split(co[4 * (q0 ^ so)], ah[2], al[2]);
             tf32_split(co[4 * (q1 ^ so)], ah[3], al[3]);
-            mma_tf32(yacc[i], ah[0], ah[1], ah[2], ah[3], th0, th1);
-            mma_tf32(yacc[i], ah[0], ah[1], ah[2], ah[3], tl0, tl1);
-            mma_tf32(yacc[i], al[0], al[1], al[2], al[3], th0, th1);
+            // three products from zero (small terms first), then one rounded FP32 add per
+            // element into Y, which sums over every group of the pass
+            float dt[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_tf32(dt, al[0], al[1], al[2], al[3], th0, th1);
+            mma_tf32(dt, ah[0], ah[1], ah[2], ah[3], tl0, tl1);
+            mma_tf32(dt, ah[0], ah[1], ah[2], ah[3], th0, th1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) yacc[i][j] += dt[j];
           }
           __syncwarp();  // every lane is done with this stage before it is refilled
           st ^= 1;

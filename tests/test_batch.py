@@ -151,6 +151,28 @@ def test_batch_tensor_core_product_vs_fp64(amm_lib, cluster):
 
 
 @pytest.mark.gpu
+def test_batch_tensor_core_product_long_passes(amm_lib):
+    """Long passes (up to 8192 columns, 1024 groups of 8 in one CTA): the tensor core's own
+    accumulation is not rounded to nearest, so the product keeps every chain of tensor-core
+    products short and sums them in FP32.  λ after 20 products stays within 1e-6 of FP64 (a
+    single accumulator through the whole pass drifted to 6e-6 .. 4e-5 on these matrices)."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver
+    sizes = [(1024, 8192), (2048, 4096), (300, 6000)]
+    rng = np.random.default_rng(11)
+    host = [(rng.standard_normal((m, n)) * np.exp(rng.standard_normal(n))[None, :]).astype(np.float32)
+            for m, n in sizes]
+    keep = [_device_col_major(A) for A in host]
+    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=20, tol=0.0, tile_gc=8, cluster=1)
+    bs.run()
+    torch.cuda.synchronize()
+    lam = bs.lam[:, 0].cpu().numpy()
+    for i, A in enumerate(host):
+        w, _ = _eigh_top(A)
+        assert abs(lam[i] - w[0]) <= 1e-6 * w[0], (i, lam[i], w[0])
+    bs.close()
+
+
+@pytest.mark.gpu
 def test_batch_tensor_core_product_is_exact_mode_only(amm_lib):
     """AMM batches have no tensor-core product: asking for it is UNSUPPORTED at the first run."""
     from eigenvaluecomputation_by_amm_b200 import BatchSolver, _lib
