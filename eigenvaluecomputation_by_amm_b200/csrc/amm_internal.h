@@ -21,8 +21,9 @@ constexpr int kCdfTile = 1024;     // columns per block of the CDF construction
 // AMM work lists drawn ahead.  The picks of an AMM step depend only on the sampling states and
 // the CDF, never on x, so the lists of up to kListWindow consecutive AMM steps are drawn and
 // compacted together before the first of them (one refill every kListWindow steps); list a of a
-// call (its a-th AMM step) lives in slot a % kListWindow.
-constexpr int kListWindow = 8;
+// call (its a-th AMM step) lives in slot a % kListWindow.  16 covers the solves the bench's
+// schedules need (7 to 9 steps) in one persistent step launch; a slot costs 4·n + 16·c bytes.
+constexpr int kListWindow = 16;
 
 // Iteration state, by iteration parity: a launch of the step kernel covering steps [i0, i1)
 // reads st[i0 & 1] and leaves the state after its last step in st[i1 & 1] (the sampler's refill

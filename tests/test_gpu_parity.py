@@ -199,6 +199,35 @@ def test_power_method_trace(method, kw, use_graph):
     assert vec_rel(x.cpu().numpy(), ref.x) < 1e-4
 
 
+@pytest.mark.parametrize("method,kw", [("previous", dict(vr_period=4)),
+                                       ("proposed", dict(vr_period=7)),
+                                       ("proposed", dict(vr_adaptive_threshold=1e-2)),
+                                       ("proposed_v2", dict(vr_period=5))])
+def test_power_method_trace_many_windows(method, kw):
+    """40 steps: the work lists are drawn 16 AMM steps at a time, so the call refills its list
+    window twice and reuses every slot; the trace, kinds and final states still follow the
+    oracle step for step."""
+    m, n, c, step = 512, 2048, 256, 40
+    A = scaled_gaussian(m, n, seed=51, shift=0.05)
+    ctx = ctx_for(A, c=c, step=step, **kw)
+    st = states(c, 52)
+    ctx.set_rng_state(tu32(st))
+    x0 = np.random.default_rng(53).standard_normal(m).astype(np.float32)
+    vstar = np.linalg.eigh(A.astype(np.float64) @ A.astype(np.float64).T)[1][:, -1]
+    ctx.set_eigenvector(torch.from_numpy(vstar))
+    ctx.power_method(method, t32(x0))
+    tr = ctx.trace()
+    ref = O.power_method(A, x0, method=method, step=step, c=c, states=st, vstar=vstar, **kw)
+    thr = kw.get("vr_adaptive_threshold", 0.0)
+    if thr and np.min(np.abs(ref.coss - (1 - thr))) < 1e-6:
+        pytest.skip("a cos lies within FP32 noise of the threshold")
+    assert tr["steps_run"] == step
+    assert tr["kinds"] == ref.modes
+    assert sum(k != "exact" for k in ref.modes) > 16
+    assert np.all(rel(tr["eigs"], ref.eigs) < RTOL_LAMBDA_F32), (tr["eigs"], ref.eigs)
+    assert np.array_equal(np_u32(ctx.get_rng_state(c)), ref.states[:c])
+
+
 EDGE_SHAPES = [(4, 1, 1), (8, 3, 5), (12, 37, 37), (1028, 513, 64), (16, 100003, 4096)]
 
 
