@@ -20,6 +20,8 @@
 // largest eigenvalue is λ_max, its eigenvector q gives v = X·q.
 
 #include <cooperative_groups.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -85,6 +87,9 @@ struct Args {
   uint32_t* rec_picks;
   int32_t rec_products;
   const int64_t* col_start;
+  // tensor-core kernel: one tensor map per matrix (FP32 {m rows, n columns}, 32 x 8 boxes,
+  // 128-byte swizzle, zero fill outside the matrix), encoded on the host
+  const CUtensorMap* tmaps;
 };
 
 // A shared-memory float4 load the compiler keeps in place (X is re-read per column group
@@ -170,10 +175,28 @@ __device__ void jacobi_warp(double* H, double* V, double* cs, int lane) {
         const double hpq = H[p * K + q];
         double c = 1.0, s = 0.0;
         if (hpq != 0.0) {
-          const double tau = (H[q * K + q] - H[p * K + p]) / (2.0 * hpq);
-          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-          c = 1.0 / sqrt(1.0 + tt * tt);
-          s = tt * c;
+          // t = tan θ = sign(d)·b / (|d| + sqrt(d² + b²)), d = h_qq − h_pp, b = 2·h_pq (the
+          // annihilating angle), to FP32 accuracy from d and b scaled by an exact power of two
+          // (max(|d|, |b|) in [1, 2)); (c, s) = (1, t)/sqrt(1 + t²) in FP32, then two Newton
+          // steps x <- x·(3 − (c² + s²))/2 in FP64 make the rotation orthogonal to FP64
+          // rounding.  An angle off by FP32 rounding leaves h_pq at ~1e-7 of its size instead of
+          // 0, which the next sweep removes; the eigenvalues depend only on the orthogonality.
+          const double dd = H[q * K + q] - H[p * K + p], bb = 2.0 * hpq;
+          const double mx = fmax(fabs(dd), fabs(bb));
+          const int ex = (int)((__double_as_longlong(mx) >> 52) & 0x7ff);
+          const double sc = __longlong_as_double((long long)(2046 - min(ex, 2045)) << 52);
+          const float df = (float)(dd * sc), bf = (float)(bb * sc);
+          const float tf = copysignf(1.f, df) *
+                           __fdividef(bf, fabsf(df) + sqrtf(fmaf(df, df, bf * bf)));
+          const float cf = rsqrtf(fmaf(tf, tf, 1.f));
+          c = (double)cf;
+          s = (double)(tf * cf);
+#pragma unroll
+          for (int nw = 0; nw < 2; ++nw) {
+            const double f = fma(-0.5, fma(c, c, s * s), 1.5);
+            c *= f;
+            s *= f;
+          }
         }
         cs[2 * lane] = c;
         cs[2 * lane + 1] = s;
@@ -221,6 +244,7 @@ __device__ void jacobi_warp(double* H, double* V, double* cs, int lane) {
 }
 
 constexpr int align16(int x) { return (x + 15) & ~15; }
+constexpr int align1024(int x) { return (x + 1023) & ~1023; }
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 // The column ring of the product pass: every thread copies its own 16 bytes of each column of
@@ -251,13 +275,15 @@ struct Smem {
   static constexpr int cs = align16(qv + K * 4);                         // double cs[kMaxK]
   static constexpr int ritz = align16(cs + kMaxK * 8);                   // double θ[K], λ
   static constexpr int ctl = align16(ritz + (kMaxK + 1) * 8);            // int [4]
-  static constexpr int xs = align16(ctl + 16);                           // float X[K][kMaxRows]
+  static constexpr int tbar = align16(ctl + 16);  // uint64 [kWarps][2]: tensor-core tile copies
+  static constexpr int xs = align16(tbar + kWarps * 2 * 8);              // float X[K][kMaxRows]
   static constexpr int xs_bytes = K * (TC ? kXsStrideTC : kMaxRows) * 4;
   // one region used in turn by: the column ring during a product pass; the team partials of Y
   // after it (yred); the block D of a sampled product with variance reduction (yred, during
   // that product, which then keeps its columns in registers); the pick histogram of an AMM draw
   // (hist, zeroed at the start of every draw)
-  static constexpr int region = align16(xs + xs_bytes);
+  // (tensor-core kernel: 1024-byte aligned, as the 128-byte swizzle of its tile copies needs)
+  static constexpr int region = TC ? align1024(xs + xs_bytes) : align16(xs + xs_bytes);
   static constexpr int yred = region;                                    // float [4*kThreads][K]
   static constexpr int hist = align16(yred + 4 * kThreads * K * 4);      // uint32 [kMaxCols]
   static constexpr int region_bytes =
@@ -295,10 +321,6 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) 
   lo = __float_as_uint(x - __uint_as_float(h));
 }
 
-// Swizzle of the 16-byte chunks of column c (0..7) in a warp's tile: chunk q of column c is
-// stored at q ^ tc_swz(c), so that both fragment loads of the tensor-core product (4 rows of
-// one column per lane; one row of columns 2t / 2t+1 per lane) hit 32 distinct banks.
-__device__ __forceinline__ int tc_swz(int c) { return ((c & 1) << 2) ^ (c & 6); }
 
 // Sum of the NV values d over the team (P threads).  Returns, in every lane, the total of value
 // lane / (32 / NV); the caller gathers value i from lane i·(32 / NV).  Fixed reduction order
@@ -388,13 +410,18 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
     double tr = 0.0;
     for (int i = 0; i < K; ++i) tr += Gp[i * K + i];
     bool ok = tr > 0.0 && isfinite(tr);
-    // Cholesky, column by column: the diagonal by lane 0, the column below it by lanes j+1..
+    // Cholesky, column by column: the diagonal by lane 0, the column below it by lanes j+1..;
+    // one reciprocal square root per column gives both L_jj = d·d^(-1/2) and 1/L_jj (kept in
+    // Ri, which takes T's place: T is dead once Gp is formed), so no step divides
+    double* Ri = T;
     for (int j = 0; j < K && ok; ++j) {
       if (lane == 0) {
         double d = Gp[j * K + j];
         for (int k = 0; k < j; ++k) d -= L[j * K + k] * L[j * K + k];
         const bool good = d > 1e-24 * tr;
-        L[j * K + j] = good ? sqrt(d) : 0.0;
+        const double r = good ? rsqrt(d) : 0.0;
+        L[j * K + j] = good ? d * r : 0.0;
+        Ri[j] = r;
         cs[0] = good ? 1.0 : 0.0;
       }
       __syncwarp();
@@ -403,7 +430,7 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
         const int i = lane;
         double sv = Gp[i * K + j];
         for (int k = 0; k < j; ++k) sv -= L[i * K + k] * L[j * K + k];
-        L[i * K + j] = sv / L[j * K + j];
+        L[i * K + j] = sv * Ri[j];
       }
       __syncwarp();
     }
@@ -414,11 +441,11 @@ __device__ __noinline__ void ritz_step(const Args& a, int mi, int it, double* Gm
       if (lane < K) {
         const int j = lane;
         for (int i = 0; i < K; ++i) Li[i * K + j] = 0.0;
-        Li[j * K + j] = 1.0 / L[j * K + j];
+        Li[j * K + j] = Ri[j];
         for (int i = j + 1; i < K; ++i) {
           double sv = 0.0;
           for (int k = j; k < i; ++k) sv += L[i * K + k] * Li[k * K + j];
-          Li[i * K + j] = -sv / L[i * K + i];
+          Li[i * K + j] = -sv * Ri[i];
         }
       }
       __syncwarp();
@@ -524,6 +551,135 @@ __device__ __noinline__ void vr_store_memo(const float (&Y)[4][K], float* Xm, fl
     }
 }
 
+// One FP64 tensor-core product D += A·B (m8n8k4, FP64 accumulation), fragments as in the PTX
+// ISA: lane = 4·g + t holds A(g, t), B(t, g), D(g, 2t) and D(g, 2t+1).
+__device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+// Gram matrices of the block, G = YᵀY and H = sym(XᵀY), in FP64 over team 0's rows (the only
+// team holding the summed Y, here in shared memory as Ys[row][v]); called by every thread of the
+// CTA.  For 8 vectors each warp of team 0 multiplies its 128 rows on the FP64 tensor cores: per
+// 4 rows one m8n8k4 product for G (A = Yᵀ, B = Y: lane 4·g + t supplies Y[row t][vector g] to
+// both) and one for XᵀY (A = Xᵀ); FP32 × FP32 products are exact in FP64.  For fewer vectors
+// each thread forms its FP64 partials over its 4 rows, 8 entries at a time, summed over the warp
+// by one multi-value butterfly per 8 entries.  The team's warps are then summed in a fixed
+// order.  Kept out of line so that its registers do not compete with the product loop's.
+template <int K, bool TC>
+__device__ __noinline__ void gram_step(const float* Xs, const float* Ys, double* gpart,
+                                       double* Gm, double* Hm, int P, int r0, int t, int warp,
+                                       int lane, int team) {
+  constexpr int NP = K * (K + 1) / 2;
+  const int tw = P / 32;  // warps of team 0
+  if constexpr (K == 8) {
+    // gpart[warp][0..63]: this warp's G (row-major), [64..127]: its XᵀY
+    if (team == 0) {  // warp-uniform (P >= 32)
+      __syncwarp();   // the warp's rows of Ys were written by its own lanes
+      double dg[2] = {0.0, 0.0}, dh[2] = {0.0, 0.0};
+      const int g = lane >> 2, tq = lane & 3;
+      const int rb = 128 * warp;  // team 0's warp w holds rows [128w, 128w + 128)
+#pragma unroll 4
+      for (int k = 0; k < 32; ++k) {
+        const int row = rb + 4 * k + tq;
+        const double y = (double)Ys[row * K + g];
+        const double x = (double)Xs[xs_idx<K, TC>(g, row)];
+        mma_f64(dg, y, y);
+        mma_f64(dh, x, y);
+      }
+      double* gp = gpart + warp * 2 * K * K;
+      gp[g * K + 2 * tq] = dg[0];
+      gp[g * K + 2 * tq + 1] = dg[1];
+      gp[K * K + g * K + 2 * tq] = dh[0];
+      gp[K * K + g * K + 2 * tq + 1] = dh[1];
+    }
+    __syncthreads();
+    if (t < 2 * NP) {
+      const int which = t / NP, pi = t % NP;
+      int a1 = 0, rem = pi;
+      while (rem >= K - a1) {
+        rem -= K - a1;
+        ++a1;
+      }
+      const int b1 = a1 + rem;
+      double s = 0.0;
+      if (which == 0) {
+        for (int w = 0; w < tw; ++w) s += gpart[w * 2 * K * K + a1 * K + b1];
+      } else {
+        double sa = 0.0, sb = 0.0;
+        for (int w = 0; w < tw; ++w) {
+          sa += gpart[w * 2 * K * K + K * K + a1 * K + b1];
+          sb += gpart[w * 2 * K * K + K * K + b1 * K + a1];
+        }
+        s = 0.5 * (sa + sb);
+      }
+      double* D = which ? Hm : Gm;
+      D[a1 * K + b1] = s;
+      D[b1 * K + a1] = s;
+    }
+    __syncthreads();
+  } else {
+    constexpr int NV2 = 2 * NP;        // G entries (pair index), then H entries
+    constexpr int NB = (NV2 + 7) / 8;  // batches of 8 entries
+    if (team == 0) {                   // warp-uniform (P >= 32)
+      float y[4][K];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+#pragma unroll
+        for (int v = 0; v < K; ++v) y[e][v] = Ys[(r0 + e) * K + v];
+#pragma unroll
+      for (int bt = 0; bt < NB; ++bt) {
+        double d[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[i] = 0.0;
+        int pidx = 0;
+#pragma unroll
+        for (int a0 = 0; a0 < K; ++a0)
+#pragma unroll
+          for (int b0 = a0; b0 < K; ++b0, ++pidx) {
+            if (pidx / 8 == bt) {
+              double gg = 0.0;
+#pragma unroll
+              for (int e = 0; e < 4; ++e) gg = fma((double)y[e][a0], (double)y[e][b0], gg);
+              d[pidx % 8] = gg;
+            }
+            if ((NP + pidx) / 8 == bt) {
+              double h = 0.0;
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const float xa = Xs[xs_idx<K, TC>(a0, r0 + e)];
+                const float xb = Xs[xs_idx<K, TC>(b0, r0 + e)];
+                h = fma(0.5 * (double)xa, (double)y[e][b0], h);
+                h = fma(0.5 * (double)xb, (double)y[e][a0], h);
+              }
+              d[(NP + pidx) % 8] = h;
+            }
+          }
+        const double r = warp_reduce_multi<double, 8>(d, lane);  // entry 8·bt + lane/4
+        const int vi = bt * 8 + (lane >> 2);
+        if ((lane & 3) == 0 && vi < NV2) gpart[warp * NV2 + vi] = r;
+      }
+    }
+    __syncthreads();
+    if (t < NV2) {
+      double s = 0.0;
+      for (int w = 0; w < tw; ++w) s += gpart[w * NV2 + t];
+      const int which = t / NP, pi = t % NP;
+      int a1 = 0, rem = pi;
+      while (rem >= K - a1) {
+        rem -= K - a1;
+        ++a1;
+      }
+      const int b1 = a1 + rem;
+      double* D = which ? Hm : Gm;
+      D[a1 * K + b1] = s;
+      D[b1 * K + a1] = s;
+    }
+    __syncthreads();
+  }
+}
+
 template <int K, int GC, bool TC = false>
 __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ Args a) {
   constexpr int NV = K * GC;
@@ -551,6 +707,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   uint32_t* scan = reinterpret_cast<uint32_t*>(smem + SL::scan);
   double* dscan = reinterpret_cast<double*>(smem + SL::scan + 40 * 4);
   float* Svr = reinterpret_cast<float*>(smem + SL::svr);
+  uint64_t* tbar = reinterpret_cast<uint64_t*>(smem + SL::tbar);
 
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   namespace cg = cooperative_groups;
@@ -558,6 +715,32 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   const int CL = (int)cluster.num_blocks();   // CTAs sharing one matrix
   const int crank = (int)cluster.block_rank();
   const bool writer = (crank == 0);           // rank 0 writes the results
+  // tensor-core kernel: the warps' stage barriers of the tile copies (one arrival each: the
+  // issuing lane's expect_tx).  The tiles' 128-byte swizzle is laid out for a 1024-byte aligned
+  // region (true of a kernel without static shared memory); were it not, no copy is issued and
+  // every matrix is reported without a result.
+  uint32_t tph = 0;         // phase parity of this warp's two stages (alike in every lane)
+  // no more copies in this warp (misaligned region, or a copy that timed out: the warp then
+  // neither issues nor waits, so that later waits cannot time out one after another)
+  bool tdead = TC && (smem_addr(smem + SL::region) & 1023u) != 0u;
+  bool tfail = tdead;       // this pass's product is not to be trusted
+  int tfail_mi = -1;        // the matrix of this CTA that gets no result for that reason
+  if constexpr (TC) {
+    if (t == 0) {
+      for (int i = 0; i < 2 * kWarps; ++i) mbar_init(&tbar[i], 1);
+      fence_barrier_init();
+    }
+    __syncthreads();
+  }
+  // the failure record, written once the cluster is done with the matrix (after the cluster
+  // barrier of the next fetch), so that no result write of a peer comes after it
+  auto record_tfail = [&]() {
+    if (TC && tfail_mi >= 0 && t == 0) {
+      for (int i = 0; i < K; ++i) a.lam[(int64_t)tfail_mi * K + i] = nan("");
+      a.iters[tfail_mi] = -1;
+    }
+    tfail_mi = -1;
+  };
   // a launch queued behind this one as a programmatic dependent may now take the SMs left
   griddep_launch_dependents();
   for (;;) {
@@ -578,6 +761,7 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
     cluster.sync();
     const int mi = *cluster.map_shared_rank(&ctl[0], 0);
     cluster.sync();
+    record_tfail();
     if (mi < 0) {
       // a launch queued behind another (programmatic dependent) ends only after it, so that
       // the work after it in the stream sees both; returns at once in any other launch
@@ -690,57 +874,28 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
 
     int it = 0, state = 0;  // state: 0 running, 1 converged / last, 2 degenerate
     for (;; ++it) {
-      // ---- Gram matrices of the block: G = YᵀY, H = sym(XᵀY) (FP64, team 0 contributes) ----
-      {
-        constexpr int NP = K * (K + 1) / 2;
-        const bool contrib = (team == 0);
-        int pidx = 0;
-        for (int a0 = 0; a0 < K; ++a0)
-          for (int b0 = a0; b0 < K; ++b0, ++pidx) {
-            double g = 0.0, h = 0.0;
-            if (contrib) {
-              float xav[4], xbv[4];
+      // ---- Gram matrices of the block: G = YᵀY, H = sym(XᵀY) (FP64, team 0's rows), from a
+      // shared-memory copy of team 0's Y (each thread reads back only its own rows) ----
+      if (team == 0) {
 #pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                xav[e] = Xs[xs_idx<K, TC>(a0, r0 + e)];
-                xbv[e] = Xs[xs_idx<K, TC>(b0, r0 + e)];
-              }
+        for (int e = 0; e < 4; ++e)
 #pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                g = fma((double)Y[e][a0], (double)Y[e][b0], g);
-                h = fma(0.5 * (double)xav[e], (double)Y[e][b0], h);
-                h = fma(0.5 * (double)xbv[e], (double)Y[e][a0], h);
-              }
-            }
-            g = warp_sum(g);
-            h = warp_sum(h);
-            if (lane == 0) {
-              gpart[warp * 2 * NP + pidx] = g;
-              gpart[warp * 2 * NP + NP + pidx] = h;
-            }
-          }
-        __syncthreads();
-        if (t < 2 * NP) {
-          double s = 0.0;
-          for (int w = 0; w < kWarps; ++w) s += gpart[w * 2 * NP + t];
-          const int which = t / NP, pi = t % NP;
-          int a1 = 0, rem = pi;
-          while (rem >= K - a1) {
-            rem -= K - a1;
-            ++a1;
-          }
-          const int b1 = a1 + rem;
-          double* D = which ? Hm : Gm;
-          D[a1 * K + b1] = s;
-          D[b1 * K + a1] = s;
-        }
-        __syncthreads();
+          for (int v = 0; v < K; ++v) yred[(r0 + e) * K + v] = Y[e][v];
       }
+      gram_step<K, TC>(Xs, yred, gpart, Gm, Hm, P, r0, t, warp, lane, team);
       // (gpart, summed into Gm and Hm above, is the Ritz step's scratch)
       if (warp == 0)
         ritz_step<K>(a, mi, it, Gm, Hm, Vm, cs, ritz, Rinv, qv, ctl, gpart, lane, writer,
                      vr && prev_exact);
       __syncthreads();
+      // team 0's Y back from its shared-memory copy (not held in registers across the two
+      // out-of-line steps, which then get the registers for themselves)
+      if (team == 0) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+          for (int v = 0; v < K; ++v) Y[e][v] = yred[(r0 + e) * K + v];
+      }
       if (ctl[2] && ctl[1] == 0) {
         // residual of the top Ritz pair, r = C·v − λ·v = (Y − λ·X)·q, over team 0's rows (FP64)
         const double lam = ritz[kMaxK];
@@ -885,57 +1040,63 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
       int buf = 0;
       if constexpr (TC) {
         // ---- tensor-core pass (exact mode, 8 vectors).  Warp wi of a team owns the team's
-        // rows [128·wi, 128·wi + 128) and copies, per group of 8 columns, only those rows
-        // (cp.async into its own swizzled 4 KB tile, two stages).  Phase 1, per 16-row block:
-        // Tᵀ(16 x 8) += [X_hi | X_lo]ᵀ·A_blk, rows 0-7 of the 16 holding X_hi, rows 8-15 X_lo,
-        // once with A_hi and once with A_lo (all four split terms in two products); the rows of
-        // the block are ordered so that a lane's operands are 4 consecutive rows (one 16-byte
-        // load each of A and X).  The team's warps sum their T (fixed order).  Phase 2, per
-        // 16-row tile: Y += A_tile·T with the 8 columns ordered 0,2,4,6 | 1,3,5,7 along k, so
-        // that the lane's T values are exactly its B operand; three products (A_hi·T_hi,
-        // A_hi·T_lo, A_lo·T_hi). ----
+        // rows [128·wi, 128·wi + 128); per group of 8 columns its lane 0 copies those rows into
+        // the warp's own 4 KB tile (two stages) with four TMA boxes of 32 rows x 8 columns
+        // (128-byte swizzle: 16-byte chunk q of a column's 32-row line stored at q ^ (column
+        // mod 8); rows past m and columns past n arrive as zeros), completing on the stage's
+        // mbarrier.  Phase 1, per 16-row block: Tᵀ(16 x 8) += [X_hi | X_lo]ᵀ·A_blk, rows 0-7 of
+        // the 16 holding X_hi, rows 8-15 X_lo, once with A_hi and once with A_lo (all four split
+        // terms in two products); the rows of the block are ordered so that a lane's operands are
+        // 4 consecutive rows (one 16-byte load each of A and X).  The team's warps sum their T
+        // (fixed order).  Phase 2, per 16-row tile: Y += A_tile·T with the 8 columns ordered
+        // 0,2,4,6 | 1,3,5,7 along k, so that the lane's T values are exactly its B operand; three
+        // products (A_hi·T_hi, A_hi·T_lo, A_lo·T_hi). ----
         const int W = P / 32;               // warps of the team
         const int wi = tl >> 5;             // this warp's place in the team
         const int g = lane >> 2, tq = lane & 3;
         const int rbase = 128 * wi;         // first row of this warp
         const int nblk = max(0, min(8, (m - rbase + 15) >> 4));  // 16-row blocks below m
+        const int nbox = (nblk + 1) >> 1;   // 32-row boxes below m
         float* wtile = reinterpret_cast<float*>(smem + SL::region) + warp * kTcWarpFloats;
+        uint64_t* wbar = tbar + 2 * warp;   // this warp's stage barriers
+        const CUtensorMap* tmap = a.tmaps + mi;
         float yacc[8][4];
 #pragma unroll
         for (int i = 0; i < 8; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) yacc[i][j] = 0.f;
-        // chunk `lane` (rows rbase + 4·lane .. + 3) of the group's 8 columns; rows past m and
-        // columns past n are zero-filled; chunks of blocks past m are not copied (not read)
         auto issue = [&](int g0, int st) {
-          float* dst = wtile + st * kTcStageFloats;
-          const int row = rbase + 4 * lane;
-          const int vb = lane < 4 * nblk ? 4 * max(0, min(4, m - row)) : -1;
-#pragma unroll
-          for (int c = 0; c < kTcCols; ++c) {
-            if (vb < 0) continue;
-            const int col = g0 + c;
-            const bool live = vb > 0 && col < ncols;
-            cp_async16_zfill(dst + c * 128 + 4 * (lane ^ tc_swz(c)),
-                             live ? M.A + (int64_t)col * M.ld + row : M.A, live ? vb : 0);
+          // (the warp's reads of the stage ended before the __syncwarp that closed the group
+          // which last used it); lane 0 announces the bytes, lanes 0..nbox-1 issue a box each
+          if (nbox > 0 && !tdead) {
+            if (lane == 0) mbar_arrive_expect_tx(&wbar[st], (uint32_t)nbox * 1024u);
+            __syncwarp();
+            if (lane < nbox)
+              tma_load_2d(wtile + st * kTcStageFloats + lane * 256, tmap, rbase + 32 * lane, g0,
+                          &wbar[st]);
           }
         };
+        // every thread's earlier accesses of the tile region (the Gram step's copy of Y, the
+        // team sums of the last pass, its tiles) are ordered before the first copies' writes
+        fence_proxy_async_smem();
+        __syncthreads();
         const int gstep = NTG * kTcCols;
         int st = 0;
         if (gteam * kTcCols < ncols) issue(gteam * kTcCols, 0);
-        cp_async_commit();
 #pragma unroll 1
         for (int g0 = gteam * kTcCols; g0 < ncols; g0 += gstep, buf ^= 1) {
           if (g0 + gstep < ncols) issue(g0 + gstep, st ^ 1);
-          cp_async_commit();
-          cp_async_wait_group<1>();  // this lane's copies of group g0 have landed
-          __syncwarp();              // ... and every lane's
+          if (nbox > 0 && !tdead) {  // group g0 has landed (bounded wait; a timeout marks the matrix)
+            const bool ok = mbar_wait_bounded(&wbar[st], (tph >> st) & 1u);
+            tph ^= 1u << st;
+            if (__any_sync(0xffffffffu, !ok)) tfail = tdead = true;
+          }
           const float* tile = wtile + st * kTcStageFloats;
           // phase 1: T = AᵀX over this warp's rows
           float d[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 2
           for (int sb = 0; sb < nblk; ++sb) {
-            const float4 av = lds_f4(tile + g * 128 + 4 * ((4 * sb + tq) ^ tc_swz(g)));
+            const float4 av = lds_f4(tile + (sb >> 1) * 256 + g * 32 + 4 * ((4 * (sb & 1) + tq) ^ g));
             const float4 xv = lds_f4(Xs + g * kXsStrideTC + rbase + 16 * sb + 4 * tq);
             uint32_t ah[4], al[4], xh[4], xl[4];
             tf32_split(av.x, ah[0], al[0]);
@@ -950,13 +1111,14 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
             // products start from zero and the block sums are added in FP32 with rounding to
             // nearest (the tensor core's own accumulation is not rounded to nearest, and a long
             // chain of it drifts: 1e-5 relative over a 2048-row pass)
-            float db[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_tf32(db, xh[0], xl[0], xh[1], xl[1], ah[0], ah[1]);
-            mma_tf32(db, xh[0], xl[0], xh[1], xl[1], al[0], al[1]);
-            mma_tf32(db, xh[2], xl[2], xh[3], xl[3], ah[2], ah[3]);
-            mma_tf32(db, xh[2], xl[2], xh[3], xl[3], al[2], al[3]);
+            // (two independent chains of two, one per k-half, so that they overlap)
+            float db0[4] = {0.f, 0.f, 0.f, 0.f}, db1[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_tf32(db0, xh[0], xl[0], xh[1], xl[1], ah[0], ah[1]);
+            mma_tf32(db1, xh[2], xl[2], xh[3], xl[3], ah[2], ah[3]);
+            mma_tf32(db0, xh[0], xl[0], xh[1], xl[1], al[0], al[1]);
+            mma_tf32(db1, xh[2], xl[2], xh[3], xl[3], al[2], al[3]);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) d[j] += db[j];
+            for (int j = 0; j < 4; ++j) d[j] += db0[j] + db1[j];
           }
           // lane (g, tq): T[col 2·tq][v g] and T[col 2·tq + 1][v g] (hi and lo rows summed)
           float t0 = d[0] + d[2], t1 = d[1] + d[3];
@@ -976,18 +1138,20 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           tf32_split(t0, th0, tl0);
           tf32_split(t1, th1, tl1);
           // phase 2: Y += A·T over this warp's 16-row tiles
-          const float* ce = tile + (2 * tq) * 128 + (g & 3);      // column 2·tq
-          const float* co = tile + (2 * tq + 1) * 128 + (g & 3);  // column 2·tq + 1
-          const int se = tc_swz(2 * tq), so = tc_swz(2 * tq + 1);
+          const int ce = 2 * tq, co = 2 * tq + 1;  // the lane's columns
+          const float* pe = tile + ce * 32 + (g & 3);
+          const float* po = tile + co * 32 + (g & 3);
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             if (i >= nblk) break;
-            const int q0 = 4 * i + (g >> 2), q1 = q0 + 2;  // chunks of rows 16i + g, + 8
+            // rows 16i + g and 16i + g + 8: box i/2, 16-byte chunks q0 and q0 + 2 of its lines
+            const int q0 = 4 * (i & 1) + (g >> 2), q1 = q0 + 2;
+            const int bo = (i >> 1) * 256;
             uint32_t ah[4], al[4];
-            tf32_split(ce[4 * (q0 ^ se)], ah[0], al[0]);
-            tf32_split(ce[4 * (q1 ^ se)], ah[1], al[1]);
-            tf32_split(co[4 * (q0 ^ so)], ah[2], al[2]);
-            tf32_split(co[4 * (q1 ^ so)], ah[3], al[3]);
+            tf32_split(pe[bo + 4 * (q0 ^ ce)], ah[0], al[0]);
+            tf32_split(pe[bo + 4 * (q1 ^ ce)], ah[1], al[1]);
+            tf32_split(po[bo + 4 * (q0 ^ co)], ah[2], al[2]);
+            tf32_split(po[bo + 4 * (q1 ^ co)], ah[3], al[3]);
             // three products from zero (small terms first), then one rounded FP32 add per
             // element into Y, which sums over every group of the pass
             float dt[4] = {0.f, 0.f, 0.f, 0.f};
@@ -1000,7 +1164,9 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
           __syncwarp();  // every lane is done with this stage before it is refilled
           st ^= 1;
         }
-        cp_async_wait_all();  // only empty groups can still be open here
+        // (every copy issued was waited on: none can still be landing in the tiles)
+        if (__syncthreads_or(tfail ? 1 : 0)) tfail_mi = mi;
+        tfail = tdead;
         // the team partials of Y through yred (which shares the tiles' memory), summed over the
         // teams in a fixed order by team 0
         __syncthreads();
@@ -1303,6 +1469,10 @@ struct amm_batch {
   uint32_t* d_states0 = nullptr;  // seeded xorshift states (AMM mode), copied per run
   uint32_t* d_states = nullptr;
   float* d_vr = nullptr;          // AMM mode with variance reduction: per-CTA memo pairs
+  // exact batches of 8 vectors: one tensor map per matrix for the tensor-core kernel's tile
+  // copies (null when they cannot be encoded; that kernel is then not a candidate)
+  CUtensorMap* d_tmaps = nullptr;
+  std::vector<CUtensorMap> h_tmaps;
   // optional record of the CDFs and picks (amm_batch_record)
   float* rec_cdf = nullptr;
   uint32_t* rec_picks = nullptr;
@@ -1432,6 +1602,7 @@ int launch_kernel(amm_batch* b, int variant, int cl, int grid, double* d_lam, fl
   a.rec_picks = b->rec_picks;
   a.rec_products = b->rec_products;
   a.col_start = b->d_col_start;
+  a.tmaps = b->d_tmaps;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(amm::batch::kThreads, 1, 1);
@@ -1542,7 +1713,7 @@ int autotune(amm_batch* b, double* d_lam, float* d_vec, int32_t* d_iters, cudaSt
   std::vector<std::tuple<int, int, int>> cand;  // (variant, cluster size, grid)
   for (int v = 0; v < n_var; ++v) {
     if (amm::batch::kVariants[v].K != b->cfg.nvec) continue;
-    if (amm::batch::kVariants[v].tc && b->amm) continue;  // the tensor-core kernel is exact-only
+    if (amm::batch::kVariants[v].tc && (b->amm || !b->d_tmaps)) continue;  // exact-only, maps
     if (b->cfg.tile_gc > 0 && amm::batch::kVariants[v].GC != b->cfg.tile_gc) continue;
     for (int cl : amm::batch::kClusterSizes) {
       if (b->cfg.cluster > 0 && cl != b->cfg.cluster) continue;
@@ -1641,6 +1812,44 @@ void amm_batch_config_default(amm_batch_config* c) {
   c->vr_period = 0;
 }
 
+// The driver's tensor-map encoder (cuTensorMapEncodeTiled), looked up once through the
+// runtime; null if the driver does not offer it.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The tensor maps of the tensor-core kernel's tile copies, one per matrix: FP32, dims {m, n}
+// (rows innermost; row stride ld·4 bytes, a multiple of 16 by the batch's alignment rule),
+// boxes of 32 rows x 8 columns with the 128-byte swizzle, zeros outside the matrix.  False if
+// any cannot be encoded.
+static bool encode_tensor_maps(const std::vector<Mat>& ms, std::vector<CUtensorMap>& out) {
+  const auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  out.resize(ms.size());
+  for (size_t i = 0; i < ms.size(); ++i) {
+    const Mat& M = ms[i];
+    const cuuint64_t dims[2] = {(cuuint64_t)M.m, (cuuint64_t)M.n};
+    const cuuint64_t strides[1] = {(cuuint64_t)M.ld * sizeof(float)};
+    const cuuint32_t box[2] = {32, (cuuint32_t)amm::batch::kTcCols};
+    const cuuint32_t elem[2] = {1, 1};
+    if (enc(&out[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(M.A), dims, strides,
+            box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
+
 int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t count,
                      const amm_batch_config* cfg, int device) {
   if (!out || !mats || !cfg || count < 1 || count > (1 << 20)) return AMM_ERR_INVALID_ARGUMENT;
@@ -1716,6 +1925,9 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   const bool with_vr = amm_mode && cfg->vr_period > 0;
   const size_t vr_floats = (size_t)amm::batch::kVrSlot * amm::batch::kMaxRows * cfg->nvec;
   const size_t o_vr = with_vr ? carve(sizeof(float) * vr_floats * b->nsm, 256) : 0;
+  // tensor maps (64-byte aligned each) when the tensor-core kernel can run: exact, 8 vectors
+  const bool with_tmaps = !amm_mode && cfg->nvec == 8 && encode_tensor_maps(ms, b->h_tmaps);
+  const size_t o_tmaps = with_tmaps ? carve(sizeof(CUtensorMap) * count, 256) : 0;
   cudaError_t e = cudaMalloc(&b->mem, bytes);
   if (e != cudaSuccess) {
     delete b;
@@ -1731,6 +1943,7 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
   b->d_states0 = reinterpret_cast<uint32_t*>(base + o_st0);
   b->d_states = reinterpret_cast<uint32_t*>(base + o_st);
   b->d_vr = with_vr ? reinterpret_cast<float*>(base + o_vr) : nullptr;
+  b->d_tmaps = with_tmaps ? reinterpret_cast<CUtensorMap*>(base + o_tmaps) : nullptr;
   std::vector<int64_t> cs((size_t)count + 1, 0);
   for (int64_t i = 0; i < count; ++i) cs[i + 1] = cs[i] + ms[i].n;
   e = cudaMemcpy(b->d_mats, ms.data(), sizeof(Mat) * count, cudaMemcpyHostToDevice);
@@ -1738,6 +1951,9 @@ int amm_batch_create(amm_batch** out, const amm_batch_matrix* mats, int64_t coun
     e = cudaMemcpy(b->d_order, b->order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_col_start, cs.data(), sizeof(int64_t) * (count + 1),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && with_tmaps)
+    e = cudaMemcpy(b->d_tmaps, b->h_tmaps.data(), sizeof(CUtensorMap) * count,
                    cudaMemcpyHostToDevice);
   if (e == cudaSuccess && nst > 0) {
     // xorshift32 states: a splitmix64 stream from the seed (never zero, a fixed point)
@@ -1885,9 +2101,14 @@ int amm_batch_set_matrices(amm_batch* b, const amm_batch_matrix* mats, int64_t c
     b->mats[i].ld = mats[i].ld;
   }
   Guard g(b->device);
-  // pageable source: the copy is staged before the call returns, then stream-ordered
+  // pageable sources: each copy is staged before the call returns, then stream-ordered
   BATCH_CUDA(cudaMemcpyAsync(b->d_mats, b->mats.data(), sizeof(Mat) * count,
                              cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)));
+  if (b->d_tmaps) {
+    if (!encode_tensor_maps(b->mats, b->h_tmaps)) return fail(cudaErrorInvalidValue, "tensor maps");
+    BATCH_CUDA(cudaMemcpyAsync(b->d_tmaps, b->h_tmaps.data(), sizeof(CUtensorMap) * count,
+                               cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)));
+  }
   return AMM_OK;
 }
 

@@ -84,6 +84,18 @@ __device__ __forceinline__ void cp_async16_zfill(void* smem_dst, const void* gsr
                "l"(gsrc), "r"(src_bytes)
                : "memory");
 }
+// 2-D tensor copy (TMA) of one box at element coordinates (x, y) of the tensor map at `tmap`
+// (global memory) into this CTA's shared memory, completing bytes on `bar` (complete_tx).  x is
+// the innermost coordinate; x times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const void* tmap, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(smem_dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // waits until at most N of this thread's committed copy groups are still in flight
 template <int N>
