@@ -151,6 +151,67 @@ def test_batch_tensor_core_product_vs_fp64(amm_lib, cluster):
 
 
 @pytest.mark.gpu
+def test_batch_tensor_core_small_and_padded_shapes(amm_lib):
+    """The tensor-core product's TMA tile copies (boxes of 32 rows x 8 columns, zeros outside
+    the matrix) on shapes that do not fill them: fewer rows than a box (m = 8, 13, 31), ragged
+    last boxes and groups (m = 33, 100; n = 9, 300), and a leading dimension well past m (the
+    rows between m and ld hold garbage that must not be read).  λ is within 1e-5 of FP64 at the
+    1e-6 residual; at a fixed 20 products the Ritz values are within 1e-5 (of λ_max) of the
+    CUDA-core product's; and rebinding to other matrices of the same shapes, which re-encodes
+    the tensor maps, gives bit for bit what a new solver on them gives."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver
+    sizes = [(8, 8), (13, 9), (31, 300), (33, 40), (100, 9), (100, 300)]
+    pads = [0, 12, 4, 20, 0, 28]  # extra rows of leading dimension past m rounded up to 4
+
+    def device(host):
+        keep = []
+        for A, pad in zip(host, pads):
+            m, n = A.shape
+            ld = (m + 3) // 4 * 4 + pad
+            buf = torch.full((n, ld), float("nan"), dtype=torch.float32, device="cuda")
+            buf[:, :m] = torch.from_numpy(A.T.copy()).cuda()
+            keep.append((buf, buf.t()[:m]))
+        return keep
+
+    host = _mats(sizes, seed=41)
+    keep = device(host)
+    mats = [v for _, v in keep]
+    tc = BatchSolver(mats, nvec=8, max_iter=3000, tol=1e-6, tile_gc=8, cluster=1)
+    lam, _, iters = tc.run()
+    torch.cuda.synchronize()
+    assert tc.tile_choice() == (8, 8, 1)
+    lam, it = lam.cpu().numpy(), iters.cpu().numpy()
+    for i, A in enumerate(host):
+        w, _ = _eigh_top(A)
+        assert 0 < it[i] < 3000, (i, it[i])
+        assert abs(lam[i] - w[0]) <= 1e-5 * w[0], (i, lam[i], w[0], it[i])
+    tc.close()
+    fixed = {}
+    for gc in (8, 4):
+        bs = BatchSolver(mats, nvec=8, max_iter=20, tol=0.0, tile_gc=gc, cluster=1)
+        bs.run()
+        torch.cuda.synchronize()
+        fixed[gc] = bs.lam.cpu().numpy()
+        if gc == 8:
+            host2 = _mats(sizes, seed=43)
+            keep2 = device(host2)
+            bs.set_matrices([v for _, v in keep2])
+            bs.run()
+            torch.cuda.synchronize()
+            rebound = bs.lam.cpu().numpy()
+            fresh = BatchSolver([v for _, v in keep2], nvec=8, max_iter=20, tol=0.0, tile_gc=8,
+                                cluster=1)
+            fresh.run()
+            torch.cuda.synchronize()
+            assert np.array_equal(rebound, fresh.lam.cpu().numpy())
+            fresh.close()
+        bs.close()
+    assert np.all(np.isfinite(fixed[8]))
+    scale = fixed[4][:, :1]
+    assert np.all(np.abs(fixed[8] - fixed[4]) <= 1e-5 * scale), np.abs(fixed[8] - fixed[4]).max()
+
+
+@pytest.mark.gpu
 def test_batch_tensor_core_product_long_passes(amm_lib):
     """Long passes (up to 8192 columns, 1024 groups of 8 in one CTA): the tensor core's own
     accumulation is not rounded to nearest, so the product keeps every chain of tensor-core
