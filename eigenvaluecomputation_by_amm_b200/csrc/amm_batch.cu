@@ -14,6 +14,8 @@
 // ring that keeps two or more groups in flight), forms the K·GC partial dots A_jᵀX over its
 // rows, reduces them across the team (warp butterfly, then shared memory for teams wider than a
 // warp) and accumulates Y += A_j·(A_jᵀX): the fused single-pass product of the main kernel.
+// Exact batches of 8 vectors take a tensor-core form of the same product instead (TF32
+// mma.sync with a hi + lo split, column tiles copied by TMA; see batch_kernel).
 // After the pass the team partials of Y are summed in a fixed order, the Gram matrices
 // G = YᵀY and H = XᵀY are reduced in FP64, X <- Y·R⁻¹ (Cholesky QR), and every rr_period
 // iterations (and at the end) H is diagonalised by a warp-parallel cyclic Jacobi in FP64: its
@@ -256,7 +258,8 @@ struct Ring {
   static constexpr int stages = kRingBytes / (kThreads * GC * 16);
 };
 
-// Tensor-core product: per warp and stage, 8 columns x 128 rows (4 KB); two stages.
+// Tensor-core product: per warp and stage, 8 columns x 128 rows (4 KB, four 32 x 8 TMA boxes);
+// two stages.
 constexpr int kTcCols = 8;
 constexpr int kTcWarpFloats = kTcCols * 128;
 constexpr int kTcStageFloats = kWarps * kTcWarpFloats;
