@@ -264,8 +264,8 @@ def grad_report(reps=5, fd_entries=32):
                             "achieved_gbs": grad_bytes / (t_grad * 1e-3) / 1e9,
                             "frac": grad_bytes / (t_grad * 1e-3) / 1e9 / hbm, "peak": hbm,
                             "peak_source": src,
-                            "note": "m·n·(4 + 4) bytes per matrix: A read, ∂λ/∂A written; the "
-                                    "64 MB batch is L2-resident between launches"},
+                            "note": "m·n·(4 + 4) bytes per matrix: A read, ∂λ/∂A written; "
+                                    "268 MB of each per launch, larger than L2"},
             "grad_rel_err_vs_fp64_eigvalsh": rel, "lambda_rel_err_max": lam_err,
             "fd_max_abs_err_over_max_grad": fd_err, "fd_entries": fd_entries, "fd_h": h}
 

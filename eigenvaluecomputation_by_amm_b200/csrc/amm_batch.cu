@@ -1384,32 +1384,120 @@ struct GradArgs {
   float* const* grads;       // count pointers
   const int64_t* grad_ld;    // count
   const float* scale;        // count (upstream gradient per matrix), or null (1)
+  int32_t vs_len;            // floats of a warp's copy of v: the largest m, rounded up to 4
 };
 
-__global__ void __launch_bounds__(256) grad_kernel(const __grid_constant__ GradArgs a) {
-  const int64_t total = a.col_start[a.count];
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  for (int64_t gc = gw; gc < total; gc += nw) {
-    int lo = 0, hi = a.count - 1;  // matrix of global column gc
+// Column prefixes a CTA of the backward keeps in shared memory (larger batches search global
+// memory).
+constexpr int kGradSmemMats = 4096;
+
+// Each warp takes a contiguous range of columns (an even share of all the batch's columns), two
+// adjacent columns at a time: both columns' loads are in flight together and their two dots
+// share one warp reduction.  The matrix of a column is found in the column prefix (copied to
+// shared memory once per CTA) by a search forward from the warp's previous matrix; when the warp
+// enters a matrix it copies v into its own 16-byte aligned shared-memory slot, so that A, v and
+// the gradient all move in 16-byte accesses (A and the gradient streaming; a gradient column
+// that does not start 16-byte aligned takes 4-byte stores).
+struct GradMat {
+  Mat M;
+  int64_t c0 = 0, c1 = 0;  // column range
+  float* g = nullptr;
+  int64_t gld = 0;
+  float k = 1.f;  // 2·scale
+  int mi = -1;
+};
+
+__device__ __forceinline__ void grad_store(const GradMat& G, const float* vs, int64_t j, float k,
+                                           int lane) {
+  const int m = G.M.m, m4 = m >> 2;
+  float* g = G.g + j * G.gld;
+  if ((reinterpret_cast<uintptr_t>(g) & 15u) == 0u) {
+#pragma unroll 4
+    for (int r4 = lane; r4 < m4; r4 += 32) {
+      const float4 vv = reinterpret_cast<const float4*>(vs)[r4];
+      __stcs(reinterpret_cast<float4*>(g) + r4, make_float4(k * vv.x, k * vv.y, k * vv.z, k * vv.w));
+    }
+    for (int r = 4 * m4 + lane; r < m; r += 32) g[r] = k * vs[r];
+  } else {
+    for (int r = lane; r < m; r += 32) g[r] = k * vs[r];
+  }
+}
+
+// this lane's part of the dot of column j with v
+__device__ __forceinline__ float grad_dot(const GradMat& G, const float* vs, int64_t j, int lane) {
+  const int m = G.M.m, m4 = m >> 2;
+  const float4* col4 = reinterpret_cast<const float4*>(G.M.A + j * G.M.ld);
+  float s = 0.f;
+#pragma unroll 4
+  for (int r4 = lane; r4 < m4; r4 += 32) {
+    const float4 c = __ldcs(col4 + r4);
+    const float4 vv = reinterpret_cast<const float4*>(vs)[r4];
+    s = fmaf(c.x, vv.x, s);
+    s = fmaf(c.y, vv.y, s);
+    s = fmaf(c.z, vv.z, s);
+    s = fmaf(c.w, vv.w, s);
+  }
+  for (int r = 4 * m4 + lane; r < m; r += 32) s = fmaf(G.M.A[j * G.M.ld + r], vs[r], s);
+  return s;
+}
+
+__global__ void __launch_bounds__(256, 4) grad_kernel(const __grid_constant__ GradArgs a) {
+  // dynamic shared memory: 8 warp slots of vs_len floats (16-byte multiples), then the column
+  // prefixes when count <= kGradSmemMats
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* vs = reinterpret_cast<float*>(gsm) + (size_t)warp * a.vs_len;
+  int64_t* cs_s = reinterpret_cast<int64_t*>(gsm + sizeof(float) * 8 * (size_t)a.vs_len);
+  const int count = a.count;
+  const bool in_smem = count <= kGradSmemMats;
+  if (in_smem)
+    for (int i = threadIdx.x; i <= count; i += blockDim.x) cs_s[i] = a.col_start[i];
+  __syncthreads();
+  auto cstart = [&](int i) -> int64_t { return in_smem ? cs_s[i] : __ldg(a.col_start + i); };
+  // the matrix holding column gc (gc not below the range of G): forward search from G's; on a
+  // change v is copied into this warp's slot (every lane reads only after the __syncwarp)
+  auto locate = [&](GradMat& G, int64_t gc) {
+    if (gc < G.c1) return;
+    int lo = G.mi + 1, hi = count - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (a.col_start[mid] <= gc)
+      if (cstart(mid) <= gc)
         lo = mid;
       else
         hi = mid - 1;
     }
-    const Mat M = a.mats[lo];
-    const int64_t j = gc - a.col_start[lo];
-    const float* col = M.A + j * M.ld;
-    const float* v = a.vec + M.out_off;
-    float s = 0.f;
-    for (int r = lane; r < M.m; r += 32) s = fmaf(col[r], v[r], s);
-    s = warp_sum(s);
-    const float k = 2.f * s * (a.scale ? a.scale[lo] : 1.f);
-    float* g = a.grads[lo] + j * a.grad_ld[lo];
-    for (int r = lane; r < M.m; r += 32) g[r] = k * v[r];
+    G.mi = lo;
+    G.M = a.mats[lo];
+    G.c0 = cstart(lo);
+    G.c1 = cstart(lo + 1);
+    G.g = a.grads[lo];
+    G.gld = a.grad_ld[lo];
+    G.k = 2.f * (a.scale ? a.scale[lo] : 1.f);
+    __syncwarp();  // every lane is done with the slot's previous vector
+    const float* v = a.vec + G.M.out_off;
+    for (int r = lane; r < G.M.m; r += 32) vs[r] = v[r];
+    __syncwarp();
+  };
+  const int64_t total = cstart(count);
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t b0 = gw * total / nw, b1 = (gw + 1) * total / nw;  // this warp's columns
+  GradMat G;
+  for (int64_t gc = b0; gc < b1;) {
+    locate(G, gc);
+    const int64_t j = gc - G.c0;
+    if (gc + 1 < b1 && gc + 1 < G.c1) {  // two columns of one matrix (the usual case)
+      float d[2] = {grad_dot(G, vs, j, lane), grad_dot(G, vs, j + 1, lane)};
+      const float s = warp_reduce_multi<float, 2>(d, lane);  // lane < 16: column j, else j + 1
+      const float s0 = __shfl_sync(0xffffffffu, s, 0), s1 = __shfl_sync(0xffffffffu, s, 16);
+      grad_store(G, vs, j, G.k * s0, lane);
+      grad_store(G, vs, j + 1, G.k * s1, lane);
+      gc += 2;
+    } else {
+      const float s0 = warp_sum(grad_dot(G, vs, j, lane));
+      grad_store(G, vs, j, G.k * s0, lane);
+      gc += 1;
+    }
   }
 }
 
@@ -2079,10 +2167,23 @@ int amm_batch_grad(amm_batch* b, const float* d_vectors, void* const* grad_ptrs,
   a.grads = b->d_grads;
   a.grad_ld = b->d_grad_ld;
   a.scale = d_scale;
-  int64_t warps = b->total_cols;
-  int64_t blocks = (warps * 32 + 255) / 256;
-  if (blocks > (int64_t)b->nsm * 16) blocks = (int64_t)b->nsm * 16;
-  amm::batch::grad_kernel<<<(int)blocks, 256, 0, s>>>(a);
+  // one warp per contiguous range of columns; a grid of the CTAs resident at once, 8 warps each
+  int max_m = 1;
+  for (const auto& M : b->mats) max_m = std::max(max_m, (int)M.m);
+  a.vs_len = (max_m + 3) / 4 * 4;
+  const size_t smem = sizeof(float) * 8 * (size_t)a.vs_len +
+                      (b->count <= amm::batch::kGradSmemMats
+                           ? sizeof(int64_t) * (size_t)(b->count + 1) : 0);
+  if (smem > 48 * 1024)
+    BATCH_CUDA(cudaFuncSetAttribute(amm::batch::grad_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  BATCH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amm::batch::grad_kernel, 256,
+                                                           smem));
+  const int64_t warps = b->total_cols;  // at least one column per warp
+  int64_t blocks = (warps + 7) / 8;
+  blocks = std::min<int64_t>(blocks, (int64_t)b->nsm * std::max(per_sm, 1));
+  amm::batch::grad_kernel<<<(int)blocks, 256, smem, s>>>(a);
   amm::count_launch(1);
   BATCH_CUDA(cudaGetLastError());
   // (the pointer arrays come from pageable host memory: the copies above were staged before
@@ -2099,19 +2200,24 @@ int amm_batch_set_matrices(amm_batch* b, const amm_batch_matrix* mats, int64_t c
       return AMM_ERR_INVALID_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(x.A) & 15) != 0 || (x.ld % 4) != 0) return AMM_ERR_ALIGNMENT;
   }
+  // the new descriptors (and tensor maps) are formed first, so that a failure leaves the
+  // context bound to the old matrices as a whole
+  std::vector<Mat> ms = b->mats;
   for (int64_t i = 0; i < count; ++i) {
-    b->mats[i].A = static_cast<const float*>(mats[i].A);
-    b->mats[i].ld = mats[i].ld;
+    ms[i].A = static_cast<const float*>(mats[i].A);
+    ms[i].ld = mats[i].ld;
   }
+  std::vector<CUtensorMap> tm;
+  if (b->d_tmaps && !encode_tensor_maps(ms, tm)) return fail(cudaErrorInvalidValue, "tensor maps");
+  b->mats.swap(ms);
+  if (b->d_tmaps) b->h_tmaps.swap(tm);
   Guard g(b->device);
   // pageable sources: each copy is staged before the call returns, then stream-ordered
   BATCH_CUDA(cudaMemcpyAsync(b->d_mats, b->mats.data(), sizeof(Mat) * count,
                              cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)));
-  if (b->d_tmaps) {
-    if (!encode_tensor_maps(b->mats, b->h_tmaps)) return fail(cudaErrorInvalidValue, "tensor maps");
+  if (b->d_tmaps)
     BATCH_CUDA(cudaMemcpyAsync(b->d_tmaps, b->h_tmaps.data(), sizeof(CUtensorMap) * count,
                                cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)));
-  }
   return AMM_OK;
 }
 
