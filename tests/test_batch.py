@@ -303,6 +303,42 @@ def test_batch_gradient_scale_and_layout(amm_lib):
 
 
 @pytest.mark.gpu
+def test_batch_gradient_many_small_matrices_unaligned(amm_lib):
+    """The backward on more matrices than its column prefix keeps in shared memory (4200 > 4096:
+    the search runs in global memory), with m not a multiple of 4 (the last chunk of a column)
+    and gradient columns that do not start 16-byte aligned (leading dimension m + 1: the 4-byte
+    stores): every gradient equals scale_b·2·v(vᵀA) within FP32 rounding, and the rows past m
+    are not written."""
+    from eigenvaluecomputation_by_amm_b200 import BatchSolver
+    rng = np.random.default_rng(17)
+    count = 4200
+    ms = rng.choice([8, 9, 10, 13], size=count)
+    ns = rng.choice([8, 11, 16], size=count)
+    host = [rng.standard_normal((int(m), int(n))).astype(np.float32) for m, n in zip(ms, ns)]
+    keep = [_device_col_major(A) for A in host]
+    bs = BatchSolver([v for _, v in keep], nvec=8, max_iter=50, tol=1e-6)
+    bs.run()
+    grads, stores = [], []
+    for A in host:
+        m, n = A.shape
+        gb = torch.full((n, m + 1), 7.0, device="cuda")
+        stores.append(gb)
+        grads.append(gb.t()[:m])
+    scale = torch.from_numpy(rng.uniform(-2.0, 2.0, count).astype(np.float32)).cuda()
+    bs.grad(grads, scale=scale)
+    torch.cuda.synchronize()
+    vecs = bs.vectors.double().cpu().numpy()
+    sc = scale.double().cpu().numpy()
+    for i, A in enumerate(host):
+        v = vecs[int(bs.offsets[i]):int(bs.offsets[i]) + A.shape[0]]
+        want = sc[i] * 2.0 * np.outer(v, v @ A.astype(np.float64))
+        got = grads[i].double().cpu().numpy()
+        np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-5 * np.abs(want).max() + 1e-30)
+        assert torch.all(stores[i][:, A.shape[0]:] == 7.0)
+    bs.close()
+
+
+@pytest.mark.gpu
 def test_batch_amm_mode_spiked_matrices(amm_lib):
     """Previous-AMM products (c = n/8) in the batch: reproducible from the seed, identical with
     one launch per matrix, and within 2% of λ_max where a spike shared by every column dominates
